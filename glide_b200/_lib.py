@@ -1,0 +1,152 @@
+"""ctypes binding of the C ABI in include/glide_b200.h (libglide_b200.so).
+
+The product path has no CPU fallback: if the sm_100a library is missing or
+fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "_lib" / "libglide_b200.so"
+
+GLIDE_OK = 0
+GLIDE_ERR_ARG = 1
+GLIDE_ERR_SHAPE = 2
+GLIDE_ERR_CUDA = 3
+GLIDE_ERR_NONFINITE = 4
+GLIDE_ERR_STATE = 5
+GLIDE_F64 = 0
+GLIDE_F32 = 1
+
+FIELDS = [
+    "u", "v", "H", "H_prev", "phi", "mask", "bed", "B", "beta", "smb", "gamma",
+    "f_u", "f_v", "f_H", "r_u", "r_v", "r_H",
+    "lambda_u", "lambda_v", "lambda_H",
+    "adj_f_u", "adj_f_v", "adj_f_H", "adj_r_u", "adj_r_v", "adj_r_H",
+    "grad_beta", "grad_bed", "grad_H_prev", "grad_smb",
+    "vjp_u", "vjp_v", "vjp_H",
+    "F_u", "F_v", "F_H",
+]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+
+USE_MASK = 1
+OPERATOR_ONLY = 2
+FREEZE_CALVING = 4
+FREEZE_PHI = 8
+
+GRAD_BETA = 1
+GRAD_BED = 2
+GRAD_H_PREV = 4
+GRAD_SMB = 8
+GRAD_ALL = 15
+
+MAX_HISTORY = 256
+
+
+class GlideError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"glide_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Phys(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "n", "eps_reg", "flotation_reg_driving", "m", "u_reg", "water_drag",
+        "flotation_reg_sliding", "calving_rate", "flotation_reg_calving", "thklim")]
+
+
+class FasConfig(ctypes.Structure):
+    _fields_ = [("freeze_coarse_calving", ctypes.c_int), ("freeze_coarse_phi", ctypes.c_int),
+                ("coarsest_steps", ctypes.c_int), ("pre_steps", ctypes.c_int),
+                ("post_steps", ctypes.c_int), ("finest_steps", ctypes.c_int),
+                ("maximum_vcycles", ctypes.c_int), ("relative_tolerance", ctypes.c_double),
+                ("absolute_tolerance", ctypes.c_double)]
+
+
+class VankaConfig(ctypes.Structure):
+    _fields_ = [("omega", ctypes.c_double), ("newton_steps", ctypes.c_int),
+                ("relaxation", ctypes.c_double), ("ssa_damping", ctypes.c_double),
+                ("mc_damping", ctypes.c_double), ("relax_phi", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("vcycles", ctypes.c_int), ("initial_norm", ctypes.c_double),
+                ("final_norm", ctypes.c_double), ("norms", ctypes.c_double * 3),
+                ("history", ctypes.c_double * MAX_HISTORY)]
+
+    def to_dict(self):
+        n = self.vcycles
+        return dict(vcycles=n, initial_norm=self.initial_norm, final_norm=self.final_norm,
+                    norms=list(self.norms), history=list(self.history[: min(n + 1, MAX_HISTORY)]))
+
+
+_H = ctypes.c_void_p
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+SIGNATURES = {
+    "glide_last_error": ([], ctypes.c_char_p),
+    "glide_version": ([], _I),
+    "glide_create": ([_I, _I, _D, _I, _I, ctypes.POINTER(_H)], _I),
+    "glide_destroy": ([_H], _I),
+    "glide_level_shape": ([_H, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D)], _I),
+    "glide_field_ptr": ([_H, _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                         ctypes.POINTER(_I)], _I),
+    "glide_set_field": ([_H, _I, _I, _P, _I, _I, _I, _P], _I),
+    "glide_get_field": ([_H, _I, _I, _P, _I, _I, _P], _I),
+    "glide_fill_field": ([_H, _I, _I, _D, _I, _P], _I),
+    "glide_restrict_field": ([_H, _I, _I, _P], _I),
+    "glide_set_phys": ([_H, _I, ctypes.POINTER(Phys)], _I),
+    "glide_get_phys": ([_H, _I, ctypes.POINTER(Phys)], _I),
+    "glide_set_fas_config": ([_H, _I, ctypes.POINTER(FasConfig)], _I),
+    "glide_get_fas_config": ([_H, _I, ctypes.POINTER(FasConfig)], _I),
+    "glide_set_vanka_config": ([_H, _I, _I, ctypes.POINTER(VankaConfig)], _I),
+    "glide_get_vanka_config": ([_H, _I, _I, ctypes.POINTER(VankaConfig)], _I),
+    "glide_set_reference_quirks": ([_H, _I], _I),
+    "glide_set_use_graphs": ([_H, _I], _I),
+    "glide_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], _I),
+    "glide_set_rhs": ([_H, _I, _D, _P], _I),
+    "glide_compute_phi": ([_H, _I, _D, _P], _I),
+    "glide_residual": ([_H, _I, _D, _I, ctypes.POINTER(_D), _P], _I),
+    "glide_vanka_sweep": ([_H, _I, _D, _I, _I, _P, _P], _I),
+    "glide_forward": ([_H, _D, _I, ctypes.POINTER(Stats), _P], _I),
+    "glide_adjoint_residual": ([_H, _I, _D, ctypes.POINTER(_D), _P], _I),
+    "glide_vjp": ([_H, _I, _D, _P], _I),
+    "glide_adjoint_sweep": ([_H, _I, _D, _I, _P], _I),
+    "glide_gradients": ([_H, _I, _D, _I, _P], _I),
+    "glide_backward": ([_H, _D, _I, _I, ctypes.POINTER(Stats), _P], _I),
+}
+
+_LIB = None
+
+
+def load(path: str | os.PathLike | None = None):
+    """Load libglide_b200.so (once) and declare every exported signature."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise GlideError(GLIDE_ERR_STATE, f"{p} is missing; build it with `python -m glide_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    for name, (argtypes, restype) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = restype
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def check(code: int):
+    if code != GLIDE_OK:
+        msg = load().glide_last_error()
+        raise GlideError(code, msg.decode() if msg else "")
+
+
+def call(name: str, *args):
+    check(getattr(load(), name)(*args))

@@ -1,0 +1,253 @@
+// forward_kernels.cuh -- residual, fused Vanka sweep and grounding kernels.
+#pragma once
+
+#include "stencil.cuh"
+#include "tile.cuh"
+
+namespace glide {
+
+constexpr int kTile = 16;
+
+// -------------------------------------------------------------------------
+// Residual of the coupled system on one level (residuals.cu:6-333 and the
+// host wrapper glide/operators.py:71-127), one thread per cell: the cell's
+// mass residual, its left u face and its top v face, plus the right/bottom
+// boundary faces for the last column/row.  Optionally subtracts a given
+// field (`sub_*`, used to form the coarse FAS right-hand side F(x_c) - R r in
+// the same pass) and accumulates per-block sums of squares for the norms.
+// -------------------------------------------------------------------------
+template <class R>
+struct ResidualArgs {
+    Arr<R> u, v, H, phi, mask, bed, B, beta, gamma;
+    Arr<R> f_u, f_v, f_H;        // forcing, used when use_forcing
+    Arr<R> o_u, o_v, o_H;        // outputs
+    Arr<R> s_u, s_v, s_H;        // optional subtrahends (p == nullptr: none)
+    double* partial;             // optional: 3 sums of squares per block
+    PhysR<R> p;
+    int ny, nx;
+    int use_forcing, use_mask;
+};
+
+template <class R>
+__global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a) {
+    using TileT = Tile<R, kTile, 1, 1>;
+    constexpr int NC = TileT::NC;
+    __shared__ TileT t;
+    __shared__ double red[3][8];
+    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int ny = a.ny, nx = a.nx;
+    stage_tile<R, kTile, 1, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
+    __syncthreads();
+    TileView<R, kTile, 1, 1> s{t, i0, j0, ny, nx};
+    for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
+        int r = k / NC, c = k % NC;
+        int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        R Bc = ldg(&a.B.p[size_t(clampi(gi, 0, ny - 1)) * a.B.pitch + clampi(gj, 0, nx - 1)]);
+        t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x / kTile, j = j0 + threadIdx.x % kTile;
+    double ssu = 0, ssv = 0, ssh = 0;
+    if (i < ny && j < nx) {
+        const bool f = a.use_forcing != 0;
+        {
+            R fH = f ? a.f_H.at(i, j) : R(0);
+            R r = mass_residual<R>(s, a.p, i, j, fH);
+            R msk = a.use_mask ? a.mask.at(i, j) : R(0);
+            R Hc = s.Hc(i, j);
+            r = (R(1) - msk) * r + msk * (Hc - a.gamma.at(i, j));
+            if (a.s_H.p) r = r - a.s_H.at(i, j);
+            a.o_H.at(i, j) = r;
+            ssh += double(r) * double(r);
+        }
+        {
+            R r = umom_residual<R>(s, a.p, i, j, f ? a.f_u.at(i, j) : R(0));
+            if (a.s_u.p) r = r - a.s_u.at(i, j);
+            a.o_u.at(i, j) = r;
+            ssu += double(r) * double(r);
+            if (j == nx - 1) {
+                R r2 = umom_residual<R>(s, a.p, i, nx, f ? a.f_u.at(i, nx) : R(0));
+                if (a.s_u.p) r2 = r2 - a.s_u.at(i, nx);
+                a.o_u.at(i, nx) = r2;
+                ssu += double(r2) * double(r2);
+            }
+        }
+        {
+            R r = vmom_residual<R>(s, a.p, i, j, f ? a.f_v.at(i, j) : R(0));
+            if (a.s_v.p) r = r - a.s_v.at(i, j);
+            a.o_v.at(i, j) = r;
+            ssv += double(r) * double(r);
+            if (i == ny - 1) {
+                R r2 = vmom_residual<R>(s, a.p, ny, j, f ? a.f_v.at(ny, j) : R(0));
+                if (a.s_v.p) r2 = r2 - a.s_v.at(ny, j);
+                a.o_v.at(ny, j) = r2;
+                ssv += double(r2) * double(r2);
+            }
+        }
+    }
+    if (a.partial) {
+        // fixed-order block reduction: warp shuffles, then warp 0
+        for (int o = 16; o > 0; o >>= 1) {
+            ssu += __shfl_down_sync(0xffffffffu, ssu, o);
+            ssv += __shfl_down_sync(0xffffffffu, ssv, o);
+            ssh += __shfl_down_sync(0xffffffffu, ssh, o);
+        }
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0) { red[0][w] = ssu; red[1][w] = ssv; red[2][w] = ssh; }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double acc = 0;
+            for (int q = 0; q < 8; ++q) acc += red[threadIdx.x][q];
+            a.partial[size_t(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = acc;
+        }
+    }
+}
+
+// Sum the per-block partials in a fixed order and take square roots:
+// out[0..2] = |r_u|, |r_v|, |r_H|; out[3] = sqrt of their squares' sum.
+__global__ void k_finish_norms(const double* partial, int nblocks, double* out);
+
+// -------------------------------------------------------------------------
+// Grounded fraction phi = (1-relax) sigmoid(c (bed + 0.917 H)) + relax phi
+// (viscosity.cu:17-36).
+// -------------------------------------------------------------------------
+template <class R>
+__global__ void k_grounded(Arr<R> phi, Arr<R> H, Arr<R> bed, R c, R relax, int ny, int nx) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (j >= nx) return;
+    R g = grounded_frac(H.at(i, j), bed.at(i, j), c);
+    phi.at(i, j) = (R(1) - relax) * g + relax * phi.at(i, j);
+}
+
+// -------------------------------------------------------------------------
+// One fused additive-Vanka sweep (vanka.cu:478-660 plus the host loop of
+// glide/operators.py:194-251): grounding prologue, per-cell damped local
+// Newton with the active-set projection, averaging of the face corrections of
+// the two cells sharing a face, and the omega-update -- written to a second
+// state buffer, because every cell reads its neighbours' old values.
+//
+// Block = 16x16 own cells + the 16 cells left of the tile + the 16 cells
+// above it (288 threads).  The halo cells are solved redundantly so that the
+// block owns its faces outright: no atomics, no zero fills, no separate axpy.
+// -------------------------------------------------------------------------
+enum GammaMode { kGammaArray = 0, kGammaWChi = 1, kGammaWPhi = 2 };
+
+template <class R>
+struct SweepArgs {
+    Arr<R> u, v, H;              // state in
+    Arr<R> uo, vo, Ho;           // state out
+    Arr<R> phi, mask, bed, B, beta;
+    Arr<R> f_u, f_v, f_H;
+    Arr<R> gamma;                // kGammaArray
+    Arr<R> wH, chi, chi_c;       // kGammaWChi: wH + chi; kGammaWPhi: wH + (-chi_c[i/2][j/2] + chi)
+    int* iters;                  // optional: Newton iterations per cell (pitch = phi.pitch)
+    PhysR<R> p;
+    R omega, ssa_damping, mc_damping;
+    int newton_steps;
+    int ny, nx;
+};
+
+constexpr int kSweepThreads = kTile * kTile + 2 * kTile;
+
+template <class R, int GMODE, bool PHI_LIVE>
+__global__ void __launch_bounds__(kSweepThreads) k_vanka_sweep(SweepArgs<R> a) {
+    using TileT = Tile<R, kTile, 2, 1>;
+    constexpr int NC = TileT::NC;     // 19
+    constexpr int ND = kTile + 1;     // deltas for rows/cols [i0-1, i0+16)
+    __shared__ TileT t;
+    __shared__ R dl[ND][ND][4];
+    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int ny = a.ny, nx = a.nx;
+    stage_tile<R, kTile, 2, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, PHI_LIVE ? nullptr : &a.phi);
+    __syncthreads();
+    TileView<R, kTile, 2, 1> s{t, i0, j0, ny, nx};
+    for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
+        int r = k / NC, c = k % NC;
+        int gi = i0 - 2 + r, gj = j0 - 2 + c;
+        int ci = clampi(gi, 0, ny - 1), cj = clampi(gj, 0, nx - 1);
+        R Bc = ldg(&a.B.p[size_t(ci) * a.B.pitch + cj]);
+        t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+        if (PHI_LIVE) t.phi[r][c] = grounded_frac(t.H[r][c], t.bed[r][c], a.p.c_ground);
+    }
+    __syncthreads();
+
+    // which cell does this thread solve?
+    int i, j;
+    const int tid = threadIdx.x;
+    if (tid < kTile * kTile) { i = i0 + tid / kTile; j = j0 + tid % kTile; }
+    else if (tid < kTile * kTile + kTile) { i = i0 + (tid - kTile * kTile); j = j0 - 1; }
+    else { i = i0 - 1; j = j0 + (tid - kTile * kTile - kTile); }
+    const bool live = i >= 0 && i < ny && j >= 0 && j < nx;
+    R dH = 0, masked = 0;
+    R dd[4] = {0, 0, 0, 0};
+    if (live) {
+        R x[5] = {s.U(i, j), s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.Hc(i, j)};
+        const R x0[5] = {x[0], x[1], x[2], x[3], x[4]};
+        R thk;
+        if (GMODE == kGammaArray) thk = a.gamma.at(i, j);
+        else if (GMODE == kGammaWChi) thk = a.wH.at(i, j) + a.chi.at(i, j);
+        else thk = a.wH.at(i, j) + (-a.chi_c.at(i >> 1, j >> 1) + a.chi.at(i, j));
+        masked = tid < kTile * kTile ? a.mask.at(i, j) : R(0);  // halo cells never write it
+        const R fu0 = a.f_u.at(i, j), fu1 = a.f_u.at(i, j + 1);
+        const R fv0 = a.f_v.at(i, j), fv1 = a.f_v.at(i + 1, j), fh = a.f_H.at(i, j);
+        R comp[5] = {0, 0, 0, 0, 0};
+        R rnorm = 1;
+        int k = 0;
+        const R tol = R(kNewtonTol);
+        while (k < a.newton_steps && rnorm > tol) {
+            R J[25], r[5], dx[5];
+            local_system<R>(s, a.p, i, j, x, J, r);
+            r[0] -= fu0; r[1] -= fu1; r[2] -= fv0; r[3] -= fv1; r[4] -= fh;
+            J[0] -= a.ssa_damping; J[6] -= a.ssa_damping; J[12] -= a.ssa_damping; J[18] -= a.ssa_damping;
+            J[24] += a.mc_damping;
+            if (j == 0) { pin(J, 0); r[0] = x[0]; }
+            if (j == nx - 1) { pin(J, 1); r[1] = x[1]; }
+            if (i == 0) { pin(J, 2); r[2] = x[2]; }
+            if (i == ny - 1) { pin(J, 3); r[3] = x[3]; }
+            if ((x[4] - a.p.dt * r[4]) <= thk) {
+                masked = R(1);
+                pin(J, 4);
+                r[4] = x[4] - thk;
+            } else {
+                masked = R(0);
+            }
+            lu5_solve(J, r, dx);
+            rnorm = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3] + r[4] * r[4];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {  // compensated update with the fixed relaxation 0.5
+                R y = -R(0.5) * dx[q] - comp[q];
+                R tq = x[q] + y;
+                comp[q] = (tq - x[q]) - y;
+                x[q] = tq;
+            }
+            x[4] = fmax(x[4], thk);
+            ++k;
+        }
+        if (a.iters && tid < kTile * kTile) a.iters[size_t(i) * a.phi.pitch + j] = k;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dd[q] = R(0.5) * (x[q] - x0[q]);
+        dH = x[4] - x0[4];
+    }
+    {
+        const int di = i - (i0 - 1), dj = j - (j0 - 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dl[di][dj][q] = dd[q];
+    }
+    __syncthreads();
+    if (tid < kTile * kTile && live) {
+        const int di = i - (i0 - 1), dj = j - (j0 - 1);
+        const R w = a.omega;
+        // left face: right half-correction of cell (i, j-1) + left of (i, j)
+        R du = (j > 0 ? dl[di][dj - 1][1] : R(0)) + dl[di][dj][0];
+        a.uo.at(i, j) = s.U(i, j) + w * du;
+        if (j == nx - 1) a.uo.at(i, nx) = s.U(i, nx) + w * dl[di][dj][1];
+        R dv = (i > 0 ? dl[di - 1][dj][3] : R(0)) + dl[di][dj][2];
+        a.vo.at(i, j) = s.V(i, j) + w * dv;
+        if (i == ny - 1) a.vo.at(ny, j) = s.V(ny, j) + w * dl[di][dj][3];
+        a.Ho.at(i, j) = s.Hc(i, j) + w * dH;
+        a.mask.at(i, j) = masked;
+        if (PHI_LIVE) a.phi.at(i, j) = s.PHI(i, j);
+    }
+}
+
+}  // namespace glide

@@ -1,0 +1,968 @@
+// runtime.cu -- level hierarchy, FASCD / FASAdjoint drivers and the C ABI.
+//
+// One handle owns the whole multigrid hierarchy in a single device arena:
+// every level's state, parameters, operator arrays and V-cycle scratch, each
+// 2-D array with its row pitch rounded up to 32 elements and its start aligned
+// to 256 bytes (coalesced rows; TMA-legal strides).  The V-cycle schedule runs
+// here, in C++, issuing fused kernels on the caller's stream; with graphs on,
+// one V-cycle plus its convergence-check residual is captured once and
+// replayed, so a solve costs one host synchronisation per V-cycle.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "glide_b200.h"
+#include "forward_kernels.cuh"
+#include "adjoint_kernels.cuh"
+#include "transfer_kernels.cuh"
+
+namespace glide {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+struct Fail {
+    int code;
+};
+
+[[noreturn]] static void fail(int code, const std::string& msg) {
+    g_err = msg;
+    throw Fail{code};
+}
+
+#define GCU(call)                                                                       \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            fail(GLIDE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+static void check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(GLIDE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+__global__ void k_finish_norms(const double* partial, int nblocks, double* out) {
+    // one warp: lane-strided sums, then a fixed shuffle tree
+    const int l = threadIdx.x;
+    double s[3] = {0, 0, 0};
+    for (int b = l; b < nblocks; b += 32)
+        for (int q = 0; q < 3; ++q) s[q] += partial[size_t(b) * 3 + q];
+    for (int o = 16; o > 0; o >>= 1)
+        for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+    if (l == 0) {
+        out[0] = sqrt(s[0]);
+        out[1] = sqrt(s[1]);
+        out[2] = sqrt(s[2]);
+        out[3] = sqrt(s[0] + s[1] + s[2]);
+    }
+}
+
+// ------------------------------------------------------------------ fields
+enum InternalField {
+    F_U_ALT = GLIDE_N_PUBLIC_FIELDS, F_V_ALT, F_H_ALT,
+    F_W_U, F_W_V, F_W_H, F_CHI,
+    F_WL_U, F_WL_V, F_WL_H,
+    F_COUNT
+};
+
+enum Kind { KU = 0, KV = 1, KC = 2 };
+
+static Kind field_kind(int f) {
+    switch (f) {
+        case GLIDE_U: case GLIDE_F_U: case GLIDE_R_U: case GLIDE_LAMBDA_U: case GLIDE_ADJ_F_U:
+        case GLIDE_ADJ_R_U: case GLIDE_VJP_U: case GLIDE_FOP_U: case F_U_ALT: case F_W_U: case F_WL_U:
+            return KU;
+        case GLIDE_V: case GLIDE_F_V: case GLIDE_R_V: case GLIDE_LAMBDA_V: case GLIDE_ADJ_F_V:
+        case GLIDE_ADJ_R_V: case GLIDE_VJP_V: case GLIDE_FOP_V: case F_V_ALT: case F_W_V: case F_WL_V:
+            return KV;
+        default:
+            return KC;
+    }
+}
+
+static glide_phys default_phys() {
+    glide_phys p;
+    p.n = 3.0; p.eps_reg = 1e-6; p.flotation_reg_driving = 0.1; p.m = 1.0; p.u_reg = 1.0;
+    p.water_drag = 1e-5; p.flotation_reg_sliding = 0.1; p.calving_rate = 0.0;
+    p.flotation_reg_calving = 0.1; p.thklim = 0.1;
+    return p;
+}
+
+static glide_fas_config default_fas() {
+    glide_fas_config c;
+    c.freeze_coarse_calving = 1; c.freeze_coarse_phi = 1;
+    c.coarsest_steps = 200; c.pre_steps = 10; c.post_steps = 20; c.finest_steps = 50;
+    c.maximum_vcycles = 10; c.relative_tolerance = 1e-3; c.absolute_tolerance = 5.0;
+    return c;
+}
+
+static glide_vanka_config default_vanka() {
+    glide_vanka_config c;
+    c.omega = 0.5; c.newton_steps = 30; c.relaxation = 0.5; c.ssa_damping = 0.01;
+    c.mc_damping = 1.0; c.relax_phi = 0.0;
+    return c;
+}
+
+static int round_up(int a, int m) { return (a + m - 1) / m * m; }
+
+struct SolverBase {
+    virtual ~SolverBase() {}
+    int dtype = GLIDE_F64;
+    int n_levels = 0;
+    glide_fas_config fas[2];
+    int quirks = 1;
+    int use_graphs = 1;
+    unsigned version = 1;
+};
+
+template <class R>
+struct Level {
+    int ny = 0, nx = 0;
+    double dx = 0;
+    int pu = 0, pv = 0, pc = 0;
+    Arr<R> a[F_COUNT];
+    glide_phys phys;
+    glide_vanka_config vk[2];  // [0] forward, [1] adjoint
+    int blocks_x() const { return (nx + kTile - 1) / kTile; }
+    int blocks_y() const { return (ny + kTile - 1) / kTile; }
+};
+
+template <class R>
+struct Solver : SolverBase {
+    std::vector<Level<R>> lv;
+    char* arena = nullptr;
+    double* partial = nullptr;
+    double* norms_dev = nullptr;
+    double* norms_host = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    unsigned graph_version = 0;
+    double graph_dt = 0;
+    int graph_start = -1, graph_kind = -1;
+    cudaStream_t own_stream = nullptr;
+    long long launches = 0;        // kernels issued by this handle (graph replays included)
+    long long graph_launches = 0;  // kernels inside the captured graph
+
+    void counted(const char* what) {
+        check_launch(what);
+        ++launches;
+    }
+
+    Solver(int ny, int nx, double dx, int L) {
+        dtype = sizeof(R) == 8 ? GLIDE_F64 : GLIDE_F32;
+        n_levels = L;
+        fas[0] = default_fas();
+        fas[1] = default_fas();
+        lv.resize(L);
+        size_t bytes = 0;
+        const size_t align = 256;
+        for (int l = 0; l < L; ++l) {
+            Level<R>& v = lv[l];
+            v.ny = ny >> l;
+            v.nx = nx >> l;
+            v.dx = dx * double(1 << l);
+            v.pu = round_up(v.nx + 1, 32);
+            v.pv = round_up(v.nx, 32);
+            v.pc = round_up(v.nx, 32);
+            v.phys = default_phys();
+            v.vk[0] = default_vanka();
+            v.vk[1] = default_vanka();
+            for (int f = 0; f < F_COUNT; ++f) {
+                Kind k = field_kind(f);
+                int rows = k == KV ? v.ny + 1 : v.ny;
+                int cols = k == KU ? v.nx + 1 : v.nx;
+                int pitch = k == KU ? v.pu : (k == KV ? v.pv : v.pc);
+                v.a[f].rows = rows;
+                v.a[f].cols = cols;
+                v.a[f].pitch = pitch;
+                v.a[f].p = reinterpret_cast<R*>(bytes);  // offset for now
+                bytes += (size_t(rows) * pitch * sizeof(R) + align - 1) / align * align;
+            }
+        }
+        const int nblk = lv[0].blocks_x() * lv[0].blocks_y();
+        size_t partial_off = bytes;
+        bytes += (size_t(nblk) * 3 * sizeof(double) + align - 1) / align * align;
+        size_t norms_off = bytes;
+        bytes += align;
+        GCU(cudaMalloc(&arena, bytes));
+        GCU(cudaMemset(arena, 0, bytes));
+        for (auto& v : lv)
+            for (int f = 0; f < F_COUNT; ++f)
+                v.a[f].p = reinterpret_cast<R*>(arena + reinterpret_cast<size_t>(v.a[f].p));
+        partial = reinterpret_cast<double*>(arena + partial_off);
+        norms_dev = reinterpret_cast<double*>(arena + norms_off);
+        GCU(cudaMallocHost(&norms_host, 4 * sizeof(double)));
+        // gamma holds thklim between sweep groups
+        for (auto& v : lv) fill(v.a[GLIDE_GAMMA], R(v.phys.thklim), nullptr);
+        GCU(cudaDeviceSynchronize());
+    }
+
+    ~Solver() override {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (own_stream) cudaStreamDestroy(own_stream);
+        if (norms_host) cudaFreeHost(norms_host);
+        if (arena) cudaFree(arena);
+    }
+
+    // ---------------------------------------------------------- utilities
+    static dim3 pw_grid(int rows, int cols) { return dim3((cols + 255) / 256, rows); }
+
+    void fill(const Arr<R>& a, R val, cudaStream_t s) {
+        k_fill<R><<<pw_grid(a.rows, a.cols), 256, 0, s>>>(a, val, a.rows, a.cols);
+        counted("fill");
+    }
+
+    void copy(const Arr<R>& dst, const Arr<R>& src, cudaStream_t s) {
+        GCU(cudaMemcpy2DAsync(dst.p, size_t(dst.pitch) * sizeof(R), src.p, size_t(src.pitch) * sizeof(R),
+                              size_t(src.cols) * sizeof(R), src.rows, cudaMemcpyDeviceToDevice, s));
+    }
+
+    void restrict_field(int f, int l, cudaStream_t s, Arr<R> copy_to = Arr<R>()) {
+        Level<R>& F = lv[l];
+        Level<R>& C = lv[l + 1];
+        restrict_arr(F.a[f], C.a[f], f == GLIDE_MASK ? kCellMax : -1, l, s, copy_to);
+    }
+
+    void restrict_arr(const Arr<R>& fa, const Arr<R>& ca, int cell_kind, int l, cudaStream_t s,
+                      Arr<R> copy_to = Arr<R>()) {
+        Level<R>& C = lv[l + 1];
+        int kind;
+        if (fa.cols == lv[l].nx + 1) kind = kFaceU;
+        else if (fa.rows == lv[l].ny + 1) kind = kFaceV;
+        else kind = cell_kind >= 0 ? cell_kind : kCellAvg;
+        k_restrict<R><<<pw_grid(C.ny + 1, C.nx + 1), 256, 0, s>>>(fa, ca, copy_to, kind, C.ny, C.nx);
+        counted("restrict");
+    }
+
+    PhysR<R> physr(int l, double dt, bool freeze_calving) const {
+        const Level<R>& v = lv[l];
+        Phys p{v.phys.n, v.phys.eps_reg, v.phys.flotation_reg_driving, v.phys.m, v.phys.u_reg,
+               v.phys.water_drag, v.phys.flotation_reg_sliding, v.phys.calving_rate,
+               v.phys.flotation_reg_calving, v.phys.thklim};
+        return PhysR<R>(p, v.dx, dt, freeze_calving ? 0.0 : v.phys.calving_rate);
+    }
+
+    void compute_phi(int l, double relax, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_PHI], v.a[GLIDE_H], v.a[GLIDE_BED],
+                                                          R(v.phys.flotation_reg_driving), R(relax), v.ny, v.nx);
+        counted("grounded");
+    }
+
+    void set_rhs(int l, double dt, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        k_set_rhs<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_F_H], v.a[GLIDE_H_PREV], v.a[GLIDE_SMB],
+                                                         R(dt), v.ny, v.nx);
+        counted("set_rhs");
+    }
+
+    // residual into (o_*) = R(x) [- f] [- sub]; norms into norms_dev when asked
+    void residual(int l, double dt, bool use_forcing, bool use_mask, bool freeze_calving, bool freeze_phi,
+                  int out_u, int out_v, int out_H, const Arr<R>* sub, bool norms, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        if (!freeze_phi) compute_phi(l, 0.0, s);
+        ResidualArgs<R> a;
+        a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+        a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+        a.beta = v.a[GLIDE_BETA]; a.gamma = v.a[GLIDE_GAMMA];
+        a.f_u = v.a[GLIDE_F_U]; a.f_v = v.a[GLIDE_F_V]; a.f_H = v.a[GLIDE_F_H];
+        a.o_u = v.a[out_u]; a.o_v = v.a[out_v]; a.o_H = v.a[out_H];
+        if (sub) { a.s_u = sub[0]; a.s_v = sub[1]; a.s_H = sub[2]; }
+        a.partial = norms ? partial : nullptr;
+        a.p = physr(l, dt, freeze_calving);
+        a.ny = v.ny; a.nx = v.nx;
+        a.use_forcing = use_forcing; a.use_mask = use_mask;
+        dim3 g(v.blocks_x(), v.blocks_y());
+        k_residual<R><<<g, 256, 0, s>>>(a);
+        counted("residual");
+        if (norms) {
+            k_finish_norms<<<1, 32, 0, s>>>(partial, g.x * g.y, norms_dev);
+            counted("finish_norms");
+        }
+    }
+
+    void read_norms(double out[4], cudaStream_t s) {
+        GCU(cudaMemcpyAsync(norms_host, norms_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GCU(cudaStreamSynchronize(s));
+        for (int q = 0; q < 4; ++q) out[q] = norms_host[q];
+    }
+
+    // n additive-Vanka sweeps on level l, ending in the home state buffers
+    void sweeps(int l, double dt, int n, int gmode, bool freeze_calving, bool freeze_phi, int* iters,
+                cudaStream_t s) {
+        if (n <= 0) return;
+        Level<R>& v = lv[l];
+        const glide_vanka_config& c = v.vk[0];
+        const bool phi_live = !freeze_phi && c.relax_phi == 0.0;
+        const int start_alt = n & 1;
+        if (start_alt) {
+            copy(v.a[F_U_ALT], v.a[GLIDE_U], s);
+            copy(v.a[F_V_ALT], v.a[GLIDE_V], s);
+            copy(v.a[F_H_ALT], v.a[GLIDE_H], s);
+        }
+        SweepArgs<R> a;
+        a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+        a.beta = v.a[GLIDE_BETA];
+        a.f_u = v.a[GLIDE_F_U]; a.f_v = v.a[GLIDE_F_V]; a.f_H = v.a[GLIDE_F_H];
+        a.gamma = v.a[GLIDE_GAMMA];
+        a.wH = v.a[F_W_H]; a.chi = v.a[F_CHI];
+        a.chi_c = (l + 1 < n_levels) ? lv[l + 1].a[F_CHI] : Arr<R>();
+        a.p = physr(l, dt, freeze_calving);
+        a.omega = R(c.omega); a.ssa_damping = R(c.ssa_damping); a.mc_damping = R(c.mc_damping);
+        a.newton_steps = c.newton_steps;
+        a.ny = v.ny; a.nx = v.nx;
+        dim3 g(v.blocks_x(), v.blocks_y());
+        for (int k = 0; k < n; ++k) {
+            const bool in_alt = (start_alt ^ (k & 1)) != 0;
+            const int U0 = GLIDE_U, V0 = GLIDE_V, H0 = GLIDE_H, U1 = F_U_ALT, V1 = F_V_ALT, H1 = F_H_ALT;
+            const int iu = in_alt ? U1 : U0, iv = in_alt ? V1 : V0, ih = in_alt ? H1 : H0;
+            const int ou = in_alt ? U0 : U1, ov = in_alt ? V0 : V1, oh = in_alt ? H0 : H1;
+            a.u = v.a[iu]; a.v = v.a[iv]; a.H = v.a[ih];
+            a.uo = v.a[ou]; a.vo = v.a[ov]; a.Ho = v.a[oh];
+            a.iters = (k == n - 1) ? iters : nullptr;
+            if (!freeze_phi && !phi_live) {
+                k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_PHI], v.a[ih], v.a[GLIDE_BED],
+                                                                  R(v.phys.flotation_reg_driving), R(c.relax_phi),
+                                                                  v.ny, v.nx);
+                counted("grounded");
+            }
+            launch_sweep(a, gmode, phi_live, g, s);
+        }
+    }
+
+    void launch_sweep(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s) {
+#define GLIDE_SWEEP(GM, PL) k_vanka_sweep<R, GM, PL><<<g, kSweepThreads, 0, s>>>(a)
+        if (gmode == kGammaArray) { if (phi_live) GLIDE_SWEEP(kGammaArray, true); else GLIDE_SWEEP(kGammaArray, false); }
+        else if (gmode == kGammaWChi) { if (phi_live) GLIDE_SWEEP(kGammaWChi, true); else GLIDE_SWEEP(kGammaWChi, false); }
+        else { if (phi_live) GLIDE_SWEEP(kGammaWPhi, true); else GLIDE_SWEEP(kGammaWPhi, false); }
+#undef GLIDE_SWEEP
+        counted("vanka_sweep");
+    }
+
+    void correct(int l, int field, int wfield, int kind, int mode, cudaStream_t s) {
+        Level<R>& F = lv[l];
+        Level<R>& C = lv[l + 1];
+        CorrectArgs<R> a;
+        a.x = F.a[field]; a.w = F.a[wfield]; a.xc = C.a[field]; a.wc = C.a[wfield];
+        a.kind = kind; a.mode = mode; a.vquirk = quirks; a.nyf = F.ny; a.nxf = F.nx;
+        k_correct<R><<<pw_grid(F.ny + 1, F.nx + 1), 256, 0, s>>>(a);
+        counted("correct");
+    }
+
+    // ------------------------------------------------------ FASCD V-cycle
+    // glide/multigrid.py:536-645
+    void vcycle(int l, bool finest, double dt, cudaStream_t s) {
+        const glide_fas_config& c = fas[0];
+        const bool coarse = !finest;
+        const bool fcal = coarse && c.freeze_coarse_calving, fphi = coarse && c.freeze_coarse_phi;
+        Level<R>& v = lv[l];
+        if (finest) {
+            k_snapshot<R><<<pw_grid(v.ny + 1, v.nx + 1), 256, 0, s>>>(
+                v.a[GLIDE_U], v.a[GLIDE_V], v.a[GLIDE_H], v.a[F_W_U], v.a[F_W_V], v.a[F_W_H], v.a[F_CHI],
+                R(v.phys.thklim), v.ny, v.nx);
+            counted("snapshot");
+        }
+        if (l == n_levels - 1) {
+            sweeps(l, dt, c.coarsest_steps, kGammaWChi, fcal, fphi, nullptr, s);
+            return;
+        }
+        Level<R>& n = lv[l + 1];
+        restrict_arr(v.a[F_CHI], n.a[F_CHI], kCellMax, l, s);
+        sweeps(l, dt, c.pre_steps, kGammaWPhi, fcal, fphi, nullptr, s);
+        restrict_field(GLIDE_U, l, s, n.a[F_W_U]);
+        restrict_field(GLIDE_V, l, s, n.a[F_W_V]);
+        restrict_field(GLIDE_H, l, s, n.a[F_W_H]);
+        restrict_field(GLIDE_H_PREV, l, s);
+        restrict_field(GLIDE_PHI, l, s);
+        restrict_field(GLIDE_MASK, l, s);
+        residual(l, dt, true, false, fcal, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, false, s);
+        restrict_field(GLIDE_R_U, l, s);
+        restrict_field(GLIDE_R_V, l, s);
+        restrict_field(GLIDE_R_H, l, s);
+        const Arr<R> sub[3] = {n.a[GLIDE_R_U], n.a[GLIDE_R_V], n.a[GLIDE_R_H]};
+        residual(l + 1, dt, false, false, c.freeze_coarse_calving != 0, c.freeze_coarse_phi != 0, GLIDE_F_U,
+                 GLIDE_F_V, GLIDE_F_H, sub, false, s);
+        vcycle(l + 1, false, dt, s);
+        correct(l, GLIDE_U, F_W_U, kFaceU, 0, s);
+        correct(l, GLIDE_V, F_W_V, kFaceV, 0, s);
+        correct(l, GLIDE_H, F_W_H, kCellAvg, 0, s);
+        sweeps(l, dt, c.post_steps, kGammaWChi, fcal, fphi, nullptr, s);
+        if (finest) sweeps(l, dt, c.finest_steps, kGammaArray, false, false, nullptr, s);
+    }
+
+    void check_quirks() {
+        if (quirks)
+            for (int l = 0; l + 1 < n_levels; ++l)
+                if (lv[l].ny != lv[l].nx)
+                    fail(GLIDE_ERR_SHAPE, "reference-quirk v prolongation needs square levels (ny == nx)");
+    }
+
+    // Replay (or capture) one V-cycle followed by the convergence residual.
+    void cycle_and_check(int kind, int start, double dt, cudaStream_t s) {
+        auto body = [&]() {
+            if (kind == 0) {
+                vcycle(start, true, dt, s);
+                residual(start, dt, true, true, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
+            } else {
+                adj_vcycle(start, true, dt, s);
+                adj_residual(start, dt, true, s);
+            }
+        };
+        if (!use_graphs) {
+            body();
+            return;
+        }
+        // The legacy default stream cannot be captured.  A stream created with
+        // default (blocking) flags is ordered against it implicitly, so the
+        // graph runs there when the caller passed NULL.
+        if (s == nullptr) {
+            if (!own_stream) GCU(cudaStreamCreate(&own_stream));
+            s = own_stream;
+        }
+        if (!graph || graph_version != version || graph_dt != dt || graph_start != start || graph_kind != kind) {
+            if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+            cudaGraph_t g;
+            const long long before = launches;
+            GCU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                body();
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+                launches = before;
+                throw;
+            }
+            graph_launches = launches - before;
+            launches = before;
+            GCU(cudaStreamEndCapture(s, &g));
+            cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) fail(GLIDE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            graph_version = version; graph_dt = dt; graph_start = start; graph_kind = kind;
+        }
+        GCU(cudaGraphLaunch(graph, s));
+        launches += graph_launches;
+    }
+
+    void forward(double dt, int start, glide_stats* st, cudaStream_t s) {
+        check_level(start);
+        check_quirks();
+        set_rhs(start, dt, s);
+        residual(start, dt, true, true, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
+        double nr[4];
+        read_norms(nr, s);
+        solve_loop(0, start, dt, nr, st, s);
+    }
+
+    void solve_loop(int kind, int start, double dt, double nr[4], glide_stats* st, cudaStream_t s) {
+        const glide_fas_config& c = fas[kind];
+        const double r0 = nr[3];
+        if (!std::isfinite(r0)) fail(GLIDE_ERR_NONFINITE, "initial residual norm is not finite");
+        double rel = 1.0, ab = r0;
+        int it = 0;
+        if (st) {
+            std::memset(st, 0, sizeof(*st));
+            st->initial_norm = r0;
+            st->history[0] = r0;
+        }
+        while (rel > c.relative_tolerance && ab > c.absolute_tolerance && it < c.maximum_vcycles) {
+            cycle_and_check(kind, start, dt, s);
+            read_norms(nr, s);
+            ab = nr[3];
+            if (!std::isfinite(ab)) fail(GLIDE_ERR_NONFINITE, "residual norm became non-finite");
+            rel = ab / r0;
+            ++it;
+            if (st && it < GLIDE_MAX_HISTORY) st->history[it] = ab;
+        }
+        if (st) {
+            st->vcycles = it;
+            st->final_norm = ab;
+            for (int q = 0; q < 3; ++q) st->norms[q] = nr[q];
+        }
+    }
+
+    void check_level(int l) const {
+        if (l < 0 || l >= n_levels) fail(GLIDE_ERR_ARG, "level out of range");
+    }
+
+    // ------------------------------------------------------------ adjoint
+    // (kernels in adjoint_kernels.cuh)
+    void vjp_into(int l, double dt, bool use_forcing, int ou, int ov, int oh, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        VjpArgs<R> a;
+        a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+        a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+        a.beta = v.a[GLIDE_BETA];
+        a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
+        a.f_u = v.a[GLIDE_ADJ_F_U]; a.f_v = v.a[GLIDE_ADJ_F_V]; a.f_H = v.a[GLIDE_ADJ_F_H];
+        a.o_u = v.a[ou]; a.o_v = v.a[ov]; a.o_H = v.a[oh];
+        a.partial = nullptr;
+        a.p = physr(l, dt, false);
+        a.ny = v.ny; a.nx = v.nx; a.use_forcing = use_forcing;
+        launch_vjp(a, s);
+    }
+
+    void launch_vjp(VjpArgs<R>& a, cudaStream_t s) {
+        dim3 g((a.nx + kTile - 1) / kTile, (a.ny + kTile - 1) / kTile);
+        k_vjp<R><<<g, 256, 0, s>>>(a);
+        counted("vjp");
+        if (a.partial) {
+            k_finish_norms<<<1, 32, 0, s>>>(partial, g.x * g.y, norms_dev);
+            counted("finish_norms");
+        }
+    }
+
+    void adj_residual(int l, double dt, bool norms, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        VjpArgs<R> a;
+        a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+        a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+        a.beta = v.a[GLIDE_BETA];
+        a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
+        a.f_u = v.a[GLIDE_ADJ_F_U]; a.f_v = v.a[GLIDE_ADJ_F_V]; a.f_H = v.a[GLIDE_ADJ_F_H];
+        a.o_u = v.a[GLIDE_ADJ_R_U]; a.o_v = v.a[GLIDE_ADJ_R_V]; a.o_H = v.a[GLIDE_ADJ_R_H];
+        a.partial = norms ? partial : nullptr;
+        a.p = physr(l, dt, false);
+        a.ny = v.ny; a.nx = v.nx; a.use_forcing = 1;
+        launch_vjp(a, s);
+    }
+
+    void adj_sweeps(int l, double dt, int n, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        const glide_vanka_config& c = v.vk[1];
+        for (int k = 0; k < n; ++k) {
+            adj_residual(l, dt, false, s);
+            AdjSweepArgs<R> a;
+            a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+            a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+            a.beta = v.a[GLIDE_BETA];
+            a.ru = v.a[GLIDE_ADJ_R_U]; a.rv = v.a[GLIDE_ADJ_R_V]; a.rH = v.a[GLIDE_ADJ_R_H];
+            a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
+            a.p = physr(l, dt, false);
+            a.omega = R(c.omega); a.ssa_damping = R(c.ssa_damping); a.mc_damping = R(c.mc_damping);
+            a.ny = v.ny; a.nx = v.nx;
+            dim3 g(v.blocks_x(), v.blocks_y());
+            k_adjoint_sweep<R><<<g, kSweepThreads, 0, s>>>(a);
+            counted("adjoint_sweep");
+        }
+    }
+
+    // glide/multigrid.py:905-973
+    void adj_vcycle(int l, bool finest, double dt, cudaStream_t s) {
+        const glide_fas_config& c = fas[1];
+        if (l == n_levels - 1) {
+            adj_sweeps(l, dt, c.coarsest_steps, s);
+            return;
+        }
+        Level<R>& n = lv[l + 1];
+        adj_sweeps(l, dt, c.pre_steps, s);
+        restrict_field(GLIDE_U, l, s);
+        restrict_field(GLIDE_V, l, s);
+        restrict_field(GLIDE_H, l, s);
+        restrict_field(GLIDE_H_PREV, l, s);
+        restrict_field(GLIDE_PHI, l, s);
+        restrict_field(GLIDE_MASK, l, s);
+        restrict_field(GLIDE_LAMBDA_U, l, s, n.a[F_WL_U]);
+        restrict_field(GLIDE_LAMBDA_V, l, s, n.a[F_WL_V]);
+        restrict_field(GLIDE_LAMBDA_H, l, s, n.a[F_WL_H]);
+        adj_residual(l, dt, false, s);
+        restrict_field(GLIDE_ADJ_R_U, l, s);
+        restrict_field(GLIDE_ADJ_R_V, l, s);
+        restrict_field(GLIDE_ADJ_R_H, l, s);
+        // coarse right-hand side f_c = vjp_c - R r, in one pass
+        {
+            VjpArgs<R> a;
+            Level<R>& v = n;
+            a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+            a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+            a.beta = v.a[GLIDE_BETA];
+            a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
+            a.f_u = v.a[GLIDE_ADJ_F_U]; a.f_v = v.a[GLIDE_ADJ_F_V]; a.f_H = v.a[GLIDE_ADJ_F_H];
+            a.o_u = v.a[GLIDE_ADJ_F_U]; a.o_v = v.a[GLIDE_ADJ_F_V]; a.o_H = v.a[GLIDE_ADJ_F_H];
+            a.s_u = v.a[GLIDE_ADJ_R_U]; a.s_v = v.a[GLIDE_ADJ_R_V]; a.s_H = v.a[GLIDE_ADJ_R_H];
+            a.partial = nullptr;
+            a.p = physr(l + 1, dt, false);
+            a.ny = v.ny; a.nx = v.nx; a.use_forcing = 0;
+            launch_vjp(a, s);
+        }
+        adj_vcycle(l + 1, false, dt, s);
+        correct(l, GLIDE_LAMBDA_U, F_WL_U, kFaceU, 1, s);
+        correct(l, GLIDE_LAMBDA_V, F_WL_V, kFaceV, 1, s);
+        correct(l, GLIDE_LAMBDA_H, F_WL_H, kCellMax, 1, s);
+        adj_sweeps(l, dt, c.post_steps, s);
+        if (finest) adj_sweeps(l, dt, c.finest_steps, s);
+    }
+
+    void backward(double dt, int start, int grad_mask, glide_stats* st, cudaStream_t s) {
+        check_level(start);
+        check_quirks();
+        adj_residual(start, dt, true, s);
+        double nr[4];
+        read_norms(nr, s);
+        solve_loop(1, start, dt, nr, st, s);
+        gradients(start, dt, grad_mask, s);
+    }
+
+    void gradients(int l, double dt, int mask, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        GradArgs<R> a;
+        a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+        a.phi = v.a[GLIDE_PHI]; a.bed = v.a[GLIDE_BED]; a.beta = v.a[GLIDE_BETA];
+        a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
+        a.g_beta = (mask & GLIDE_GRAD_BETA_BIT) ? v.a[GLIDE_GRAD_BETA] : Arr<R>();
+        a.g_bed = (mask & GLIDE_GRAD_BED_BIT) ? v.a[GLIDE_GRAD_BED] : Arr<R>();
+        a.g_Hp = (mask & GLIDE_GRAD_H_PREV_BIT) ? v.a[GLIDE_GRAD_H_PREV] : Arr<R>();
+        a.g_smb = (mask & GLIDE_GRAD_SMB_BIT) ? v.a[GLIDE_GRAD_SMB] : Arr<R>();
+        a.p = physr(l, dt, false);
+        a.dt = R(dt);
+        a.ny = v.ny; a.nx = v.nx;
+        k_gradients<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(a);
+        counted("gradients");
+    }
+};
+
+}  // namespace glide
+
+// ====================================================================== C ABI
+using namespace glide;
+
+struct glide_solver {
+    std::unique_ptr<SolverBase> impl;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return GLIDE_OK;
+    } catch (const Fail& e) {
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return GLIDE_ERR_STATE;
+    }
+}
+
+template <class F>
+void dispatch(glide_handle h, F&& f) {
+    if (!h || !h->impl) fail(GLIDE_ERR_ARG, "null handle");
+    if (h->impl->dtype == GLIDE_F64) f(*static_cast<Solver<double>*>(h->impl.get()));
+    else f(*static_cast<Solver<float>*>(h->impl.get()));
+}
+
+cudaStream_t S(void* p) { return static_cast<cudaStream_t>(p); }
+
+template <class R>
+Arr<R>& field_arr(Solver<R>& s, int field, int level) {
+    s.check_level(level);
+    if (field < 0 || field >= GLIDE_N_PUBLIC_FIELDS) fail(GLIDE_ERR_ARG, "unknown field id");
+    return s.lv[level].a[field];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* glide_last_error(void) { return g_err.c_str(); }
+int glide_version(void) { return 1; }
+
+int glide_create(int ny, int nx, double dx, int n_levels, int dtype, glide_handle* out) {
+    return guarded([&] {
+        if (!out) fail(GLIDE_ERR_ARG, "out is null");
+        *out = nullptr;
+        if (ny <= 0 || nx <= 0 || n_levels <= 0 || !(dx > 0)) fail(GLIDE_ERR_ARG, "bad grid arguments");
+        if (n_levels > 16) fail(GLIDE_ERR_ARG, "too many levels");
+        const int d = 1 << (n_levels - 1);
+        if (ny % d || nx % d)
+            fail(GLIDE_ERR_SHAPE, "ny and nx must be divisible by 2^(n_levels-1)");
+        if ((ny >> (n_levels - 1)) < 2 || (nx >> (n_levels - 1)) < 2)
+            fail(GLIDE_ERR_SHAPE, "coarsest level must have at least 2x2 cells");
+        auto h = std::make_unique<glide_solver>();
+        if (dtype == GLIDE_F64) h->impl = std::make_unique<Solver<double>>(ny, nx, dx, n_levels);
+        else if (dtype == GLIDE_F32) h->impl = std::make_unique<Solver<float>>(ny, nx, dx, n_levels);
+        else fail(GLIDE_ERR_ARG, "dtype must be GLIDE_F64 or GLIDE_F32");
+        *out = h.release();
+    });
+}
+
+int glide_destroy(glide_handle h) {
+    return guarded([&] { delete h; });
+}
+
+int glide_level_shape(glide_handle h, int level, int* ny, int* nx, double* dx) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            if (ny) *ny = s.lv[level].ny;
+            if (nx) *nx = s.lv[level].nx;
+            if (dx) *dx = s.lv[level].dx;
+        });
+    });
+}
+
+int glide_field_ptr(glide_handle h, int field, int level, void** ptr, int* rows, int* cols, int* pitch) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            auto& a = field_arr(s, field, level);
+            if (ptr) *ptr = a.p;
+            if (rows) *rows = a.rows;
+            if (cols) *cols = a.cols;
+            if (pitch) *pitch = a.pitch;
+        });
+    });
+}
+
+int glide_set_field(glide_handle h, int field, int level, const void* src, int src_ld, int src_on_host,
+                    int restrict_down, void* stream) {
+    return guarded([&] {
+        if (!src) fail(GLIDE_ERR_ARG, "src is null");
+        dispatch(h, [&](auto& s) {
+            using R = std::remove_reference_t<decltype(*s.lv[0].a[0].p)>;
+            auto& a = field_arr(s, field, level);
+            const int ld = src_ld > 0 ? src_ld : a.cols;
+            if (ld < a.cols) fail(GLIDE_ERR_ARG, "src_ld smaller than the field's columns");
+            GCU(cudaMemcpy2DAsync(a.p, size_t(a.pitch) * sizeof(R), src, size_t(ld) * sizeof(R),
+                                  size_t(a.cols) * sizeof(R), a.rows,
+                                  src_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, S(stream)));
+            if (restrict_down)
+                for (int l = level; l + 1 < s.n_levels; ++l) s.restrict_field(field, l, S(stream));
+            if (src_on_host) GCU(cudaStreamSynchronize(S(stream)));
+        });
+    });
+}
+
+int glide_get_field(glide_handle h, int field, int level, void* dst, int dst_ld, int dst_on_host, void* stream) {
+    return guarded([&] {
+        if (!dst) fail(GLIDE_ERR_ARG, "dst is null");
+        dispatch(h, [&](auto& s) {
+            using R = std::remove_reference_t<decltype(*s.lv[0].a[0].p)>;
+            auto& a = field_arr(s, field, level);
+            const int ld = dst_ld > 0 ? dst_ld : a.cols;
+            if (ld < a.cols) fail(GLIDE_ERR_ARG, "dst_ld smaller than the field's columns");
+            GCU(cudaMemcpy2DAsync(dst, size_t(ld) * sizeof(R), a.p, size_t(a.pitch) * sizeof(R),
+                                  size_t(a.cols) * sizeof(R), a.rows,
+                                  dst_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, S(stream)));
+            if (dst_on_host) GCU(cudaStreamSynchronize(S(stream)));
+        });
+    });
+}
+
+int glide_fill_field(glide_handle h, int field, int level, double value, int restrict_down, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            using R = std::remove_reference_t<decltype(*s.lv[0].a[0].p)>;
+            auto& a = field_arr(s, field, level);
+            s.fill(a, R(value), S(stream));
+            if (restrict_down)
+                for (int l = level; l + 1 < s.n_levels; ++l) s.restrict_field(field, l, S(stream));
+        });
+    });
+}
+
+int glide_restrict_field(glide_handle h, int field, int level, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            field_arr(s, field, level);
+            for (int l = level; l + 1 < s.n_levels; ++l) s.restrict_field(field, l, S(stream));
+        });
+    });
+}
+
+int glide_set_phys(glide_handle h, int level, const glide_phys* p) {
+    return guarded([&] {
+        if (!p) fail(GLIDE_ERR_ARG, "null phys");
+        dispatch(h, [&](auto& s) {
+            using R = std::remove_reference_t<decltype(*s.lv[0].a[0].p)>;
+            for (int l = 0; l < s.n_levels; ++l) {
+                if (level >= 0 && l != level) continue;
+                const bool thk_changed = s.lv[l].phys.thklim != p->thklim;
+                s.lv[l].phys = *p;
+                if (thk_changed) s.fill(s.lv[l].a[GLIDE_GAMMA], R(p->thklim), nullptr);
+            }
+            if (level >= s.n_levels) fail(GLIDE_ERR_ARG, "level out of range");
+            ++s.version;
+            GCU(cudaDeviceSynchronize());
+        });
+    });
+}
+
+int glide_get_phys(glide_handle h, int level, glide_phys* p) {
+    return guarded([&] {
+        if (!p) fail(GLIDE_ERR_ARG, "null phys");
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            *p = s.lv[level].phys;
+        });
+    });
+}
+
+int glide_set_fas_config(glide_handle h, int adjoint, const glide_fas_config* c) {
+    return guarded([&] {
+        if (!c) fail(GLIDE_ERR_ARG, "null config");
+        dispatch(h, [&](auto& s) {
+            s.fas[adjoint ? 1 : 0] = *c;
+            ++s.version;
+        });
+    });
+}
+
+int glide_get_fas_config(glide_handle h, int adjoint, glide_fas_config* c) {
+    return guarded([&] {
+        if (!c) fail(GLIDE_ERR_ARG, "null config");
+        dispatch(h, [&](auto& s) { *c = s.fas[adjoint ? 1 : 0]; });
+    });
+}
+
+int glide_set_vanka_config(glide_handle h, int adjoint, int level, const glide_vanka_config* c) {
+    return guarded([&] {
+        if (!c) fail(GLIDE_ERR_ARG, "null config");
+        dispatch(h, [&](auto& s) {
+            if (level >= s.n_levels) fail(GLIDE_ERR_ARG, "level out of range");
+            for (int l = 0; l < s.n_levels; ++l)
+                if (level < 0 || l == level) s.lv[l].vk[adjoint ? 1 : 0] = *c;
+            ++s.version;
+        });
+    });
+}
+
+int glide_get_vanka_config(glide_handle h, int adjoint, int level, glide_vanka_config* c) {
+    return guarded([&] {
+        if (!c) fail(GLIDE_ERR_ARG, "null config");
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            *c = s.lv[level].vk[adjoint ? 1 : 0];
+        });
+    });
+}
+
+int glide_set_reference_quirks(glide_handle h, int on) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.quirks = on ? 1 : 0;
+            ++s.version;
+        });
+    });
+}
+
+int glide_set_use_graphs(glide_handle h, int use_graphs) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.use_graphs = use_graphs ? 1 : 0;
+            ++s.version;
+        });
+    });
+}
+
+int glide_set_rhs(glide_handle h, int level, double dt, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.set_rhs(level, dt, S(stream));
+        });
+    });
+}
+
+int glide_compute_phi(glide_handle h, int level, double relaxation, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.compute_phi(level, relaxation, S(stream));
+        });
+    });
+}
+
+int glide_residual(glide_handle h, int level, double dt, int flags, double* norms3, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            const bool op = flags & GLIDE_OPERATOR_ONLY;
+            s.residual(level, dt, !op, (flags & GLIDE_USE_MASK) != 0, (flags & GLIDE_FREEZE_CALVING) != 0,
+                       (flags & GLIDE_FREEZE_PHI) != 0, op ? GLIDE_FOP_U : GLIDE_R_U, op ? GLIDE_FOP_V : GLIDE_R_V,
+                       op ? GLIDE_FOP_H : GLIDE_R_H, nullptr, norms3 != nullptr, S(stream));
+            if (norms3) {
+                double nr[4];
+                s.read_norms(nr, S(stream));
+                for (int q = 0; q < 3; ++q) norms3[q] = nr[q];
+            }
+        });
+    });
+}
+
+int glide_vanka_sweep(glide_handle h, int level, double dt, int n, int flags, int* newton_iters, void* stream) {
+    return guarded([&] {
+        if (n < 0) fail(GLIDE_ERR_ARG, "negative sweep count");
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.sweeps(level, dt, n, kGammaArray, (flags & GLIDE_FREEZE_CALVING) != 0,
+                     (flags & GLIDE_FREEZE_PHI) != 0, newton_iters, S(stream));
+        });
+    });
+}
+
+int glide_forward(glide_handle h, double dt, int start_level, glide_stats* stats, void* stream) {
+    return guarded([&] { dispatch(h, [&](auto& s) { s.forward(dt, start_level, stats, S(stream)); }); });
+}
+
+int glide_adjoint_residual(glide_handle h, int level, double dt, double* norms3, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.adj_residual(level, dt, norms3 != nullptr, S(stream));
+            if (norms3) {
+                double nr[4];
+                s.read_norms(nr, S(stream));
+                for (int q = 0; q < 3; ++q) norms3[q] = nr[q];
+            }
+        });
+    });
+}
+
+int glide_vjp(glide_handle h, int level, double dt, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.vjp_into(level, dt, false, GLIDE_VJP_U, GLIDE_VJP_V, GLIDE_VJP_H, S(stream));
+        });
+    });
+}
+
+int glide_adjoint_sweep(glide_handle h, int level, double dt, int n, void* stream) {
+    return guarded([&] {
+        if (n < 0) fail(GLIDE_ERR_ARG, "negative sweep count");
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.adj_sweeps(level, dt, n, S(stream));
+        });
+    });
+}
+
+int glide_gradients(glide_handle h, int level, double dt, int grad_mask, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.gradients(level, dt, grad_mask, S(stream));
+        });
+    });
+}
+
+int glide_launch_count(glide_handle h, long long* count) {
+    return guarded([&] {
+        if (!count) fail(GLIDE_ERR_ARG, "null count");
+        dispatch(h, [&](auto& s) { *count = s.launches; });
+    });
+}
+
+int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, glide_stats* stats, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) { s.backward(dt, start_level, grad_mask, stats, S(stream)); });
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// transfer_kernels.cuh -- restriction, prolongation and the small pointwise
+// kernels of the V-cycle (glide/cuda/transfer.cu semantics; the elementwise
+// CuPy expressions of glide/multigrid.py fused into the transfers).
+#pragma once
+
+#include "glide_common.cuh"
+
+namespace glide {
+
+enum FieldKind { kFaceU = 0, kFaceV = 1, kCellAvg = 2, kCellMax = 3, kCellMin = 4 };
+
+// Restriction of one field (transfer.cu:2-139).  Coarse sizes (nyc, nxc).
+// Optional second output `copy` receives the same values (w_c = x_c).
+template <class R>
+__global__ void k_restrict(Arr<R> f, Arr<R> c, Arr<R> copy, int kind, int nyc, int nxc) {
+    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y;
+    R o;
+    if (kind == kFaceU) {
+        if (J >= nyc || I > nxc) return;
+        o = R(0.5) * (f.at(2 * J, 2 * I) + f.at(2 * J + 1, 2 * I));
+    } else if (kind == kFaceV) {
+        if (J > nyc || I >= nxc) return;
+        o = R(0.5) * (f.at(2 * J, 2 * I) + f.at(2 * J, 2 * I + 1));
+    } else {
+        if (J >= nyc || I >= nxc) return;
+        R a = f.at(2 * J, 2 * I), b = f.at(2 * J, 2 * I + 1);
+        R cc = f.at(2 * J + 1, 2 * I), d = f.at(2 * J + 1, 2 * I + 1);
+        if (kind == kCellAvg) o = R(0.25) * (a + b + cc + d);
+        else if (kind == kCellMax) o = fmax(fmax(a, b), fmax(cc, d));
+        else o = fmin(fmin(a, b), fmin(cc, d));
+    }
+    c.at(J, I) = o;
+    if (copy.p) copy.at(J, I) = o;
+}
+
+// Bilinear u-face value at fine (j, i) from coarse data addressed through
+// `get(J, I)` with coarse sizes (nyc, nxc+1) (transfer.cu:177-229).
+template <class R, class G>
+__device__ __forceinline__ R bilinear_u(const G& get, int j, int i, int nyc, int nxc) {
+    R Jf = (R(j) - R(0.5)) * R(0.5), If = R(i) * R(0.5);
+    Jf = fmax(R(0), fmin(Jf, R(nyc - 1)));
+    If = fmax(R(0), fmin(If, R(nxc)));
+    int Jlo = int(Jf), Ilo = int(If);
+    int Jhi = min(Jlo + 1, nyc - 1), Ihi = min(Ilo + 1, nxc);
+    R ty = Jf - R(Jlo), tx = If - R(Ilo);
+    R v00 = get(Jlo, Ilo), v01 = get(Jlo, Ihi), v10 = get(Jhi, Ilo), v11 = get(Jhi, Ihi);
+    return (R(1) - ty) * ((R(1) - tx) * v00 + tx * v01) + ty * ((R(1) - tx) * v10 + tx * v11);
+}
+
+// Bilinear v-face value (transfer.cu:270-323).
+template <class R, class G>
+__device__ __forceinline__ R bilinear_v(const G& get, int j, int i, int nyc, int nxc) {
+    R Jf = R(j) * R(0.5), If = (R(i) - R(0.5)) * R(0.5);
+    Jf = fmax(R(0), fmin(Jf, R(nyc)));
+    If = fmax(R(0), fmin(If, R(nxc - 1)));
+    int Jlo = int(Jf), Ilo = int(If);
+    int Jhi = min(Jlo + 1, nyc), Ihi = min(Ilo + 1, nxc - 1);
+    R ty = Jf - R(Jlo), tx = If - R(Ilo);
+    R v00 = get(Jlo, Ilo), v01 = get(Jlo, Ihi), v10 = get(Jhi, Ilo), v11 = get(Jhi, Ihi);
+    return (R(1) - ty) * ((R(1) - tx) * v00 + tx * v01) + ty * ((R(1) - tx) * v10 + tx * v11);
+}
+
+// Bilinear cell value (transfer.cu:348-395).
+template <class R, class G>
+__device__ __forceinline__ R bilinear_c(const G& get, int j, int i, int nyc, int nxc) {
+    R Jf = (R(j) - R(0.5)) * R(0.5), If = (R(i) - R(0.5)) * R(0.5);
+    Jf = fmax(R(0), fmin(Jf, R(nyc - 1)));
+    If = fmax(R(0), fmin(If, R(nxc - 1)));
+    int Jlo = int(Jf), Ilo = int(If);
+    int Jhi = min(Jlo + 1, nyc - 1), Ihi = min(Ilo + 1, nxc - 1);
+    R ty = Jf - R(Jlo), tx = If - R(Ilo);
+    R v00 = get(Jlo, Ilo), v01 = get(Jlo, Ihi), v10 = get(Jhi, Ilo), v11 = get(Jhi, Ihi);
+    return (R(1) - ty) * ((R(1) - tx) * v00 + tx * v01) + ty * ((R(1) - tx) * v10 + tx * v11);
+}
+
+// Coarse-grid correction of one field.  With z_c = xc - wc (computed on the
+// fly) and P the prolongation of this field:
+//   mode 0 (FAS forward, multigrid.py:616-632): x = w + (P z_c + (x - w))
+//   mode 1 (adjoint,     multigrid.py:958-967): x = x + P z_c
+// `kind`: kFaceU bilinear, kFaceV bilinear, kCellAvg = cell injection,
+// kCellMax = cell bilinear; `vquirk` prolongates v data with the u-face
+// formula on the v arrays' memory, as the reference does (multigrid.py:212-235).
+template <class R>
+struct CorrectArgs {
+    Arr<R> x, w, xc, wc;
+    int kind, mode, vquirk;
+    int nyf, nxf;  // fine cell counts
+};
+
+template <class R>
+__global__ void k_correct(CorrectArgs<R> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    const int nyc = a.nyf / 2, nxc = a.nxf / 2;
+    auto zc = [&](int J, int I) { return a.xc.at(J, I) - a.wc.at(J, I); };
+    R pz;
+    if (a.kind == kFaceU) {
+        if (j >= a.nyf || i > a.nxf) return;
+        pz = bilinear_u<R>(zc, j, i, nyc, nxc);
+    } else if (a.kind == kFaceV) {
+        if (j > a.nyf || i >= a.nxf) return;
+        if (a.vquirk) {
+            // fine flat index in v layout -> (jj, ii) in the u layout the
+            // reference's kernel assumes; coarse flat index back to v layout
+            const long flat = long(j) * a.nxf + i;
+            const int jj = int(flat / (a.nxf + 1)), ii = int(flat % (a.nxf + 1));
+            auto zq = [&](int J, int I) {
+                const long cf = long(J) * (nxc + 1) + I;
+                return zc(int(cf / nxc), int(cf % nxc));
+            };
+            pz = bilinear_u<R>(zq, jj, ii, nyc, nxc);
+        } else {
+            pz = bilinear_v<R>(zc, j, i, nyc, nxc);
+        }
+    } else {
+        if (j >= a.nyf || i >= a.nxf) return;
+        if (a.kind == kCellAvg) pz = zc(j >> 1, i >> 1);
+        else pz = bilinear_c<R>(zc, j, i, nyc, nxc);
+    }
+    R& x = a.x.at(j, i);
+    if (a.mode == 0) {
+        R w = a.w.at(j, i);
+        x = w + (pz + (x - w));
+    } else {
+        x = x + pz;
+    }
+}
+
+// Finest-level snapshot at the top of a V-cycle (multigrid.py:552-556):
+// w = x, chi = thklim - H.
+template <class R>
+__global__ void k_snapshot(Arr<R> u, Arr<R> v, Arr<R> H, Arr<R> wu, Arr<R> wv, Arr<R> wH, Arr<R> chi,
+                           R thklim, int ny, int nx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < ny && j <= nx) wu.at(i, j) = u.at(i, j);
+    if (i <= ny && j < nx) wv.at(i, j) = v.at(i, j);
+    if (i < ny && j < nx) {
+        R h = H.at(i, j);
+        wH.at(i, j) = h;
+        if (chi.p) chi.at(i, j) = thklim - h;
+    }
+}
+
+// f = H_prev / dt + smb (glide/operators.py:275-276)
+template <class R>
+__global__ void k_set_rhs(Arr<R> fH, Arr<R> Hp, Arr<R> smb, R dt, int ny, int nx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < ny && j < nx) fH.at(i, j) = Hp.at(i, j) / dt + smb.at(i, j);
+}
+
+// a = s * b + c over a pitched array (c may alias a)
+template <class R>
+__global__ void k_axpby(Arr<R> a, Arr<R> b, Arr<R> c, R s, int rows, int cols) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < rows && j < cols) a.at(i, j) = s * b.at(i, j) + (c.p ? c.at(i, j) : R(0));
+}
+
+template <class R>
+__global__ void k_fill(Arr<R> a, R val, int rows, int cols) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < rows && j < cols) a.at(i, j) = val;
+}
+
+}  // namespace glide

@@ -1,0 +1,159 @@
+/* glide_b200.h -- C ABI of the B200-native SSA momentum + mass-conservation
+ * solver (drop-in for the hot path of JacobDowns/glide).
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA device addresses;
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ * Every function returns GLIDE_OK (0) or an error code; glide_last_error()
+ * gives the message of the last failure on the calling thread.  A handle is
+ * not thread-safe: use one handle per host thread.
+ *
+ * Reference interfaces each entry point replaces (paths inside the
+ * JacobDowns/glide project):
+ *   glide_create / glide_destroy   glide/multigrid.py:8-52 Multigrid.__init__ (+ grid.py:147-233)
+ *   glide_field_ptr                Field.data of every level (glide/field.py:41-61, grid.py:235-350)
+ *   glide_set_field                HierarchyFieldManager.set (glide/multigrid.py:271-274)
+ *   glide_restrict_field           HierarchyFieldManager.restrict_down (glide/multigrid.py:276-280)
+ *   glide_get_field                reading Field.data / Field.grad
+ *   glide_set_phys / get_phys      Constant fields of Geometry/Rheology/Sliding/Calving (grid.py:8-145)
+ *   glide_set_fas_config           FASCDOptions.set / FASAdjointOptions.set (glide/multigrid.py:767-777, :1045-1049)
+ *   glide_set_vanka_config         VankaOptions / NewtonOptions .set / .set_level (glide/multigrid.py:780-852)
+ *   glide_set_rhs                  ForwardOperators.set_rhs (glide/operators.py:275-276)
+ *   glide_compute_phi              ForwardOperators.compute_phi (glide/operators.py:173-192)
+ *   glide_residual                 ForwardOperators.compute_residual (glide/operators.py:71-127)
+ *   glide_vanka_sweep              ForwardOperators.vanka_sweep (glide/operators.py:243-251)
+ *   glide_forward                  FASCDSolver.solve (glide/multigrid.py:502-533) as called by
+ *                                  IceDynamics.forward (glide/model.py:65-72)
+ *   glide_adjoint_residual         AdjointOperators.compute_residual (glide/operators.py:379-425)
+ *   glide_vjp                      AdjointOperators.compute_vjp (glide/operators.py:429-472)
+ *   glide_adjoint_sweep            AdjointOperators.vanka_sweep (glide/operators.py:517-524)
+ *   glide_gradients                AdjointOperators.compute_gradient_* (glide/operators.py:526-593)
+ *   glide_backward                 IceDynamics.backward (glide/model.py:74-94) with
+ *                                  FASAdjointSolver.solve (glide/multigrid.py:873-903)
+ */
+#ifndef GLIDE_B200_H
+#define GLIDE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GLIDE_OK 0
+#define GLIDE_ERR_ARG 1        /* bad argument (level, field, flag, null pointer) */
+#define GLIDE_ERR_SHAPE 2      /* grid size not divisible by 2^(levels-1), or unsupported shape */
+#define GLIDE_ERR_CUDA 3       /* a CUDA call failed */
+#define GLIDE_ERR_NONFINITE 4  /* residual norm became NaN or Inf */
+#define GLIDE_ERR_STATE 5      /* call not valid in the handle's current state */
+
+#define GLIDE_F64 0
+#define GLIDE_F32 1
+
+/* Field identifiers.  Face fields: U (ny, nx+1), V (ny+1, nx); all others are
+ * cell fields (ny, nx).  ADJ_* are the adjoint operators' arrays, GRAD_* the
+ * gradients written by glide_gradients / glide_backward, VJP_* the plain
+ * transpose product written by glide_vjp, FOP_* the operator without forcing
+ * written by glide_residual(GLIDE_OPERATOR_ONLY). */
+enum glide_field {
+    GLIDE_U = 0, GLIDE_V, GLIDE_H, GLIDE_H_PREV, GLIDE_PHI, GLIDE_MASK,
+    GLIDE_BED, GLIDE_B, GLIDE_BETA, GLIDE_SMB, GLIDE_GAMMA,
+    GLIDE_F_U, GLIDE_F_V, GLIDE_F_H,
+    GLIDE_R_U, GLIDE_R_V, GLIDE_R_H,
+    GLIDE_LAMBDA_U, GLIDE_LAMBDA_V, GLIDE_LAMBDA_H,
+    GLIDE_ADJ_F_U, GLIDE_ADJ_F_V, GLIDE_ADJ_F_H,
+    GLIDE_ADJ_R_U, GLIDE_ADJ_R_V, GLIDE_ADJ_R_H,
+    GLIDE_GRAD_BETA, GLIDE_GRAD_BED, GLIDE_GRAD_H_PREV, GLIDE_GRAD_SMB,
+    GLIDE_VJP_U, GLIDE_VJP_V, GLIDE_VJP_H,
+    GLIDE_FOP_U, GLIDE_FOP_V, GLIDE_FOP_H,
+    GLIDE_N_PUBLIC_FIELDS
+};
+
+/* Flags of glide_residual / glide_vanka_sweep. */
+#define GLIDE_USE_MASK 1
+#define GLIDE_OPERATOR_ONLY 2
+#define GLIDE_FREEZE_CALVING 4
+#define GLIDE_FREEZE_PHI 8
+
+/* Gradient selection of glide_gradients / glide_backward. */
+#define GLIDE_GRAD_BETA_BIT 1
+#define GLIDE_GRAD_BED_BIT 2
+#define GLIDE_GRAD_H_PREV_BIT 4
+#define GLIDE_GRAD_SMB_BIT 8
+
+typedef struct glide_solver* glide_handle;
+
+/* Physical constants of a level (defaults of glide/grid.py). */
+typedef struct {
+    double n, eps_reg, flotation_reg_driving, m, u_reg, water_drag,
+        flotation_reg_sliding, calving_rate, flotation_reg_calving, thklim;
+} glide_phys;
+
+/* FASCD / FASAdjoint schedule (glide/multigrid.py:672-682, :993-1001). */
+typedef struct {
+    int freeze_coarse_calving, freeze_coarse_phi;
+    int coarsest_steps, pre_steps, post_steps, finest_steps, maximum_vcycles;
+    double relative_tolerance, absolute_tolerance;
+} glide_fas_config;
+
+/* Vanka smoother + local Newton (glide/operators.py:314-327).  `relaxation`
+ * is stored but, as in the reference kernel, the local Newton uses 0.5. */
+typedef struct {
+    double omega;
+    int newton_steps;
+    double relaxation, ssa_damping, mc_damping, relax_phi;
+} glide_vanka_config;
+
+#define GLIDE_MAX_HISTORY 256
+typedef struct {
+    int vcycles;                     /* V-cycles run */
+    double initial_norm, final_norm; /* sqrt(|r_u|^2+|r_v|^2+|r_H|^2) */
+    double norms[3];                 /* final |r_u|, |r_v|, |r_H| */
+    double history[GLIDE_MAX_HISTORY];
+} glide_stats;
+
+const char* glide_last_error(void);
+int glide_version(void);
+
+int glide_create(int ny, int nx, double dx, int n_levels, int dtype, glide_handle* out);
+int glide_destroy(glide_handle h);
+int glide_level_shape(glide_handle h, int level, int* ny, int* nx, double* dx);
+int glide_field_ptr(glide_handle h, int field, int level, void** ptr, int* rows, int* cols,
+                    int* pitch_elems);
+int glide_set_field(glide_handle h, int field, int level, const void* src, int src_ld,
+                    int src_on_host, int restrict_down, void* stream);
+int glide_get_field(glide_handle h, int field, int level, void* dst, int dst_ld, int dst_on_host,
+                    void* stream);
+int glide_fill_field(glide_handle h, int field, int level, double value, int restrict_down,
+                     void* stream);
+int glide_restrict_field(glide_handle h, int field, int level, void* stream);
+int glide_set_phys(glide_handle h, int level, const glide_phys* p);
+int glide_get_phys(glide_handle h, int level, glide_phys* p);
+int glide_set_fas_config(glide_handle h, int adjoint, const glide_fas_config* c);
+int glide_get_fas_config(glide_handle h, int adjoint, glide_fas_config* c);
+int glide_set_vanka_config(glide_handle h, int adjoint, int level, const glide_vanka_config* c);
+int glide_get_vanka_config(glide_handle h, int adjoint, int level, glide_vanka_config* c);
+/* on = 1 reproduces the reference's v-face prolongation (its u-face kernel
+ * run on v arrays, glide/multigrid.py:212-235; square grids only). */
+int glide_set_reference_quirks(glide_handle h, int on);
+/* use_graphs = 1 replays each V-cycle as a captured CUDA graph. */
+int glide_set_use_graphs(glide_handle h, int use_graphs);
+/* Number of kernels this handle has launched so far (graph replays count
+ * every kernel node).  No counterpart in the reference: instrumentation. */
+int glide_launch_count(glide_handle h, long long* count);
+
+int glide_set_rhs(glide_handle h, int level, double dt, void* stream);
+int glide_compute_phi(glide_handle h, int level, double relaxation, void* stream);
+int glide_residual(glide_handle h, int level, double dt, int flags, double* norms3, void* stream);
+int glide_vanka_sweep(glide_handle h, int level, double dt, int n, int flags, int* newton_iters,
+                      void* stream);
+int glide_forward(glide_handle h, double dt, int start_level, glide_stats* stats, void* stream);
+
+int glide_adjoint_residual(glide_handle h, int level, double dt, double* norms3, void* stream);
+int glide_vjp(glide_handle h, int level, double dt, void* stream);
+int glide_adjoint_sweep(glide_handle h, int level, double dt, int n, void* stream);
+int glide_gradients(glide_handle h, int level, double dt, int grad_mask, void* stream);
+int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, glide_stats* stats,
+                   void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLIDE_B200_H */

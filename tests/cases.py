@@ -1,0 +1,79 @@
+"""Seeded synthetic inputs with the shapes and value ranges of the workloads
+(no datasets exist here; these stand in for them).
+
+* `slab_c1`   -- 64x64, dx = 1 km, 4 levels, dt = 10 a: tilted bed with a
+                 500 m sinusoidal bump, uniform 1000 m ice, A = 1e-16, beta
+                 1000 + 500 sin(2 pi x / 64 km) (ISMIP-HOM-like slab).
+* `dome`      -- radius-R Vialov-style dome, H = 3000 (1 - (r/R)^(4/3))^(3/8)
+                 floored at 0.1 m, Gaussian random bed (spectral slope -3,
+                 std 400 m, mean 200 m), log-normal beta smoothed over 10 km,
+                 smb = 0.5 - 2e-3 (s - 1500), A = 1e-16.
+All parameters are in the reference's "head units": B and beta divided by
+rho_i g with rho_i = 910 kg m^-3, g = 9.81 m s^-2.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RHO_I = 910.0
+G = 9.81
+
+
+def slab_c1(ny=64, nx=64, dx=1000.0):
+    x = (np.arange(nx) + 0.5) * dx
+    y = (np.arange(ny) + 0.5) * dx
+    X, Y = np.meshgrid(x, y)
+    L = 64e3
+    bed = -X * np.tan(np.deg2rad(0.5)) + 500.0 * np.sin(2 * np.pi * X / L) * np.sin(2 * np.pi * Y / L)
+    H = np.full((ny, nx), 1000.0)
+    B = np.full((ny, nx), (1e-16 ** (-1.0 / 3.0)) / (RHO_I * G))
+    beta = (1000.0 + 500.0 * np.sin(2 * np.pi * X / L)) / (RHO_I * G)
+    smb = np.full((ny, nx), 0.3)
+    return dict(bed=bed, H=H, H_prev=H.copy(), B=B, beta=beta, smb=smb)
+
+
+def _smooth(field, sigma_cells):
+    """Gaussian smoothing by FFT (periodic), width in cells."""
+    ny, nx = field.shape
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.fftfreq(nx)[None, :]
+    g = np.exp(-2 * (np.pi * sigma_cells) ** 2 * (kx ** 2 + ky ** 2))
+    return np.fft.ifft2(np.fft.fft2(field) * g).real
+
+
+def dome(n=512, dx=1500.0, R=600e3, seed=0, lapse=2e-3):
+    rng = np.random.default_rng(seed)
+    c = (np.arange(n) + 0.5) * dx - n * dx / 2
+    X, Y = np.meshgrid(c, c)
+    r = np.sqrt(X ** 2 + Y ** 2)
+    H = 3000.0 * np.clip(1.0 - (r / R) ** (4.0 / 3.0), 0.0, None) ** (3.0 / 8.0)
+    H = np.maximum(H, 0.1)
+    k = np.sqrt(np.fft.fftfreq(n)[:, None] ** 2 + np.fft.fftfreq(n)[None, :] ** 2)
+    k[0, 0] = 1.0
+    w = np.fft.ifft2(np.fft.fft2(rng.standard_normal((n, n))) * k ** (-1.5)).real
+    bed = 200.0 + 400.0 * (w - w.mean()) / w.std()
+    beta = np.exp(rng.normal(np.log(2000.0), 0.8, (n, n)))
+    beta = _smooth(beta, 10e3 / dx) / (RHO_I * G)
+    s = np.maximum(bed + H, (1.0 - 0.917) * H)
+    smb = 0.5 - lapse * (s - 1500.0)
+    B = np.full((n, n), (1e-16 ** (-1.0 / 3.0)) / (RHO_I * G))
+    return dict(bed=bed, H=H, H_prev=H.copy(), B=B, beta=beta, smb=smb)
+
+
+def random_state(ny, nx, seed=1, thin_frac=0.2):
+    """A rough state exercising every branch: random velocities, thickness
+    with thin-ice patches at the floor, mixed grounding, random mask."""
+    rng = np.random.default_rng(seed)
+    u = rng.normal(0, 50, (ny, nx + 1))
+    v = rng.normal(0, 50, (ny + 1, nx))
+    H = rng.uniform(50, 1500, (ny, nx))
+    H[rng.random((ny, nx)) < thin_frac] = 0.1
+    bed = rng.normal(-200, 400, (ny, nx))
+    B = np.full((ny, nx), (1e-16 ** (-1.0 / 3.0)) / (RHO_I * G)) * rng.uniform(0.8, 1.2, (ny, nx))
+    beta = rng.uniform(0.05, 0.5, (ny, nx))
+    smb = rng.normal(0.3, 0.5, (ny, nx))
+    mask = (rng.random((ny, nx)) < 0.15).astype(float)
+    f_u = rng.normal(0, 1e-2, (ny, nx + 1))
+    f_v = rng.normal(0, 1e-2, (ny + 1, nx))
+    H_prev = H * rng.uniform(0.95, 1.05, (ny, nx))
+    return dict(u=u, v=v, H=H, H_prev=H_prev, bed=bed, B=B, beta=beta, smb=smb, mask=mask, f_u=f_u, f_v=f_v)

@@ -1,0 +1,163 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference package (JacobDowns/glide, read from its checkout) on host
+cores through oracle/refpy.py: the reference's own Python sequencing, option
+objects and CUDA kernel sources, the kernels executed by the host fiber
+emulator.  binary64 fixtures use the binary64 build of the same sources; one
+binary32 fixture uses the kernels as written.
+
+    python tests/golden/make_golden.py [--reference DIR]
+
+Each .npz stores the inputs it was made from and the reference's outputs.
+"""
+from __future__ import annotations
+
+import argparse
+import contextlib
+import io
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(HERE.parent))
+
+from cases import random_state, slab_c1  # noqa: E402
+from oracle.refpy import load_reference  # noqa: E402
+
+
+def quiet():
+    return contextlib.redirect_stdout(io.StringIO())
+
+
+def c1_forward_and_adjoint(glide, tag):
+    from glide.model import IceDynamics
+    f = slab_c1()
+    with quiet():
+        model = IceDynamics(n_levels=4, ny=64, nx=64, dx=1000.0)
+    mg = model.mg
+    for k in ("bed", "B", "beta", "smb"):
+        getattr({"bed": mg.geometry, "B": mg.rheology, "beta": mg.sliding, "smb": mg.forcing}[k], k).set(f[k])
+    mg.state.H.set(f["H"])
+    mg.state.H_prev.set(f["H_prev"])
+    s = model.forward_solver
+    s.fas_options.set(maximum_vcycles=3, relative_tolerance=0.0, absolute_tolerance=0.0, report_norms=False)
+    with quiet():
+        model.forward(0.0, 10.0, update_geometry=False)
+    lv = mg.levels[0]
+    out = {f"in_{k}": np.asarray(v) for k, v in f.items()}
+    for k in ("u", "v", "H", "mask", "phi"):
+        out[f"out_{k}"] = np.array(getattr(lv.state, k).data, dtype=np.float64)
+    np.savez_compressed(HERE / f"c1_forward_{tag}.npz", **out)
+    if tag != "f64":
+        return
+    u, v = np.array(lv.state.u.data), np.array(lv.state.v.data)
+    dJdu = u - 1.1 * u
+    dJdv = v - 0.9 * v
+    a = model.adjoint_solver
+    a.fas_options.set(maximum_vcycles=2, relative_tolerance=0.0, absolute_tolerance=0.0, report_norms=False)
+    with quiet():
+        model.backward(0.0, 10.0, dJdu=dJdu, dJdv=dJdv)
+    adj = dict(out)
+    adj["in_dJdu"], adj["in_dJdv"] = dJdu, dJdv
+    for k in ("lambda_u", "lambda_v", "lambda_H"):
+        adj[f"out_{k}"] = np.array(getattr(lv.adjoint, k).data)
+    adj["out_grad_beta"] = np.array(lv.sliding.beta.grad)
+    adj["out_grad_bed"] = np.array(lv.geometry.bed.grad)
+    adj["out_grad_H_prev"] = np.array(lv.state.H_prev.grad)
+    adj["out_grad_smb"] = np.array(lv.forcing.smb.grad)
+    np.savez_compressed(HERE / "c1_adjoint_f64.npz", **adj)
+
+
+def random_grid(glide, st, calving=0.0):
+    from glide.grid import Grid
+    ny, nx = st["H"].shape
+    g = Grid(ny, nx, 1500.0)
+    for k in ("u", "v", "H", "H_prev", "mask"):
+        getattr(g.state, k).set(st[k])
+    g.geometry.bed.set(st["bed"])
+    g.rheology.B.set(st["B"])
+    g.sliding.beta.set(st["beta"])
+    g.forcing.smb.set(st["smb"])
+    g.calving.calving_rate.set(calving)
+    g.forward_operators.f_u[:, :] = st["f_u"]
+    g.forward_operators.f_v[:, :] = st["f_v"]
+    return g
+
+
+def random_cases(glide):
+    st = random_state(40, 56, seed=7)
+    dt = 5.0
+    out = {f"in_{k}": v for k, v in st.items()}
+    for tag, calving in (("", 0.0), ("_calving", 2.0)):
+        g = random_grid(glide, st, calving)
+        ops = g.forward_operators
+        ops.set_rhs(dt)
+        ops.compute_residual(dt, use_mask=True)
+        for k in ("r_u", "r_v", "r_H"):
+            out[f"out_{k}{tag}"] = np.array(getattr(ops, k))
+        out[f"out_phi{tag}"] = np.array(g.state.phi.data)
+        ops.compute_residual(dt, use_mask=False, operator_only=True, freeze_phi=True)
+        for k in ("F_u", "F_v", "F_H"):
+            out[f"out_{k}{tag}"] = np.array(getattr(ops, k))
+    np.savez_compressed(HERE / "random_residual_f64.npz", **out)
+
+    out = {f"in_{k}": v for k, v in st.items()}
+    g = random_grid(glide, st)
+    ops = g.forward_operators
+    ops.set_rhs(dt)
+    ops.vanka_sweep(dt, 3)
+    for k in ("u", "v", "H", "mask", "phi"):
+        out[f"out_{k}"] = np.array(getattr(g.state, k).data)
+    np.savez_compressed(HERE / "random_vanka_f64.npz", **out)
+
+    rng = np.random.default_rng(11)
+    ny, nx = st["H"].shape
+    lam = dict(lambda_u=rng.normal(0, 1, (ny, nx + 1)), lambda_v=rng.normal(0, 1, (ny + 1, nx)),
+               lambda_H=rng.normal(0, 1, (ny, nx)))
+    af = dict(adj_f_u=rng.normal(0, 1, (ny, nx + 1)), adj_f_v=rng.normal(0, 1, (ny + 1, nx)),
+              adj_f_H=rng.normal(0, 1, (ny, nx)))
+    out = {f"in_{k}": v for k, v in {**st, **lam, **af}.items()}
+    g = random_grid(glide, st)
+    g.forward_operators.compute_phi()
+    for k, v in lam.items():
+        getattr(g.adjoint, k).set(v)
+    aops = g.adjoint_operators
+    aops.f_u[:, :] = af["adj_f_u"]
+    aops.f_v[:, :] = af["adj_f_v"]
+    aops.f_H[:, :] = af["adj_f_H"]
+    aops.compute_vjp(dt)
+    for k in ("vjp_u", "vjp_v", "vjp_H"):
+        out[f"out_{k}"] = np.array(getattr(aops, k))
+    aops.compute_residual(dt)
+    for k in ("r_u", "r_v", "r_H"):
+        out[f"out_adj_{k}"] = np.array(getattr(aops, k))
+    aops.vanka_sweep(dt, 2)
+    for k in ("lambda_u", "lambda_v", "lambda_H"):
+        out[f"out_sweep_{k}"] = np.array(getattr(g.adjoint, k).data)
+    aops.compute_gradient_beta()
+    aops.compute_gradient_bed()
+    out["out_grad_beta"] = np.array(g.sliding.beta.grad)
+    out["out_grad_bed"] = np.array(g.geometry.bed.grad)
+    out["out_phi"] = np.array(g.state.phi.data)
+    np.savez_compressed(HERE / "random_adjoint_f64.npz", **out)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args(argv)
+    glide = load_reference(fp64=True, reference=a.reference)
+    c1_forward_and_adjoint(glide, "f64")
+    random_cases(glide)
+    glide32 = load_reference(fp64=False, reference=a.reference)
+    c1_forward_and_adjoint(glide32, "f32")
+    for p in sorted(HERE.glob("*.npz")):
+        print(p.name, p.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

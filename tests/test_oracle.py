@@ -1,0 +1,145 @@
+"""Pin the CPU oracle (oracle/glide_oracle.*) against the golden fixtures
+produced by the reference itself (tests/golden/make_golden.py), and -- where
+the reference checkout is present -- against the reference run live."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from util import load_golden, oracle_c1, oracle_single_level, rel_err
+
+DT_RANDOM = 5.0
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    from oracle import build_oracle
+    build_oracle.build_oracle()
+
+
+def test_c1_forward_matches_reference_f64():
+    g = load_golden("c1_forward_f64")
+    o = oracle_c1(g)
+    o.fas.maximum_vcycles = 3
+    o.fas.relative_tolerance = 0.0
+    o.fas.absolute_tolerance = 0.0
+    assert o.solve(10.0) == 3
+    lev = o.levels[0]
+    for k in ("u", "v", "H", "mask", "phi"):
+        assert rel_err(getattr(lev, k), g[f"out_{k}"]) <= 1e-13, k
+
+
+def test_c1_forward_matches_reference_f32():
+    g = load_golden("c1_forward_f32")
+    o = oracle_c1(g, dtype=np.float32)
+    o.fas.maximum_vcycles = 3
+    o.fas.relative_tolerance = 0.0
+    o.fas.absolute_tolerance = 0.0
+    o.solve(10.0)
+    lev = o.levels[0]
+    for k in ("u", "v", "H"):
+        assert rel_err(getattr(lev, k), g[f"out_{k}"]) <= 1e-5, k
+
+
+def test_c1_adjoint_matches_reference_f64():
+    g = load_golden("c1_adjoint_f64")
+    o = oracle_c1(g)
+    o.fas.maximum_vcycles = 3
+    o.fas.relative_tolerance = 0.0
+    o.fas.absolute_tolerance = 0.0
+    o.solve(10.0)
+    o.adj.maximum_vcycles = 2
+    o.adj.relative_tolerance = 0.0
+    o.adj.absolute_tolerance = 0.0
+    grads = o.backward(10.0, dJdu=g["in_dJdu"], dJdv=g["in_dJdv"])
+    lev = o.levels[0]
+    assert rel_err(lev.l_u, g["out_lambda_u"]) <= 1e-12
+    assert rel_err(lev.l_v, g["out_lambda_v"]) <= 1e-12
+    assert rel_err(lev.l_H, g["out_lambda_H"]) <= 1e-12
+    for k in ("beta", "bed", "H_prev", "smb"):
+        assert rel_err(grads[k], g[f"out_grad_{k}"]) <= 1e-12, k
+
+
+@pytest.mark.parametrize("tag,calving", [("", 0.0), ("_calving", 2.0)])
+def test_random_residual_matches_reference(tag, calving):
+    g = load_golden("random_residual_f64")
+    o = oracle_single_level(g, 1500.0, calving=calving)
+    lev = o.levels[0]
+    lev.f_H[...] = lev.H_prev / DT_RANDOM + lev.smb
+    lev.residual(DT_RANDOM, use_mask=True)
+    for k in ("r_u", "r_v", "r_H", "phi"):
+        assert rel_err(getattr(lev, k), g[f"out_{k}{tag}"]) <= 1e-13, k
+    lev.residual(DT_RANDOM, use_mask=False, operator_only=True, freeze_phi=True)
+    for k in ("F_u", "F_v", "F_H"):
+        assert rel_err(getattr(lev, k), g[f"out_{k}{tag}"]) <= 1e-13, k
+
+
+def test_random_vanka_matches_reference():
+    g = load_golden("random_vanka_f64")
+    o = oracle_single_level(g, 1500.0)
+    lev = o.levels[0]
+    lev.f_H[...] = lev.H_prev / DT_RANDOM + lev.smb
+    lev.vanka_sweep(DT_RANDOM, 3)
+    for k in ("u", "v", "H", "mask", "phi"):
+        assert rel_err(getattr(lev, k), g[f"out_{k}"]) <= 1e-12, k
+
+
+def test_random_adjoint_matches_reference():
+    g = load_golden("random_adjoint_f64")
+    o = oracle_single_level(g, 1500.0)
+    lev = o.levels[0]
+    lev.compute_phi()
+    lev.l_u[...], lev.l_v[...], lev.l_H[...] = g["in_lambda_u"], g["in_lambda_v"], g["in_lambda_H"]
+    lev.af_u[...], lev.af_v[...], lev.af_H[...] = g["in_adj_f_u"], g["in_adj_f_v"], g["in_adj_f_H"]
+    lev.adj_vjp(DT_RANDOM)
+    for k in ("vjp_u", "vjp_v", "vjp_H"):
+        assert rel_err(getattr(lev, k), g[f"out_{k}"]) <= 1e-12, k
+    lev.adj_residual(DT_RANDOM)
+    assert rel_err(lev.ar_u, g["out_adj_r_u"]) <= 1e-12
+    assert rel_err(lev.ar_v, g["out_adj_r_v"]) <= 1e-12
+    assert rel_err(lev.ar_H, g["out_adj_r_H"]) <= 1e-12
+    lev.adj_sweep(DT_RANDOM, 2)
+    assert rel_err(lev.l_u, g["out_sweep_lambda_u"]) <= 1e-12
+    assert rel_err(lev.l_v, g["out_sweep_lambda_v"]) <= 1e-12
+    assert rel_err(lev.l_H, g["out_sweep_lambda_H"]) <= 1e-12
+    lev.gradients()
+    assert rel_err(lev.g_beta, g["out_grad_beta"]) <= 1e-12
+    assert rel_err(lev.g_bed, g["out_grad_bed"]) <= 1e-12
+
+
+REF = os.environ.get("GLIDE_REFERENCE", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "glide", "cuda")),
+                    reason="reference checkout not present")
+def test_oracle_matches_live_reference_on_new_seed():
+    """Fresh random state (seed not used by the fixtures), reference run live."""
+    import contextlib
+    import io
+
+    from cases import random_state
+    from oracle import build_oracle
+    from oracle.refpy import load_reference
+    build_oracle.build_reference(REF)
+    load_reference(fp64=True, reference=REF)
+    from glide.grid import Grid
+    st = random_state(24, 30, seed=123)
+    with contextlib.redirect_stdout(io.StringIO()):
+        gr = Grid(24, 30, 900.0)
+    for k in ("u", "v", "H", "H_prev", "mask"):
+        getattr(gr.state, k).set(st[k])
+    gr.geometry.bed.set(st["bed"]); gr.rheology.B.set(st["B"])
+    gr.sliding.beta.set(st["beta"]); gr.forcing.smb.set(st["smb"])
+    gr.forward_operators.f_u[:, :] = st["f_u"]
+    gr.forward_operators.f_v[:, :] = st["f_v"]
+    gr.forward_operators.set_rhs(2.0)
+    gr.forward_operators.vanka_sweep(2.0, 2)
+    inp = {f"in_{k}": v for k, v in st.items()}
+    o = oracle_single_level(inp, 900.0)
+    lev = o.levels[0]
+    lev.f_H[...] = lev.H_prev / 2.0 + lev.smb
+    lev.vanka_sweep(2.0, 2)
+    for k in ("u", "v", "H", "mask"):
+        assert rel_err(getattr(lev, k), np.array(getattr(gr.state, k).data)) <= 1e-12, k
