@@ -49,7 +49,31 @@ def parse():
     ap.add_argument("--max-vcycles", type=int, default=40)
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="step", choices=["step", "sweeps"],
+                    help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
+    ap.add_argument("--sweeps", type=int, default=3)
     return ap.parse_args()
+
+
+def run_sweeps(a):
+    """Profiling case: the workload's finest level and N fused Vanka sweeps."""
+    import torch
+
+    from cases import dome
+    from glide_b200.hierarchy import Hierarchy
+    dtype = torch.float64 if a.precision == "fp64" else torch.float32
+    f = dome(a.size, a.dx, a.radius, seed=0)
+    h = Hierarchy(a.size, a.size, a.dx, 1, dtype=dtype)
+    for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+        h.set(k, 0, torch.as_tensor(f[k]))
+    h.set_rhs(0, a.dt)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    h.vanka_sweep(0, a.dt, a.sweeps)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "sweeps", "size": a.size, "sweeps": a.sweeps,
+                      "ms_per_sweep": e0.elapsed_time(e1) / a.sweeps}), flush=True)
 
 
 # ------------------------------------------------------------------ clocks
@@ -365,6 +389,9 @@ def main():
         return 0
     import torch
     import torch.distributed as dist
+    if a.mode == "sweeps":
+        run_sweeps(a)
+        return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     res, sweeps_per_step = run_ours(a, rank, world)
