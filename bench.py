@@ -52,7 +52,32 @@ def parse():
     ap.add_argument("--mode", default="step", choices=["step", "sweeps"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
+    ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
+    ap.add_argument("--sweep-blocks", type=int, default=2, help="Vanka sweep blocks per SM (1 or 2)")
+    ap.add_argument("--schedule", default=None,
+                    help="pre,post,finest,coarsest sweeps of the FASCD V-cycle (default: the reference's 10,20,50,200)")
+    ap.add_argument("--omega", type=float, default=None, help="Vanka omega (default 0.5)")
+    ap.add_argument("--relax", type=float, default=None, help="local Newton step length (native mode only)")
+    ap.add_argument("--native", action="store_true",
+                    help="native mode: corrected v prolongation and the configured Newton relaxation")
+    ap.add_argument("--quick", action="store_true", help="time the solve only (no e2e, roofline, CPU leg)")
     return ap.parse_args()
+
+
+def apply_solver_options(h, a):
+    h.set_tuning(sweep_blocks_per_sm=a.sweep_blocks)
+    if a.native:
+        h.set_reference_quirks(False)
+    if a.schedule:
+        pre, post, fin, coarse = (int(x) for x in a.schedule.split(","))
+        h.set_fas(False, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
+    kw = {}
+    if a.omega is not None:
+        kw["omega"] = a.omega
+    if a.relax is not None:
+        kw["relaxation"] = a.relax
+    if kw:
+        h.set_vanka(False, -1, **kw)
 
 
 def run_sweeps(a):
@@ -63,17 +88,25 @@ def run_sweeps(a):
     from glide_b200.hierarchy import Hierarchy
     dtype = torch.float64 if a.precision == "fp64" else torch.float32
     f = dome(a.size, a.dx, a.radius, seed=0)
-    h = Hierarchy(a.size, a.size, a.dx, 1, dtype=dtype)
+    levels = a.levels if a.presolve > 0 else 1
+    h = Hierarchy(a.size, a.size, a.dx, levels, dtype=dtype)
+    h.set_tuning(sweep_blocks_per_sm=a.sweep_blocks)
     for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
-        h.set(k, 0, torch.as_tensor(f[k]))
+        h.set(k, 0, torch.as_tensor(f[k]), restrict_down=True)
+    if a.presolve > 0:  # move to the near-converged regime of later V-cycles
+        h.set_fas(False, maximum_vcycles=a.presolve, relative_tolerance=0.0, absolute_tolerance=0.0)
+        h.forward(a.dt, 0)
     h.set_rhs(0, a.dt)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    h.vanka_sweep(0, a.dt, a.sweeps)
-    e1.record()
-    torch.cuda.synchronize()
-    print(json.dumps({"mode": "sweeps", "size": a.size, "sweeps": a.sweeps,
-                      "ms_per_sweep": e0.elapsed_time(e1) / a.sweeps}), flush=True)
+    out = {"mode": "sweeps", "size": a.size, "presolve_vcycles": a.presolve,
+           "sweep_blocks_per_sm": a.sweep_blocks}
+    for label, n in (("first", 1), ("next", a.sweeps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h.vanka_sweep(0, a.dt, n)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"ms_per_sweep_{label}"] = e0.elapsed_time(e1) / n
+    print(json.dumps(out), flush=True)
 
 
 # ------------------------------------------------------------------ clocks
@@ -169,6 +202,8 @@ def run_ours(a, rank, world):
     for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
         h.set(k, 0, torch.as_tensor(f[k]), restrict_down=True)
     h.set_fas(False, maximum_vcycles=a.max_vcycles, relative_tolerance=a.rtol, absolute_tolerance=0.0)
+    apply_solver_options(h, a)
+    fas = h.get_fas(False)
     stream = torch.cuda.current_stream()
 
     def step():
@@ -209,6 +244,9 @@ def run_ours(a, rank, world):
     ms = float(t.item())
     vcyc = float(np.mean([s["vcycles"] for s in stats]))
     final_rel = float(np.max([s["final_norm"] / s["initial_norm"] for s in stats]))
+    if a.quick:  # schedule exploration: the solve only
+        return {"ms_per_step": ms, "vcycles_per_step": vcyc, "final_relative_residual": final_rel,
+                "schedule": a.schedule, "omega": a.omega, "relax": a.relax, "native": a.native}, None
 
     # dominant kernel: the fused fine-level Vanka sweep, timed alone
     n_sw = 20
@@ -286,7 +324,11 @@ def run_ours(a, rank, world):
                      "algorithmic_bytes_per_launch": bytes_per_sweep},
         "clocks": clocks,
     }
-    return res, sweeps_per_vcycle(a.levels) * vcyc
+    res["config"]["schedule"] = {k: fas[k] for k in ("pre_steps", "post_steps", "finest_steps", "coarsest_steps")}
+    res["config"]["reference_quirks"] = not a.native
+    spv = sweeps_per_vcycle(a.levels, fas["pre_steps"], fas["post_steps"], fas["finest_steps"],
+                            fas["coarsest_steps"])
+    return res, spv * vcyc
 
 
 # -------------------------------------------------------------- CPU legs
@@ -395,7 +437,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     res, sweeps_per_step = run_ours(a, rank, world)
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and not a.quick:
         res["cpu_baseline"] = cpu_oracle_sample(a, sweeps_per_step, a.cpu_seconds)
     if world > 1:
         dist.barrier()

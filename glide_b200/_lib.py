@@ -109,6 +109,7 @@ SIGNATURES = {
     "glide_set_reference_quirks": ([_H, _I], _I),
     "glide_set_use_graphs": ([_H, _I], _I),
     "glide_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], _I),
+    "glide_set_tuning": ([_H, _I, _I], _I),
     "glide_set_rhs": ([_H, _I, _D, _P], _I),
     "glide_compute_phi": ([_H, _I, _D, _P], _I),
     "glide_residual": ([_H, _I, _D, _I, ctypes.POINTER(_D), _P], _I),

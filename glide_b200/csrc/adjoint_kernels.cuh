@@ -40,7 +40,7 @@ __device__ __forceinline__ R eta_dot_at(const S& s, R Bc, const PhysR<R>& p, int
     R dshear = R(0.25) * (R(2) * e1 * d1 + R(2) * e2 * d2 + R(2) * e3 * d3 + R(2) * e4 * d4);
     R eII = ux * ux + vy * vy + ux * vy + shear + p.eps_reg;
     R deII = R(2) * ux * dux + R(2) * vy * dvy + (ux * dvy + dux * vy) + dshear;
-    return R(0.5) * Bc * p.gexp * pow(eII, p.gexp - R(1)) * deII;
+    return R(0.5) * Bc * p.gexp * glen_pow_m1(eII, p) * deII;
 }
 
 // Staged tile for the transpose: forward state, lambda and eta / eta-dot.
@@ -85,7 +85,7 @@ __device__ __forceinline__ CellSrc<R> cell_src(const S& s, const PhysR<R>& p, in
     CellSrc<R> o;
     R Hc = s.Hc(i, j), phc = s.PHI(i, j), dc;
     R lam = s.LHm(i, j);
-    R h = lam / p.dt;
+    R h = lam * p.dti;
     FluxT<R> f = lflux(s.U(i, j), s.Hc(i, j - 1), Hc, j, nx);
     h += -lam * f.d_H1 * dxi; o.Hl = -lam * f.d_H0 * dxi; o.Ul = -lam * f.d_w * dxi;
     calve(Hc, phc, s.PHI(i, j - 1), p.calving_rate, dc); h += lam * dc * dxi;

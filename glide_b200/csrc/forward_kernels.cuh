@@ -143,14 +143,18 @@ struct SweepArgs {
     int* iters;                  // optional: Newton iterations per cell (pitch = phi.pitch)
     PhysR<R> p;
     R omega, ssa_damping, mc_damping;
+    R relax;                     // local Newton step length (the reference fixes 0.5)
     int newton_steps;
     int ny, nx;
 };
 
 constexpr int kSweepThreads = kTile * kTile + 2 * kTile;
 
-template <class R, int GMODE, bool PHI_LIVE>
-__global__ void __launch_bounds__(kSweepThreads) k_vanka_sweep(SweepArgs<R> a) {
+// MINB = resident blocks per SM the register allocation is fitted to: 1
+// keeps every value in registers, 2 doubles the warps that hide the FP64
+// dependency latency at the price of some spills; the runtime picks one.
+template <class R, int GMODE, bool PHI_LIVE, int MINB>
+__global__ void __launch_bounds__(kSweepThreads, MINB) k_vanka_sweep(SweepArgs<R> a) {
     using TileT = Tile<R, kTile, 2, 1>;
     constexpr int NC = TileT::NC;     // 19
     constexpr int ND = kTile + 1;     // deltas for rows/cols [i0-1, i0+16)
@@ -182,22 +186,22 @@ __global__ void __launch_bounds__(kSweepThreads) k_vanka_sweep(SweepArgs<R> a) {
     R dd[4] = {0, 0, 0, 0};
     if (live) {
         R x[5] = {s.U(i, j), s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.Hc(i, j)};
-        const R x0[5] = {x[0], x[1], x[2], x[3], x[4]};
         R thk;
         if (GMODE == kGammaArray) thk = a.gamma.at(i, j);
         else if (GMODE == kGammaWChi) thk = a.wH.at(i, j) + a.chi.at(i, j);
         else thk = a.wH.at(i, j) + (-a.chi_c.at(i >> 1, j >> 1) + a.chi.at(i, j));
         masked = tid < kTile * kTile ? a.mask.at(i, j) : R(0);  // halo cells never write it
-        const R fu0 = a.f_u.at(i, j), fu1 = a.f_u.at(i, j + 1);
-        const R fv0 = a.f_v.at(i, j), fv1 = a.f_v.at(i + 1, j), fh = a.f_H.at(i, j);
         R comp[5] = {0, 0, 0, 0, 0};
         R rnorm = 1;
         int k = 0;
         const R tol = R(kNewtonTol);
         while (k < a.newton_steps && rnorm > tol) {
-            R J[25], r[5], dx[5];
+            R J[25], r[5];
             local_system<R>(s, a.p, i, j, x, J, r);
-            r[0] -= fu0; r[1] -= fu1; r[2] -= fv0; r[3] -= fv1; r[4] -= fh;
+            // forcing is re-read each iteration (L1 hits) to keep registers free
+            r[0] -= ldg(&a.f_u.at(i, j)); r[1] -= ldg(&a.f_u.at(i, j + 1));
+            r[2] -= ldg(&a.f_v.at(i, j)); r[3] -= ldg(&a.f_v.at(i + 1, j));
+            r[4] -= ldg(&a.f_H.at(i, j));
             J[0] -= a.ssa_damping; J[6] -= a.ssa_damping; J[12] -= a.ssa_damping; J[18] -= a.ssa_damping;
             J[24] += a.mc_damping;
             if (j == 0) { pin(J, 0); r[0] = x[0]; }
@@ -211,11 +215,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_vanka_sweep(SweepArgs<R> a) {
             } else {
                 masked = R(0);
             }
-            lu5_solve(J, r, dx);
+            // squared norm of the pre-update local residual (vanka.cu:613)
             rnorm = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3] + r[4] * r[4];
+            lu5_solve(J, r, r);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {  // compensated update with the fixed relaxation 0.5
-                R y = -R(0.5) * dx[q] - comp[q];
+            for (int q = 0; q < 5; ++q) {  // compensated (Kahan) update, vanka.cu:617-640
+                R y = -a.relax * r[q] - comp[q];
                 R tq = x[q] + y;
                 comp[q] = (tq - x[q]) - y;
                 x[q] = tq;
@@ -224,9 +229,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_vanka_sweep(SweepArgs<R> a) {
             ++k;
         }
         if (a.iters && tid < kTile * kTile) a.iters[size_t(i) * a.phi.pitch + j] = k;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dd[q] = R(0.5) * (x[q] - x0[q]);
-        dH = x[4] - x0[4];
+        dd[0] = R(0.5) * (x[0] - s.U(i, j));
+        dd[1] = R(0.5) * (x[1] - s.U(i, j + 1));
+        dd[2] = R(0.5) * (x[2] - s.V(i, j));
+        dd[3] = R(0.5) * (x[3] - s.V(i + 1, j));
+        dH = x[4] - s.Hc(i, j);
     }
     {
         const int di = i - (i0 - 1), dj = j - (j0 - 1);

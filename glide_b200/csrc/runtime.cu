@@ -119,6 +119,8 @@ struct SolverBase {
     int quirks = 1;
     int use_graphs = 1;
     unsigned version = 1;
+    // Vanka sweep register budget: resident blocks per SM (1 or 2)
+    int sweep_blocks_per_sm = 2;
 };
 
 template <class R>
@@ -314,6 +316,8 @@ struct Solver : SolverBase {
         a.chi_c = (l + 1 < n_levels) ? lv[l + 1].a[F_CHI] : Arr<R>();
         a.p = physr(l, dt, freeze_calving);
         a.omega = R(c.omega); a.ssa_damping = R(c.ssa_damping); a.mc_damping = R(c.mc_damping);
+        // reference mode: the kernel's fixed 0.5 (vanka.cu:615); otherwise the configured value
+        a.relax = quirks ? R(0.5) : R(c.relaxation);
         a.newton_steps = c.newton_steps;
         a.ny = v.ny; a.nx = v.nx;
         dim3 g(v.blocks_x(), v.blocks_y());
@@ -335,12 +339,18 @@ struct Solver : SolverBase {
         }
     }
 
-    void launch_sweep(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s) {
-#define GLIDE_SWEEP(GM, PL) k_vanka_sweep<R, GM, PL><<<g, kSweepThreads, 0, s>>>(a)
+    template <int MINB>
+    void launch_sweep_occ(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s) {
+#define GLIDE_SWEEP(GM, PL) k_vanka_sweep<R, GM, PL, MINB><<<g, kSweepThreads, 0, s>>>(a)
         if (gmode == kGammaArray) { if (phi_live) GLIDE_SWEEP(kGammaArray, true); else GLIDE_SWEEP(kGammaArray, false); }
         else if (gmode == kGammaWChi) { if (phi_live) GLIDE_SWEEP(kGammaWChi, true); else GLIDE_SWEEP(kGammaWChi, false); }
         else { if (phi_live) GLIDE_SWEEP(kGammaWPhi, true); else GLIDE_SWEEP(kGammaWPhi, false); }
 #undef GLIDE_SWEEP
+    }
+
+    void launch_sweep(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s) {
+        if (sweep_blocks_per_sm >= 2) launch_sweep_occ<2>(a, gmode, phi_live, g, s);
+        else launch_sweep_occ<1>(a, gmode, phi_live, g, s);
         counted("vanka_sweep");
     }
 
@@ -846,6 +856,20 @@ int glide_set_reference_quirks(glide_handle h, int on) {
     return guarded([&] {
         dispatch(h, [&](auto& s) {
             s.quirks = on ? 1 : 0;
+            ++s.version;
+        });
+    });
+}
+
+int glide_set_tuning(glide_handle h, int key, int value) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            if (key == GLIDE_TUNE_SWEEP_BLOCKS_PER_SM) {
+                if (value < 1 || value > 2) fail(GLIDE_ERR_ARG, "sweep blocks per SM must be 1 or 2");
+                s.sweep_blocks_per_sm = value;
+            } else {
+                fail(GLIDE_ERR_ARG, "unknown tuning key");
+            }
             ++s.version;
         });
     });

@@ -16,14 +16,38 @@ namespace glide {
 
 template <class R>
 struct PhysR {
-    R n, eps_reg, m, u_reg, water_drag, calving_rate, dx, dxi, dt, gexp, c_ground;
+    R n, eps_reg, m, u_reg, water_drag, calving_rate, dx, dxi, dt, dti, gexp, c_ground;
+    int glen3;  // n == 3: the viscosity power is a reciprocal cube root
     __device__ PhysR() {}
     __host__ __device__ PhysR(const Phys& p, double dx_, double dt_, double calving)
         : n(R(p.n)), eps_reg(R(p.eps_reg)), m(R(p.m)), u_reg(R(p.u_reg)),
           water_drag(R(p.water_drag)), calving_rate(R(calving)), dx(R(dx_)),
-          dxi(R(1) / R(dx_)), dt(R(dt_)), gexp((R(1) - R(p.n)) / (R(2) * R(p.n))),
-          c_ground(R(p.fr_driving)) {}
+          dxi(R(1) / R(dx_)), dt(R(dt_)), dti(R(1) / R(dt_)), gexp((R(1) - R(p.n)) / (R(2) * R(p.n))),
+          c_ground(R(p.fr_driving)), glen3(p.n == 3.0) {}
 };
+
+__device__ __forceinline__ double rcbrt_r(double x) { return rcbrt(x); }
+__device__ __forceinline__ float rcbrt_r(float x) { return rcbrtf(x); }
+__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+
+// x^((1-n)/(2n)); for Glen's n = 3 that is x^(-1/3), evaluated as a
+// reciprocal cube root (a few ulp from pow, an order of magnitude cheaper).
+template <class R>
+__device__ __forceinline__ R glen_pow(R x, const PhysR<R>& p) {
+    return p.glen3 ? rcbrt_r(x) : pow(x, p.gexp);
+}
+
+// x^((1-n)/(2n) - 1), the exponent of the viscosity's derivative.
+template <class R>
+__device__ __forceinline__ R glen_pow_m1(R x, const PhysR<R>& p) {
+    if (p.glen3) {
+        R r = rcbrt_r(x);
+        R r2 = r * r;
+        return r2 * r2;
+    }
+    return pow(x, p.gexp - R(1));
+}
 
 // Glen's-law cell viscosity from staged velocities; corner shear rates on
 // the domain edge are masked with the raw indices (viscosity.cu:119-168).
@@ -41,7 +65,7 @@ __device__ __forceinline__ R eta_at(const S& s, R Bc, const PhysR<R>& p, int i, 
     R e_br = R(0.5) * ((ur - s.U(i + 1, j + 1)) * dxi + (s.V(i + 1, j + 1) - vb) * dxi) * m_br;
     R shear = R(0.25) * (e_tl * e_tl + e_tr * e_tr + e_bl * e_bl + e_br * e_br);
     R eII = ux * ux + vy * vy + ux * vy + shear + p.eps_reg;
-    return R(0.5) * Bc * pow(eII, p.gexp);
+    return R(0.5) * Bc * glen_pow(eII, p);
 }
 
 // sigmoid grounding flag (common.cu:66-82)
@@ -159,8 +183,10 @@ __device__ __forceinline__ FluxT<R> lflux(R w, R H0, R H1, int k, int nk) {
     FluxT<R> o{0, 0, 0, 0};
     if (k <= 0 || k >= nk) return o;
     R Hm = R(0.5) * (H0 + H1);
-    R a = sqrt(w * w + R(10));
-    R sg = w / a;
+    const R q2 = w * w + R(10);
+    const R ra = rsqrt_r(q2);
+    R a = q2 * ra;   // sqrt(w^2 + 10)
+    R sg = w * ra;   // w / sqrt(w^2 + 10)
     o.q = Hm * w - R(0.5) * a * (H1 - H0);
     o.d_H0 = R(0.5) * (w + a);
     o.d_H1 = R(0.5) * (w - a);
@@ -183,7 +209,7 @@ __device__ __forceinline__ R mass_residual(const S& s, const PhysR<R>& p, int i,
     const int ny = s.ny, nx = s.nx;
     const R dxi = p.dxi;
     R Hc = s.Hc(i, j), phc = s.PHI(i, j), dum;
-    R r = Hc / p.dt;
+    R r = Hc * p.dti;
     r -= fH;
     r -= lflux(s.U(i, j), s.Hc(i, j - 1), Hc, j, nx).q * dxi;
     r += calve(Hc, phc, s.PHI(i, j - 1), p.calving_rate, dum) * dxi;
@@ -267,8 +293,8 @@ __device__ __forceinline__ void local_system(const S& s, const PhysR<R>& p, int 
     const R Hl = s.Hc(i, j - 1), Hr = s.Hc(i, j + 1), Ht = s.Hc(i - 1, j), Hb = s.Hc(i + 1, j);
     {
         R dc, c;
-        J[24] = R(1) / p.dt;
-        r[4] += Hc / p.dt;
+        J[24] = p.dti;
+        r[4] += Hc * p.dti;
         FluxT<R> f = lflux(ul, Hl, Hc, j, nx);
         J[20] -= f.d_w * dxi; J[24] -= f.d_H1 * dxi; r[4] -= f.q * dxi;
         c = calve(Hc, phc, phl, p.calving_rate, dc); J[24] += dc * dxi; r[4] += c * dxi;
@@ -364,16 +390,20 @@ __device__ __forceinline__ void pin(R* J, int k) {
     J[k * 5 + k] = R(1);
 }
 
-// In-place Doolittle LU without pivoting and the two triangular solves, in
-// the operation order of the reference (vanka.cu:5-48).  J is destroyed.
+// In-place Doolittle LU without pivoting and the two triangular solves (the
+// factorisation order of vanka.cu:5-48).  The pivot reciprocals computed by
+// the factorisation are reused by the back substitution, so one reciprocal
+// per pivot replaces the reference's extra divisions.  J is destroyed; b may
+// alias x.
 template <class R>
 __device__ __forceinline__ void lu5_solve(R* J, const R* b, R* x) {
+    R inv[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-        R inv = R(1) / J[k * 5 + k];
+        inv[k] = R(1) / J[k * 5 + k];
 #pragma unroll
         for (int a = k + 1; a < 5; ++a) {
-            J[a * 5 + k] *= inv;
+            J[a * 5 + k] *= inv[k];
 #pragma unroll
             for (int c = k + 1; c < 5; ++c) J[a * 5 + c] -= J[a * 5 + k] * J[k * 5 + c];
         }
@@ -383,11 +413,12 @@ __device__ __forceinline__ void lu5_solve(R* J, const R* b, R* x) {
     R y2 = b[2] - J[10] * y0 - J[11] * y1;
     R y3 = b[3] - J[15] * y0 - J[16] * y1 - J[17] * y2;
     R y4 = b[4] - J[20] * y0 - J[21] * y1 - J[22] * y2 - J[23] * y3;
-    x[4] = y4 / J[24];
-    x[3] = (y3 - J[19] * x[4]) / J[18];
-    x[2] = (y2 - J[13] * x[3] - J[14] * x[4]) / J[12];
-    x[1] = (y1 - J[7] * x[2] - J[8] * x[3] - J[9] * x[4]) / J[6];
-    x[0] = (y0 - J[1] * x[1] - J[2] * x[2] - J[3] * x[3] - J[4] * x[4]) / J[0];
+    R x4 = y4 * inv[4];
+    R x3 = (y3 - J[19] * x4) * inv[3];
+    R x2 = (y2 - J[13] * x3 - J[14] * x4) * inv[2];
+    R x1 = (y1 - J[7] * x2 - J[8] * x3 - J[9] * x4) * inv[1];
+    R x0 = (y0 - J[1] * x1 - J[2] * x2 - J[3] * x3 - J[4] * x4) * inv[0];
+    x[0] = x0; x[1] = x1; x[2] = x2; x[3] = x3; x[4] = x4;
 }
 
 }  // namespace glide

@@ -155,6 +155,10 @@ class Hierarchy:
     def set_use_graphs(self, on: bool):
         call("glide_set_use_graphs", self._h, int(bool(on)))
 
+    def set_tuning(self, sweep_blocks_per_sm: int | None = None):
+        if sweep_blocks_per_sm is not None:
+            call("glide_set_tuning", self._h, 1, int(sweep_blocks_per_sm))
+
     def launch_count(self) -> int:
         c = ctypes.c_longlong()
         call("glide_launch_count", self._h, ctypes.byref(c))

@@ -138,6 +138,10 @@ int glide_set_use_graphs(glide_handle h, int use_graphs);
 /* Number of kernels this handle has launched so far (graph replays count
  * every kernel node).  No counterpart in the reference: instrumentation. */
 int glide_launch_count(glide_handle h, long long* count);
+/* Kernel tuning knobs (no counterpart in the reference).
+ * GLIDE_TUNE_SWEEP_BLOCKS_PER_SM: 1 or 2 resident Vanka-sweep blocks per SM. */
+#define GLIDE_TUNE_SWEEP_BLOCKS_PER_SM 1
+int glide_set_tuning(glide_handle h, int key, int value);
 
 int glide_set_rhs(glide_handle h, int level, double dt, void* stream);
 int glide_compute_phi(glide_handle h, int level, double relaxation, void* stream);
