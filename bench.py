@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--dx", type=float, default=750.0)
     ap.add_argument("--radius", type=float, default=1200e3)
     ap.add_argument("--dt", type=float, default=5.0)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"])
+    ap.add_argument("--inner", type=int, default=None, help="mixed: binary32 V-cycles per defect correction")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--max-vcycles", type=int, default=40)
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
@@ -61,6 +62,12 @@ def parse():
     ap.add_argument("--native", action="store_true",
                     help="native mode: corrected v prolongation and the configured Newton relaxation")
     ap.add_argument("--quick", action="store_true", help="time the solve only (no e2e, roofline, CPU leg)")
+    ap.add_argument("--method", default=None, choices=["fascd", "newton"],
+                    help="forward solve: FASCD V-cycles, or FASCD then Newton with the tangent multigrid")
+    ap.add_argument("--switch", type=int, default=None, help="newton: switch at rel. residual 10^-k")
+    ap.add_argument("--tangent-vcycles", type=int, default=None)
+    ap.add_argument("--tangent-schedule", default=None, help="pre,post,finest,coarsest of the tangent multigrid")
+    ap.add_argument("--tangent-omega", type=float, default=None)
     return ap.parse_args()
 
 
@@ -78,6 +85,12 @@ def apply_solver_options(h, a):
         kw["relaxation"] = a.relax
     if kw:
         h.set_vanka(False, -1, **kw)
+    h.set_tuning(forward_method=a.method, newton_switch_exp10=a.switch, tangent_vcycles=a.tangent_vcycles)
+    if a.tangent_schedule:
+        pre, post, fin, coarse = (int(x) for x in a.tangent_schedule.split(","))
+        h.set_fas(2, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
+    if a.tangent_omega is not None:
+        h.set_vanka(2, -1, omega=a.tangent_omega)
 
 
 def run_sweeps(a):
@@ -196,9 +209,11 @@ def run_ours(a, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    dtype = torch.float64 if a.precision == "fp64" else torch.float32
+    dtype = torch.float32 if a.precision == "fp32" else torch.float64
     f = dome(a.size, a.dx, a.radius, seed=0)
-    h = Hierarchy(a.size, a.size, a.dx, a.levels, dtype=dtype)
+    h = Hierarchy(a.size, a.size, a.dx, a.levels, precision=a.precision)
+    if a.inner is not None:
+        h.set_tuning(mixed_inner_vcycles=a.inner)
     for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
         h.set(k, 0, torch.as_tensor(f[k]), restrict_down=True)
     h.set_fas(False, maximum_vcycles=a.max_vcycles, relative_tolerance=a.rtol, absolute_tolerance=0.0)
@@ -246,7 +261,9 @@ def run_ours(a, rank, world):
     final_rel = float(np.max([s["final_norm"] / s["initial_norm"] for s in stats]))
     if a.quick:  # schedule exploration: the solve only
         return {"ms_per_step": ms, "vcycles_per_step": vcyc, "final_relative_residual": final_rel,
-                "schedule": a.schedule, "omega": a.omega, "relax": a.relax, "native": a.native}, None
+                "precision": a.precision, "method": a.method, "switch": a.switch,
+                "schedule": a.schedule, "omega": a.omega, "relax": a.relax, "native": a.native,
+                "tangent": [a.tangent_vcycles, a.tangent_schedule, a.tangent_omega]}, None
 
     # dominant kernel: the fused fine-level Vanka sweep, timed alone
     n_sw = 20
@@ -306,7 +323,7 @@ def run_ours(a, rank, world):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if dtype == torch.float64 else "f32",
+        "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f64 residual / f32 smoother"}[a.precision],
         "data": "synthetic (seeded dome, Gaussian random bed, log-normal beta)",
         "config": {"workload": f"dome {a.size}x{a.size}, dx={a.dx:g} m, {a.levels} levels, dt={a.dt:g} a, "
                                f"FASCD to rel. residual {a.rtol:g} (max {a.max_vcycles} V-cycles)",

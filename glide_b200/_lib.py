@@ -20,6 +20,7 @@ GLIDE_ERR_NONFINITE = 4
 GLIDE_ERR_STATE = 5
 GLIDE_F64 = 0
 GLIDE_F32 = 1
+GLIDE_MIXED = 2
 
 FIELDS = [
     "u", "v", "H", "H_prev", "phi", "mask", "bed", "B", "beta", "smb", "gamma",
@@ -29,6 +30,7 @@ FIELDS = [
     "grad_beta", "grad_bed", "grad_H_prev", "grad_smb",
     "vjp_u", "vjp_v", "vjp_H",
     "F_u", "F_v", "F_H",
+    "var_u", "var_v", "var_H", "jvp_u", "jvp_v", "jvp_H",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
@@ -117,6 +119,7 @@ SIGNATURES = {
     "glide_forward": ([_H, _D, _I, ctypes.POINTER(Stats), _P], _I),
     "glide_adjoint_residual": ([_H, _I, _D, ctypes.POINTER(_D), _P], _I),
     "glide_vjp": ([_H, _I, _D, _P], _I),
+    "glide_jvp": ([_H, _I, _D, _I, _P], _I),
     "glide_adjoint_sweep": ([_H, _I, _D, _I, _P], _I),
     "glide_gradients": ([_H, _I, _D, _I, _P], _I),
     "glide_backward": ([_H, _D, _I, _I, ctypes.POINTER(Stats), _P], _I),

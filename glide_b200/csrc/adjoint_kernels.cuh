@@ -394,7 +394,11 @@ struct AdjSweepArgs {
     int ny, nx;
 };
 
-template <class R>
+// TR = true: adjoint block smoother (solve with J^T; pinned rows get a zero
+// right-hand side, as the reference does).  TR = false: the same smoother for
+// the tangent system J e = f of the binary64 Newton outer iteration, whose
+// pinned rows are identity rows (the correction there equals the residual).
+template <class R, bool TR>
 __global__ void __launch_bounds__(kSweepThreads) k_adjoint_sweep(AdjSweepArgs<R> a) {
     using TileT = Tile<R, kTile, 2, 1>;
     constexpr int NC = TileT::NC;
@@ -429,16 +433,21 @@ __global__ void __launch_bounds__(kSweepThreads) k_adjoint_sweep(AdjSweepArgs<R>
         J[24] += a.mc_damping;
         b[0] = a.ru.at(i, j); b[1] = a.ru.at(i, j + 1); b[2] = a.rv.at(i, j); b[3] = a.rv.at(i + 1, j);
         b[4] = a.rH.at(i, j);
-        if (j == 0) { pin(J, 0); b[0] = R(0); }
-        if (j == nx - 1) { pin(J, 1); b[1] = R(0); }
-        if (i == 0) { pin(J, 2); b[2] = R(0); }
-        if (i == ny - 1) { pin(J, 3); b[3] = R(0); }
-        if (a.mask.at(i, j) > R(0.5)) { pin(J, 4); b[4] = R(0); }
+        const R zpin = R(0);
+        if (j == 0) { pin(J, 0); b[0] = TR ? zpin : b[0]; }
+        if (j == nx - 1) { pin(J, 1); b[1] = TR ? zpin : b[1]; }
+        if (i == 0) { pin(J, 2); b[2] = TR ? zpin : b[2]; }
+        if (i == ny - 1) { pin(J, 3); b[3] = TR ? zpin : b[3]; }
+        if (a.mask.at(i, j) > R(0.5)) { pin(J, 4); b[4] = TR ? zpin : b[4]; }
+        if (TR) {
 #pragma unroll
-        for (int r = 0; r < 5; ++r)
+            for (int r = 0; r < 5; ++r)
 #pragma unroll
-            for (int c = 0; c < 5; ++c) JT[r * 5 + c] = J[c * 5 + r];
-        lu5_solve(JT, b, dlam);
+                for (int c = 0; c < 5; ++c) JT[r * 5 + c] = J[c * 5 + r];
+            lu5_solve(JT, b, dlam);
+        } else {
+            lu5_solve(J, b, dlam);
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) dd[q] = R(0.5) * dlam[q];
         d4 = dlam[4];
@@ -459,6 +468,139 @@ __global__ void __launch_bounds__(kSweepThreads) k_adjoint_sweep(AdjSweepArgs<R>
         a.lv.at(i, j) = a.lv.at(i, j) - w * dv;
         if (i == ny - 1) a.lv.at(ny, j) = a.lv.at(ny, j) - w * dl[di][dj][3];
         a.lH.at(i, j) = a.lH.at(i, j) - w * d4;
+    }
+}
+
+// -------------------------------------------------------------------------
+// Block factors of the linear smoothers.  During a linear solve the state is
+// fixed, so each cell's 5x5 block (local Newton matrix + damping, pinned
+// rows, transposed for the adjoint) is factored once per V-cycle and stored:
+// 25 values per cell, structure-of-arrays (value k of cell (i,j) at
+// f[k * plane + i * pitch + j]), L below the diagonal, U above it and the
+// pivot reciprocals on it.  The smoother then costs one triangular solve.
+// -------------------------------------------------------------------------
+template <class R>
+struct BlockArgs {
+    Arr<R> u, v, H, phi, mask, bed, B, beta;
+    Arr<R> ru, rv, rH;  // residual of the linear system (sweep)
+    Arr<R> xu, xv, xH;  // unknowns, updated in place (sweep)
+    R* f;               // factors
+    size_t plane;
+    int pitch;
+    PhysR<R> p;
+    R omega, ssa_damping, mc_damping;
+    int ny, nx;
+};
+
+template <class R, bool TR>
+__global__ void __launch_bounds__(kTile * kTile) k_block_factor(BlockArgs<R> a) {
+    using TileT = Tile<R, kTile, 1, 1>;
+    constexpr int NC = TileT::NC;
+    __shared__ TileT t;
+    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int ny = a.ny, nx = a.nx;
+    stage_tile<R, kTile, 1, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
+    __syncthreads();
+    TileView<R, kTile, 1, 1> s{t, i0, j0, ny, nx};
+    for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
+        int r = k / NC, c = k % NC;
+        int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        R Bc = a.B.at(clampi(gi, 0, ny - 1), clampi(gj, 0, nx - 1));
+        t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x / kTile, j = j0 + threadIdx.x % kTile;
+    if (i >= ny || j >= nx) return;
+    R x[5] = {s.U(i, j), s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.Hc(i, j)};
+    R J[25], rr[5];
+    local_system<R>(s, a.p, i, j, x, J, rr);
+    J[0] -= a.ssa_damping; J[6] -= a.ssa_damping; J[12] -= a.ssa_damping; J[18] -= a.ssa_damping;
+    J[24] += a.mc_damping;
+    if (j == 0) pin(J, 0);
+    if (j == nx - 1) pin(J, 1);
+    if (i == 0) pin(J, 2);
+    if (i == ny - 1) pin(J, 3);
+    if (a.mask.at(i, j) > R(0.5)) pin(J, 4);
+    R M[25];
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) M[r * 5 + c] = TR ? J[c * 5 + r] : J[r * 5 + c];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const R inv = R(1) / M[k * 5 + k];
+#pragma unroll
+        for (int r = k + 1; r < 5; ++r) {
+            M[r * 5 + k] *= inv;
+#pragma unroll
+            for (int c = k + 1; c < 5; ++c) M[r * 5 + c] -= M[r * 5 + k] * M[k * 5 + c];
+        }
+        M[k * 5 + k] = inv;
+    }
+    R* f = a.f + size_t(i) * a.pitch + j;
+#pragma unroll
+    for (int k = 0; k < 25; ++k) f[k * a.plane] = M[k];
+}
+
+// One linear block-smoother sweep with stored factors: x += omega * delta
+// with delta = B^-1 (f - Op x) per cell, face corrections averaged between
+// the two cells of a face (adjoint: lambda -= omega * B^-T r, r = J^T lambda - f).
+template <class R, bool TR>
+__global__ void __launch_bounds__(kSweepThreads) k_block_sweep(BlockArgs<R> a) {
+    constexpr int ND = kTile + 1;
+    __shared__ R dl[ND][ND][4];
+    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int ny = a.ny, nx = a.nx;
+    int i, j;
+    const int tid = threadIdx.x;
+    if (tid < kTile * kTile) { i = i0 + tid / kTile; j = j0 + tid % kTile; }
+    else if (tid < kTile * kTile + kTile) { i = i0 + (tid - kTile * kTile); j = j0 - 1; }
+    else { i = i0 - 1; j = j0 + (tid - kTile * kTile - kTile); }
+    const bool live = i >= 0 && i < ny && j >= 0 && j < nx;
+    R d4 = 0;
+    R dd[4] = {0, 0, 0, 0};
+    if (live) {
+        R b[5] = {a.ru.at(i, j), a.ru.at(i, j + 1), a.rv.at(i, j), a.rv.at(i + 1, j), a.rH.at(i, j)};
+        if (TR) {  // the adjoint zeroes the pinned rows' right-hand side
+            if (j == 0) b[0] = R(0);
+            if (j == nx - 1) b[1] = R(0);
+            if (i == 0) b[2] = R(0);
+            if (i == ny - 1) b[3] = R(0);
+            if (a.mask.at(i, j) > R(0.5)) b[4] = R(0);
+        }
+        const R* f = a.f + size_t(i) * a.pitch + j;
+        R M[25];
+#pragma unroll
+        for (int k = 0; k < 25; ++k) M[k] = ldg(f + k * a.plane);
+        R y0 = b[0];
+        R y1 = b[1] - M[5] * y0;
+        R y2 = b[2] - M[10] * y0 - M[11] * y1;
+        R y3 = b[3] - M[15] * y0 - M[16] * y1 - M[17] * y2;
+        R y4 = b[4] - M[20] * y0 - M[21] * y1 - M[22] * y2 - M[23] * y3;
+        R x4 = y4 * M[24];
+        R x3 = (y3 - M[19] * x4) * M[18];
+        R x2 = (y2 - M[13] * x3 - M[14] * x4) * M[12];
+        R x1 = (y1 - M[7] * x2 - M[8] * x3 - M[9] * x4) * M[6];
+        R x0 = (y0 - M[1] * x1 - M[2] * x2 - M[3] * x3 - M[4] * x4) * M[0];
+        dd[0] = R(0.5) * x0; dd[1] = R(0.5) * x1; dd[2] = R(0.5) * x2; dd[3] = R(0.5) * x3;
+        d4 = x4;
+    }
+    {
+        const int di = i - (i0 - 1), dj = j - (j0 - 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dl[di][dj][q] = dd[q];
+    }
+    __syncthreads();
+    if (tid < kTile * kTile && live) {
+        const int di = i - (i0 - 1), dj = j - (j0 - 1);
+        const R w = a.omega;
+        R du = (j > 0 ? dl[di][dj - 1][1] : R(0)) + dl[di][dj][0];
+        a.xu.at(i, j) = a.xu.at(i, j) - w * du;
+        if (j == nx - 1) a.xu.at(i, nx) = a.xu.at(i, nx) - w * dl[di][dj][1];
+        R dv = (i > 0 ? dl[di - 1][dj][3] : R(0)) + dl[di][dj][2];
+        a.xv.at(i, j) = a.xv.at(i, j) - w * dv;
+        if (i == ny - 1) a.xv.at(ny, j) = a.xv.at(ny, j) - w * dl[di][dj][3];
+        a.xH.at(i, j) = a.xH.at(i, j) - w * d4;
     }
 }
 

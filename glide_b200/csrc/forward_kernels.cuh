@@ -26,6 +26,7 @@ struct ResidualArgs {
     PhysR<R> p;
     int ny, nx;
     int use_forcing, use_mask;
+    int active_set;              // Newton mode (see the mass row below)
 };
 
 template <class R>
@@ -50,7 +51,19 @@ __global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a) {
     double ssu = 0, ssv = 0, ssh = 0;
     if (i < ny && j < nx) {
         const bool f = a.use_forcing != 0;
-        {
+        if (a.active_set) {
+            // Newton mode: store the unmasked mass residual, decide the active
+            // set with the smoother's rule H - dt r_H <= gamma, and accumulate
+            // the norm of the masked residual (H - gamma on active cells)
+            R fH = f ? a.f_H.at(i, j) : R(0);
+            R r = mass_residual<R>(s, a.p, i, j, fH);
+            R Hc = s.Hc(i, j), g = a.gamma.at(i, j);
+            const bool act = (Hc - a.p.dt * r) <= g;
+            a.mask.at(i, j) = act ? R(1) : R(0);
+            a.o_H.at(i, j) = r;
+            R rn = act ? Hc - g : r;
+            ssh += double(rn) * double(rn);
+        } else {
             R fH = f ? a.f_H.at(i, j) : R(0);
             R r = mass_residual<R>(s, a.p, i, j, fH);
             R msk = a.use_mask ? a.mask.at(i, j) : R(0);

@@ -19,6 +19,7 @@
 #include "glide_b200.h"
 #include "forward_kernels.cuh"
 #include "adjoint_kernels.cuh"
+#include "tangent_kernels.cuh"
 #include "transfer_kernels.cuh"
 
 namespace glide {
@@ -47,19 +48,31 @@ static void check_launch(const char* what) {
     if (e != cudaSuccess) fail(GLIDE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-__global__ void k_finish_norms(const double* partial, int nblocks, double* out) {
-    // one warp: lane-strided sums, then a fixed shuffle tree
-    const int l = threadIdx.x;
+constexpr int kNormThreads = 1024;
+
+__global__ void __launch_bounds__(kNormThreads) k_finish_norms(const double* partial, int nblocks, double* out) {
+    // thread-strided sums, a fixed shuffle tree per warp, then warp 0 over
+    // the 32 warp sums: the same order on every call
+    __shared__ double ws[3][32];
+    const int t = threadIdx.x, l = t & 31, w = t >> 5;
     double s[3] = {0, 0, 0};
-    for (int b = l; b < nblocks; b += 32)
+    for (int b = t; b < nblocks; b += kNormThreads)
         for (int q = 0; q < 3; ++q) s[q] += partial[size_t(b) * 3 + q];
     for (int o = 16; o > 0; o >>= 1)
         for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
-    if (l == 0) {
-        out[0] = sqrt(s[0]);
-        out[1] = sqrt(s[1]);
-        out[2] = sqrt(s[2]);
-        out[3] = sqrt(s[0] + s[1] + s[2]);
+    if (l == 0)
+        for (int q = 0; q < 3; ++q) ws[q][w] = s[q];
+    __syncthreads();
+    if (w == 0) {
+        for (int q = 0; q < 3; ++q) s[q] = ws[q][l];
+        for (int o = 16; o > 0; o >>= 1)
+            for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+        if (l == 0) {
+            out[0] = sqrt(s[0]);
+            out[1] = sqrt(s[1]);
+            out[2] = sqrt(s[2]);
+            out[3] = sqrt(s[0] + s[1] + s[2]);
+        }
     }
 }
 
@@ -68,6 +81,9 @@ enum InternalField {
     F_U_ALT = GLIDE_N_PUBLIC_FIELDS, F_V_ALT, F_H_ALT,
     F_W_U, F_W_V, F_W_H, F_CHI,
     F_WL_U, F_WL_V, F_WL_H,
+    // tangent (Newton correction) system: correction, right-hand side,
+    // residual and the coarse-level snapshot of the correction
+    F_E_U, F_E_V, F_E_H, F_TF_U, F_TF_V, F_TF_H, F_TR_U, F_TR_V, F_TR_H, F_TW_U, F_TW_V, F_TW_H,
     F_COUNT
 };
 
@@ -77,9 +93,11 @@ static Kind field_kind(int f) {
     switch (f) {
         case GLIDE_U: case GLIDE_F_U: case GLIDE_R_U: case GLIDE_LAMBDA_U: case GLIDE_ADJ_F_U:
         case GLIDE_ADJ_R_U: case GLIDE_VJP_U: case GLIDE_FOP_U: case F_U_ALT: case F_W_U: case F_WL_U:
+        case F_E_U: case F_TF_U: case F_TR_U: case F_TW_U: case GLIDE_VAR_U: case GLIDE_JVP_U:
             return KU;
         case GLIDE_V: case GLIDE_F_V: case GLIDE_R_V: case GLIDE_LAMBDA_V: case GLIDE_ADJ_F_V:
         case GLIDE_ADJ_R_V: case GLIDE_VJP_V: case GLIDE_FOP_V: case F_V_ALT: case F_W_V: case F_WL_V:
+        case F_E_V: case F_TF_V: case F_TR_V: case F_TW_V: case GLIDE_VAR_V: case GLIDE_JVP_V:
             return KV;
         default:
             return KC;
@@ -109,18 +127,39 @@ static glide_vanka_config default_vanka() {
     return c;
 }
 
+// Linear multigrid of the Newton correction: light smoothing, no extra
+// finest-level sweeps; block smoother with the forward damping and omega 0.8.
+static glide_fas_config default_tangent_fas() {
+    glide_fas_config c = default_fas();
+    c.coarsest_steps = 50; c.pre_steps = 4; c.post_steps = 4; c.finest_steps = 0;
+    return c;
+}
+
+static glide_vanka_config default_tangent_vanka() {
+    glide_vanka_config c = default_vanka();
+    c.omega = 0.8;
+    return c;
+}
+
 static int round_up(int a, int m) { return (a + m - 1) / m * m; }
 
 struct SolverBase {
     virtual ~SolverBase() {}
     int dtype = GLIDE_F64;
     int n_levels = 0;
-    glide_fas_config fas[2];
+    // [0] forward FASCD, [1] FASAdjoint, [2] tangent (Newton correction) multigrid
+    glide_fas_config fas[3];
     int quirks = 1;
     int use_graphs = 1;
     unsigned version = 1;
     // Vanka sweep register budget: resident blocks per SM (1 or 2)
     int sweep_blocks_per_sm = 2;
+    // forward solve: 0 = FASCD V-cycles only (the reference's method);
+    // 1 = FASCD until rel. residual <= newton_switch, then Newton steps whose
+    //     correction comes from the tangent linear multigrid
+    int forward_method = 0;
+    double newton_switch = 1e-2;
+    double newton_stall_ratio = 0.7;
 };
 
 template <class R>
@@ -130,7 +169,7 @@ struct Level {
     int pu = 0, pv = 0, pc = 0;
     Arr<R> a[F_COUNT];
     glide_phys phys;
-    glide_vanka_config vk[2];  // [0] forward, [1] adjoint
+    glide_vanka_config vk[3];  // [0] forward, [1] adjoint, [2] tangent
     int blocks_x() const { return (nx + kTile - 1) / kTile; }
     int blocks_y() const { return (ny + kTile - 1) / kTile; }
 };
@@ -160,6 +199,7 @@ struct Solver : SolverBase {
         n_levels = L;
         fas[0] = default_fas();
         fas[1] = default_fas();
+        fas[2] = default_tangent_fas();
         lv.resize(L);
         size_t bytes = 0;
         const size_t align = 256;
@@ -174,6 +214,7 @@ struct Solver : SolverBase {
             v.phys = default_phys();
             v.vk[0] = default_vanka();
             v.vk[1] = default_vanka();
+            v.vk[2] = default_tangent_vanka();
             for (int f = 0; f < F_COUNT; ++f) {
                 Kind k = field_kind(f);
                 int rows = k == KV ? v.ny + 1 : v.ny;
@@ -206,6 +247,7 @@ struct Solver : SolverBase {
 
     ~Solver() override {
         if (graph) cudaGraphExecDestroy(graph);
+        for (R* b : blk) if (b) cudaFree(b);
         if (own_stream) cudaStreamDestroy(own_stream);
         if (norms_host) cudaFreeHost(norms_host);
         if (arena) cudaFree(arena);
@@ -265,7 +307,8 @@ struct Solver : SolverBase {
 
     // residual into (o_*) = R(x) [- f] [- sub]; norms into norms_dev when asked
     void residual(int l, double dt, bool use_forcing, bool use_mask, bool freeze_calving, bool freeze_phi,
-                  int out_u, int out_v, int out_H, const Arr<R>* sub, bool norms, cudaStream_t s) {
+                  int out_u, int out_v, int out_H, const Arr<R>* sub, bool norms, cudaStream_t s,
+                  bool active_set = false) {
         Level<R>& v = lv[l];
         if (!freeze_phi) compute_phi(l, 0.0, s);
         ResidualArgs<R> a;
@@ -279,11 +322,12 @@ struct Solver : SolverBase {
         a.p = physr(l, dt, freeze_calving);
         a.ny = v.ny; a.nx = v.nx;
         a.use_forcing = use_forcing; a.use_mask = use_mask;
+        a.active_set = active_set ? 1 : 0;
         dim3 g(v.blocks_x(), v.blocks_y());
         k_residual<R><<<g, 256, 0, s>>>(a);
         counted("residual");
         if (norms) {
-            k_finish_norms<<<1, 32, 0, s>>>(partial, g.x * g.y, norms_dev);
+            k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
             counted("finish_norms");
         }
     }
@@ -418,9 +462,16 @@ struct Solver : SolverBase {
             if (kind == 0) {
                 vcycle(start, true, dt, s);
                 residual(start, dt, true, true, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
-            } else {
+            } else if (kind == 1) {
                 adj_vcycle(start, true, dt, s);
                 adj_residual(start, dt, true, s);
+            } else {
+                if (kind == 4) {
+                    newton_cycle(start, dt, s);
+                } else if constexpr (sizeof(R) == 8) {
+                    if (kind == 2) mixed_cycle(start, dt, s);
+                    else mixed_adj_cycle(start, dt, s);
+                }
             }
         };
         if (!use_graphs) {
@@ -459,9 +510,122 @@ struct Solver : SolverBase {
         launches += graph_launches;
     }
 
+    // ------------------------------------------------ mixed precision
+    // binary64 state and residual on the solve level; a binary32 shadow
+    // hierarchy runs the smoother and every coarse level.  Each outer step is
+    // a nonlinear defect correction:
+    //   r = R64(x)  (unmasked),   g = F32(fl(x)) - fl(r),
+    //   y = FASCD V-cycle(s) of F32(y) = g from y0 = fl(x),
+    //   x <- x + (y - fl(x))  (binary64),  mask <- mask32, H = gamma on masked cells,
+    // and the convergence test is the reference's masked binary64 residual.
+    std::unique_ptr<Solver<float>> lo;
+    int mixed_inner = 1;
+
+    template <class D, class Src>
+    void convert(const Arr<D>& d, const Arr<Src>& src, double scale, cudaStream_t s) {
+        k_convert<D, Src><<<pw_grid(src.rows, src.cols), 256, 0, s>>>(d, src, scale, src.rows, src.cols);
+        counted("convert");
+    }
+
+    void sync_shadow() {
+        Solver<float>& f = *lo;
+        for (int q = 0; q < 3; ++q) f.fas[q] = fas[q];
+        f.quirks = quirks;
+        f.sweep_blocks_per_sm = sweep_blocks_per_sm;
+        f.use_graphs = 0;
+        for (int l = 0; l < n_levels; ++l) {
+            if (f.lv[l].phys.thklim != lv[l].phys.thklim)
+                f.fill(f.lv[l].a[GLIDE_GAMMA], float(lv[l].phys.thklim), nullptr);
+            f.lv[l].phys = lv[l].phys;
+            for (int q = 0; q < 3; ++q) f.lv[l].vk[q] = lv[l].vk[q];
+        }
+    }
+
+    // binary64 level-l fields -> shadow, then restricted down in the shadow
+    void push_to_shadow(int l, std::initializer_list<int> fields, bool restrict_down, cudaStream_t s) {
+        Solver<float>& f = *lo;
+        for (int fld : fields) {
+            convert(f.lv[l].a[fld], lv[l].a[fld], 1.0, s);
+            if (restrict_down)
+                for (int q = l; q + 1 < n_levels; ++q) f.restrict_field(fld, q, s);
+        }
+    }
+
+    void mixed_cycle(int l, double dt, cudaStream_t s) {
+        Solver<float>& f = *lo;
+        Level<R>& D = lv[l];
+        Level<float>& F = f.lv[l];
+        push_to_shadow(l, {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_MASK, GLIDE_PHI}, false, s);
+        residual(l, dt, true, false, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, false, s);
+        push_to_shadow(l, {GLIDE_R_U, GLIDE_R_V, GLIDE_R_H}, false, s);
+        const Arr<float> sub[3] = {F.a[GLIDE_R_U], F.a[GLIDE_R_V], F.a[GLIDE_R_H]};
+        f.residual(l, dt, false, false, false, true, GLIDE_F_U, GLIDE_F_V, GLIDE_F_H, sub, false, s);
+        for (int k = 0; k < mixed_inner; ++k) f.vcycle(l, true, dt, s);
+        k_defect_update<R, float><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
+            D.a[GLIDE_U], D.a[GLIDE_V], D.a[GLIDE_H], D.a[GLIDE_MASK], D.a[GLIDE_GAMMA], F.a[GLIDE_U],
+            F.a[GLIDE_V], F.a[GLIDE_H], F.a[GLIDE_MASK], D.ny, D.nx);
+        counted("defect_update");
+        residual(l, dt, true, true, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
+    }
+
+    void mixed_adj_cycle(int l, double dt, cudaStream_t s) {
+        Solver<float>& f = *lo;
+        Level<R>& D = lv[l];
+        Level<float>& F = f.lv[l];
+        adj_residual(l, dt, false, s);
+        for (int fld : {GLIDE_LAMBDA_U, GLIDE_LAMBDA_V, GLIDE_LAMBDA_H}) f.fill(F.a[fld], 0.0f, s);
+        convert(F.a[GLIDE_ADJ_F_U], D.a[GLIDE_ADJ_R_U], -1.0, s);
+        convert(F.a[GLIDE_ADJ_F_V], D.a[GLIDE_ADJ_R_V], -1.0, s);
+        convert(F.a[GLIDE_ADJ_F_H], D.a[GLIDE_ADJ_R_H], -1.0, s);
+        for (int k = 0; k < mixed_inner; ++k) f.adj_vcycle(l, true, dt, s);
+        convert_add(D.a[GLIDE_LAMBDA_U], F.a[GLIDE_LAMBDA_U], s);
+        convert_add(D.a[GLIDE_LAMBDA_V], F.a[GLIDE_LAMBDA_V], s);
+        convert_add(D.a[GLIDE_LAMBDA_H], F.a[GLIDE_LAMBDA_H], s);
+        adj_residual(l, dt, true, s);
+    }
+
+    template <class Src>
+    void convert_add(const Arr<R>& d, const Arr<Src>& src, cudaStream_t s) {
+        k_add_converted<R, Src><<<pw_grid(src.rows, src.cols), 256, 0, s>>>(d, src, src.rows, src.cols);
+        counted("add_converted");
+    }
+
+    void forward_mixed(double dt, int start, glide_stats* st, cudaStream_t s) {
+        sync_shadow();
+        lo->check_quirks();
+        set_rhs(start, dt, s);
+        push_to_shadow(start, {GLIDE_BED, GLIDE_B, GLIDE_BETA, GLIDE_SMB, GLIDE_H_PREV}, true, s);
+        residual(start, dt, true, true, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
+        double nr[4];
+        read_norms(nr, s);
+        solve_loop(2, start, dt, nr, st, s);
+    }
+
+    void backward_mixed(double dt, int start, int grad_mask, glide_stats* st, cudaStream_t s) {
+        sync_shadow();
+        lo->check_quirks();
+        push_to_shadow(start, {GLIDE_BED, GLIDE_B, GLIDE_BETA, GLIDE_SMB}, true, s);
+        push_to_shadow(start, {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_H_PREV, GLIDE_PHI, GLIDE_MASK}, false, s);
+        adj_residual(start, dt, true, s);
+        double nr[4];
+        read_norms(nr, s);
+        solve_loop(3, start, dt, nr, st, s);
+        gradients(start, dt, grad_mask, s);
+    }
+
     void forward(double dt, int start, glide_stats* st, cudaStream_t s) {
         check_level(start);
         check_quirks();
+        if (forward_method == 1) ensure_blocks();
+        if constexpr (sizeof(R) == 8) {
+            if (lo) lo->ensure_blocks();
+        }
+        if constexpr (sizeof(R) == 8) {
+            if (lo) {
+                forward_mixed(dt, start, st, s);
+                return;
+            }
+        }
         set_rhs(start, dt, s);
         residual(start, dt, true, true, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
         double nr[4];
@@ -470,22 +634,41 @@ struct Solver : SolverBase {
     }
 
     void solve_loop(int kind, int start, double dt, double nr[4], glide_stats* st, cudaStream_t s) {
-        const glide_fas_config& c = fas[kind];
+        const glide_fas_config& c = fas[kind & 1];  // 0/2 forward, 1/3 adjoint
         const double r0 = nr[3];
         if (!std::isfinite(r0)) fail(GLIDE_ERR_NONFINITE, "initial residual norm is not finite");
         double rel = 1.0, ab = r0;
         int it = 0;
+        bool in_newton = false;
         if (st) {
             std::memset(st, 0, sizeof(*st));
             st->initial_norm = r0;
             st->history[0] = r0;
         }
+        // Newton safeguard: two consecutive steps that fail to cut the residual
+        // by `newton_stall_ratio` hand the rest of the solve back to FASCD
+        bool newton_off = false;
+        int stall = 0;
+        double prev = ab;
         while (rel > c.relative_tolerance && ab > c.absolute_tolerance && it < c.maximum_vcycles) {
-            cycle_and_check(kind, start, dt, s);
+            // forward solves may finish with Newton steps once the FAS phase is close
+            int k = kind;
+            if ((kind == 0 || kind == 2) && forward_method == 1 && rel <= newton_switch && !newton_off) k = 4;
+            if (k == 4 && !in_newton) {
+                newton_prologue(start, dt, s);
+                in_newton = true;
+            }
+            if (k != 4) in_newton = false;
+            cycle_and_check(k, start, dt, s);
             read_norms(nr, s);
             ab = nr[3];
             if (!std::isfinite(ab)) fail(GLIDE_ERR_NONFINITE, "residual norm became non-finite");
             rel = ab / r0;
+            if (k == 4) {
+                stall = ab > newton_stall_ratio * prev ? stall + 1 : 0;
+                if (stall >= 2) newton_off = true;
+            }
+            prev = ab;
             ++it;
             if (st && it < GLIDE_MAX_HISTORY) st->history[it] = ab;
         }
@@ -500,117 +683,209 @@ struct Solver : SolverBase {
         if (l < 0 || l >= n_levels) fail(GLIDE_ERR_ARG, "level out of range");
     }
 
-    // ------------------------------------------------------------ adjoint
-    // (kernels in adjoint_kernels.cuh)
-    void vjp_into(int l, double dt, bool use_forcing, int ou, int ov, int oh, cudaStream_t s) {
+    // ------------------------------------------------------ linear systems
+    // The adjoint J^T lambda = f (FASAdjoint, glide/multigrid.py:857-973) and
+    // the tangent J e = f of the Newton outer iteration share one linear
+    // multigrid: the same transfers, block smoother and V-cycle, with the
+    // operator transposed or not.
+    struct Lin {
+        int x[3], f[3], r[3], w[3];
+        bool tr;  // transpose: the adjoint system
+        int cfg;  // schedule / smoother config: 1 adjoint, 2 tangent
+    };
+    static Lin adj_sys() {
+        return {{GLIDE_LAMBDA_U, GLIDE_LAMBDA_V, GLIDE_LAMBDA_H}, {GLIDE_ADJ_F_U, GLIDE_ADJ_F_V, GLIDE_ADJ_F_H},
+                {GLIDE_ADJ_R_U, GLIDE_ADJ_R_V, GLIDE_ADJ_R_H}, {F_WL_U, F_WL_V, F_WL_H}, true, 1};
+    }
+    static Lin tan_sys() {
+        return {{F_E_U, F_E_V, F_E_H}, {F_TF_U, F_TF_V, F_TF_H}, {F_TR_U, F_TR_V, F_TR_H},
+                {F_TW_U, F_TW_V, F_TW_H}, false, 2};
+    }
+
+    // out = Op(x) [- f] [- sub], Op = J^T (vjp) or J (jvp) at the level's state
+    void lin_op(int l, double dt, const Lin& L, const int* out, const int* sub, bool use_forcing, bool norms,
+                bool ref_rows, cudaStream_t s) {
         Level<R>& v = lv[l];
         VjpArgs<R> a;
         a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
         a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
         a.beta = v.a[GLIDE_BETA];
-        a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
-        a.f_u = v.a[GLIDE_ADJ_F_U]; a.f_v = v.a[GLIDE_ADJ_F_V]; a.f_H = v.a[GLIDE_ADJ_F_H];
-        a.o_u = v.a[ou]; a.o_v = v.a[ov]; a.o_H = v.a[oh];
-        a.partial = nullptr;
+        a.lu = v.a[L.x[0]]; a.lv = v.a[L.x[1]]; a.lH = v.a[L.x[2]];
+        a.f_u = v.a[L.f[0]]; a.f_v = v.a[L.f[1]]; a.f_H = v.a[L.f[2]];
+        a.o_u = v.a[out[0]]; a.o_v = v.a[out[1]]; a.o_H = v.a[out[2]];
+        if (sub) { a.s_u = v.a[sub[0]]; a.s_v = v.a[sub[1]]; a.s_H = v.a[sub[2]]; }
+        a.partial = norms ? partial : nullptr;
         a.p = physr(l, dt, false);
         a.ny = v.ny; a.nx = v.nx; a.use_forcing = use_forcing;
-        launch_vjp(a, s);
-    }
-
-    void launch_vjp(VjpArgs<R>& a, cudaStream_t s) {
-        dim3 g((a.nx + kTile - 1) / kTile, (a.ny + kTile - 1) / kTile);
-        k_vjp<R><<<g, 256, 0, s>>>(a);
-        counted("vjp");
-        if (a.partial) {
-            k_finish_norms<<<1, 32, 0, s>>>(partial, g.x * g.y, norms_dev);
+        dim3 g((a.nx + kTileA - 1) / kTileA, (a.ny + kTileA - 1) / kTileA);
+        if (L.tr) {
+            k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a);
+            counted("vjp");
+        } else {
+            k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, ref_rows ? 1 : 0);
+            counted("jvp");
+        }
+        if (norms) {
+            k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
             counted("finish_norms");
         }
     }
 
-    void adj_residual(int l, double dt, bool norms, cudaStream_t s) {
+    void vjp_into(int l, double dt, bool use_forcing, int ou, int ov, int oh, cudaStream_t s) {
+        const int out[3] = {ou, ov, oh};
+        lin_op(l, dt, adj_sys(), out, nullptr, use_forcing, false, false, s);
+    }
+
+    void lin_residual(int l, double dt, const Lin& L, bool norms, cudaStream_t s) {
+        lin_op(l, dt, L, L.r, nullptr, true, norms, false, s);
+    }
+
+    void adj_residual(int l, double dt, bool norms, cudaStream_t s) { lin_residual(l, dt, adj_sys(), norms, s); }
+
+    // stored block factors of the linear smoother, one buffer per level
+    std::vector<R*> blk;
+
+    // allocated on first use, before any stream capture begins
+    void ensure_blocks() {
+        if (!blk.empty()) return;
+        blk.assign(n_levels, nullptr);
+        for (int l = 0; l < n_levels; ++l)
+            GCU(cudaMalloc(&blk[l], size_t(25) * lv[l].ny * lv[l].pc * sizeof(R)));
+    }
+
+    BlockArgs<R> block_args(int l, double dt, const Lin& L) {
         Level<R>& v = lv[l];
-        VjpArgs<R> a;
+        if (blk.empty()) fail(GLIDE_ERR_STATE, "block factor buffers not allocated");
+        const glide_vanka_config& c = v.vk[L.cfg];
+        BlockArgs<R> a;
         a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
         a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
         a.beta = v.a[GLIDE_BETA];
-        a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
-        a.f_u = v.a[GLIDE_ADJ_F_U]; a.f_v = v.a[GLIDE_ADJ_F_V]; a.f_H = v.a[GLIDE_ADJ_F_H];
-        a.o_u = v.a[GLIDE_ADJ_R_U]; a.o_v = v.a[GLIDE_ADJ_R_V]; a.o_H = v.a[GLIDE_ADJ_R_H];
-        a.partial = norms ? partial : nullptr;
+        a.ru = v.a[L.r[0]]; a.rv = v.a[L.r[1]]; a.rH = v.a[L.r[2]];
+        a.xu = v.a[L.x[0]]; a.xv = v.a[L.x[1]]; a.xH = v.a[L.x[2]];
+        a.f = blk[l];
+        a.plane = size_t(v.ny) * v.pc;
+        a.pitch = v.pc;
         a.p = physr(l, dt, false);
-        a.ny = v.ny; a.nx = v.nx; a.use_forcing = 1;
-        launch_vjp(a, s);
+        a.omega = R(c.omega); a.ssa_damping = R(c.ssa_damping); a.mc_damping = R(c.mc_damping);
+        a.ny = v.ny; a.nx = v.nx;
+        return a;
     }
 
-    void adj_sweeps(int l, double dt, int n, cudaStream_t s) {
-        Level<R>& v = lv[l];
-        const glide_vanka_config& c = v.vk[1];
+    void block_factor(int l, double dt, const Lin& L, cudaStream_t s) {
+        BlockArgs<R> a = block_args(l, dt, L);
+        dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
+        if (L.tr) k_block_factor<R, true><<<g, kTile * kTile, 0, s>>>(a);
+        else k_block_factor<R, false><<<g, kTile * kTile, 0, s>>>(a);
+        counted("block_factor");
+    }
+
+    // n linear smoother sweeps (residual, then block solve and update); the
+    // factors are refreshed first unless the caller just did
+    void lin_sweeps(int l, double dt, int n, const Lin& L, cudaStream_t s, bool factor = true) {
+        if (n <= 0) return;
+        if (factor) block_factor(l, dt, L, s);
+        BlockArgs<R> a = block_args(l, dt, L);
+        dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
         for (int k = 0; k < n; ++k) {
-            adj_residual(l, dt, false, s);
-            AdjSweepArgs<R> a;
-            a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
-            a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
-            a.beta = v.a[GLIDE_BETA];
-            a.ru = v.a[GLIDE_ADJ_R_U]; a.rv = v.a[GLIDE_ADJ_R_V]; a.rH = v.a[GLIDE_ADJ_R_H];
-            a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
-            a.p = physr(l, dt, false);
-            a.omega = R(c.omega); a.ssa_damping = R(c.ssa_damping); a.mc_damping = R(c.mc_damping);
-            a.ny = v.ny; a.nx = v.nx;
-            dim3 g(v.blocks_x(), v.blocks_y());
-            k_adjoint_sweep<R><<<g, kSweepThreads, 0, s>>>(a);
-            counted("adjoint_sweep");
+            lin_residual(l, dt, L, false, s);
+            if (L.tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
+            else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
+            counted("linear_sweep");
         }
     }
 
-    // glide/multigrid.py:905-973
-    void adj_vcycle(int l, bool finest, double dt, cudaStream_t s) {
-        const glide_fas_config& c = fas[1];
+    void adj_sweeps(int l, double dt, int n, cudaStream_t s) { lin_sweeps(l, dt, n, adj_sys(), s); }
+
+    // glide/multigrid.py:905-973 (linear FAS)
+    void lin_vcycle(int l, bool finest, double dt, const Lin& L, cudaStream_t s) {
+        const glide_fas_config& c = fas[L.cfg];
+        block_factor(l, dt, L, s);  // the state is fixed for this visit of level l
         if (l == n_levels - 1) {
-            adj_sweeps(l, dt, c.coarsest_steps, s);
+            lin_sweeps(l, dt, c.coarsest_steps, L, s, false);
             return;
         }
         Level<R>& n = lv[l + 1];
-        adj_sweeps(l, dt, c.pre_steps, s);
+        lin_sweeps(l, dt, c.pre_steps, L, s, false);
         restrict_field(GLIDE_U, l, s);
         restrict_field(GLIDE_V, l, s);
         restrict_field(GLIDE_H, l, s);
         restrict_field(GLIDE_H_PREV, l, s);
         restrict_field(GLIDE_PHI, l, s);
         restrict_field(GLIDE_MASK, l, s);
-        restrict_field(GLIDE_LAMBDA_U, l, s, n.a[F_WL_U]);
-        restrict_field(GLIDE_LAMBDA_V, l, s, n.a[F_WL_V]);
-        restrict_field(GLIDE_LAMBDA_H, l, s, n.a[F_WL_H]);
-        adj_residual(l, dt, false, s);
-        restrict_field(GLIDE_ADJ_R_U, l, s);
-        restrict_field(GLIDE_ADJ_R_V, l, s);
-        restrict_field(GLIDE_ADJ_R_H, l, s);
-        // coarse right-hand side f_c = vjp_c - R r, in one pass
-        {
-            VjpArgs<R> a;
-            Level<R>& v = n;
-            a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
-            a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
-            a.beta = v.a[GLIDE_BETA];
-            a.lu = v.a[GLIDE_LAMBDA_U]; a.lv = v.a[GLIDE_LAMBDA_V]; a.lH = v.a[GLIDE_LAMBDA_H];
-            a.f_u = v.a[GLIDE_ADJ_F_U]; a.f_v = v.a[GLIDE_ADJ_F_V]; a.f_H = v.a[GLIDE_ADJ_F_H];
-            a.o_u = v.a[GLIDE_ADJ_F_U]; a.o_v = v.a[GLIDE_ADJ_F_V]; a.o_H = v.a[GLIDE_ADJ_F_H];
-            a.s_u = v.a[GLIDE_ADJ_R_U]; a.s_v = v.a[GLIDE_ADJ_R_V]; a.s_H = v.a[GLIDE_ADJ_R_H];
-            a.partial = nullptr;
-            a.p = physr(l + 1, dt, false);
-            a.ny = v.ny; a.nx = v.nx; a.use_forcing = 0;
-            launch_vjp(a, s);
+        for (int q = 0; q < 3; ++q) restrict_field(L.x[q], l, s, n.a[L.w[q]]);
+        lin_residual(l, dt, L, false, s);
+        for (int q = 0; q < 3; ++q) restrict_field(L.r[q], l, s);
+        // coarse right-hand side f_c = Op_c(x_c) - R r, in one pass
+        lin_op(l + 1, dt, L, L.f, L.r, false, false, false, s);
+        lin_vcycle(l + 1, false, dt, L, s);
+        correct(l, L.x[0], L.w[0], kFaceU, 1, s);
+        correct(l, L.x[1], L.w[1], kFaceV, 1, s);
+        correct(l, L.x[2], L.w[2], kCellMax, 1, s);
+        lin_sweeps(l, dt, c.post_steps, L, s, false);
+        if (finest) lin_sweeps(l, dt, c.finest_steps, L, s, false);
+    }
+
+    void adj_vcycle(int l, bool finest, double dt, cudaStream_t s) { lin_vcycle(l, finest, dt, adj_sys(), s); }
+
+    // ----------------------------------------------------- Newton cycle
+    // One outer step of Newton's method on the binary64 residual.  On entry
+    // R_* hold the unmasked residual of the current state and MASK its active
+    // set (the smoother's rule H - dt r_H <= gamma; see newton_prologue).  The
+    // tangent system J(x) e = -r (identity rows on active cells and Dirichlet
+    // faces) is solved by `tangent_vcycles` V-cycles of the linear multigrid --
+    // on the binary32 shadow for a mixed handle, on this hierarchy otherwise --
+    // then x <- x + e with H floored at gamma, and one binary64 residual pass
+    // recomputes phi, the residual, the next active set and the masked norms.
+    int tangent_vcycles = 1;
+
+    void newton_prologue(int l, double dt, cudaStream_t s) {
+        residual(l, dt, true, false, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, false, s, true);
+    }
+
+    template <class T>
+    void newton_cycle_on(Solver<T>& ts, int l, double dt, cudaStream_t s) {
+        Level<R>& D = lv[l];
+        Level<T>& F = ts.lv[l];
+        if constexpr (!std::is_same<T, R>::value) {
+            push_to_shadow(l, {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_MASK}, false, s);
         }
-        adj_vcycle(l + 1, false, dt, s);
-        correct(l, GLIDE_LAMBDA_U, F_WL_U, kFaceU, 1, s);
-        correct(l, GLIDE_LAMBDA_V, F_WL_V, kFaceV, 1, s);
-        correct(l, GLIDE_LAMBDA_H, F_WL_H, kCellMax, 1, s);
-        adj_sweeps(l, dt, c.post_steps, s);
-        if (finest) adj_sweeps(l, dt, c.finest_steps, s);
+        k_tangent_rhs<T, R><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
+            F.a[F_TF_U], F.a[F_TF_V], F.a[F_TF_H], D.a[GLIDE_R_U], D.a[GLIDE_R_V], D.a[GLIDE_R_H], D.a[GLIDE_H],
+            D.a[GLIDE_GAMMA], D.a[GLIDE_MASK], D.ny, D.nx);
+        counted("tangent_rhs");
+        for (int fld : {F_E_U, F_E_V, F_E_H}) ts.fill(F.a[fld], T(0), s);
+        for (int k = 0; k < tangent_vcycles; ++k) ts.lin_vcycle(l, true, dt, Solver<T>::tan_sys(), s);
+        k_newton_update<R, T><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
+            D.a[GLIDE_U], D.a[GLIDE_V], D.a[GLIDE_H], D.a[GLIDE_GAMMA], F.a[F_E_U], F.a[F_E_V], F.a[F_E_H],
+            D.ny, D.nx);
+        counted("newton_update");
+        residual(l, dt, true, false, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s, true);
+    }
+
+    void newton_cycle(int l, double dt, cudaStream_t s) {
+        if constexpr (sizeof(R) == 8) {
+            if (lo) {
+                newton_cycle_on(*lo, l, dt, s);
+                return;
+            }
+        }
+        newton_cycle_on(*this, l, dt, s);
     }
 
     void backward(double dt, int start, int grad_mask, glide_stats* st, cudaStream_t s) {
         check_level(start);
         check_quirks();
+        ensure_blocks();
+        if constexpr (sizeof(R) == 8) {
+            if (lo) lo->ensure_blocks();
+        }
+        if constexpr (sizeof(R) == 8) {
+            if (lo) {
+                backward_mixed(dt, start, grad_mask, st, s);
+                return;
+            }
+        }
         adj_residual(start, dt, true, s);
         double nr[4];
         read_norms(nr, s);
@@ -695,9 +970,18 @@ int glide_create(int ny, int nx, double dx, int n_levels, int dtype, glide_handl
         if ((ny >> (n_levels - 1)) < 2 || (nx >> (n_levels - 1)) < 2)
             fail(GLIDE_ERR_SHAPE, "coarsest level must have at least 2x2 cells");
         auto h = std::make_unique<glide_solver>();
-        if (dtype == GLIDE_F64) h->impl = std::make_unique<Solver<double>>(ny, nx, dx, n_levels);
-        else if (dtype == GLIDE_F32) h->impl = std::make_unique<Solver<float>>(ny, nx, dx, n_levels);
-        else fail(GLIDE_ERR_ARG, "dtype must be GLIDE_F64 or GLIDE_F32");
+        if (dtype == GLIDE_F64) {
+            h->impl = std::make_unique<Solver<double>>(ny, nx, dx, n_levels);
+        } else if (dtype == GLIDE_F32) {
+            h->impl = std::make_unique<Solver<float>>(ny, nx, dx, n_levels);
+        } else if (dtype == GLIDE_MIXED) {
+            auto d = std::make_unique<Solver<double>>(ny, nx, dx, n_levels);
+            d->lo = std::make_unique<Solver<float>>(ny, nx, dx, n_levels);
+            d->forward_method = 1;  // FAS in binary32 stalls at its rounding floor: finish with Newton
+            h->impl = std::move(d);
+        } else {
+            fail(GLIDE_ERR_ARG, "dtype must be GLIDE_F64, GLIDE_F32 or GLIDE_MIXED");
+        }
         *out = h.release();
     });
 }
@@ -813,41 +1097,47 @@ int glide_get_phys(glide_handle h, int level, glide_phys* p) {
     });
 }
 
-int glide_set_fas_config(glide_handle h, int adjoint, const glide_fas_config* c) {
+static int which_config(int which) {
+    if (which < 0 || which > 2) fail(GLIDE_ERR_ARG, "config selector must be 0 (forward), 1 (adjoint) or 2 (tangent)");
+    return which;
+}
+
+int glide_set_fas_config(glide_handle h, int which, const glide_fas_config* c) {
     return guarded([&] {
         if (!c) fail(GLIDE_ERR_ARG, "null config");
         dispatch(h, [&](auto& s) {
-            s.fas[adjoint ? 1 : 0] = *c;
+            s.fas[which_config(which)] = *c;
             ++s.version;
         });
     });
 }
 
-int glide_get_fas_config(glide_handle h, int adjoint, glide_fas_config* c) {
+int glide_get_fas_config(glide_handle h, int which, glide_fas_config* c) {
     return guarded([&] {
         if (!c) fail(GLIDE_ERR_ARG, "null config");
-        dispatch(h, [&](auto& s) { *c = s.fas[adjoint ? 1 : 0]; });
+        dispatch(h, [&](auto& s) { *c = s.fas[which_config(which)]; });
     });
 }
 
-int glide_set_vanka_config(glide_handle h, int adjoint, int level, const glide_vanka_config* c) {
+int glide_set_vanka_config(glide_handle h, int which, int level, const glide_vanka_config* c) {
     return guarded([&] {
         if (!c) fail(GLIDE_ERR_ARG, "null config");
         dispatch(h, [&](auto& s) {
+            const int q = which_config(which);
             if (level >= s.n_levels) fail(GLIDE_ERR_ARG, "level out of range");
             for (int l = 0; l < s.n_levels; ++l)
-                if (level < 0 || l == level) s.lv[l].vk[adjoint ? 1 : 0] = *c;
+                if (level < 0 || l == level) s.lv[l].vk[q] = *c;
             ++s.version;
         });
     });
 }
 
-int glide_get_vanka_config(glide_handle h, int adjoint, int level, glide_vanka_config* c) {
+int glide_get_vanka_config(glide_handle h, int which, int level, glide_vanka_config* c) {
     return guarded([&] {
         if (!c) fail(GLIDE_ERR_ARG, "null config");
         dispatch(h, [&](auto& s) {
             s.check_level(level);
-            *c = s.lv[level].vk[adjoint ? 1 : 0];
+            *c = s.lv[level].vk[which_config(which)];
         });
     });
 }
@@ -867,6 +1157,18 @@ int glide_set_tuning(glide_handle h, int key, int value) {
             if (key == GLIDE_TUNE_SWEEP_BLOCKS_PER_SM) {
                 if (value < 1 || value > 2) fail(GLIDE_ERR_ARG, "sweep blocks per SM must be 1 or 2");
                 s.sweep_blocks_per_sm = value;
+            } else if (key == GLIDE_TUNE_MIXED_INNER_VCYCLES) {
+                if (value < 1 || value > 16) fail(GLIDE_ERR_ARG, "inner V-cycles must be in [1, 16]");
+                s.mixed_inner = value;
+            } else if (key == GLIDE_TUNE_FORWARD_METHOD) {
+                if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "forward method must be 0 (FASCD) or 1 (FASCD + Newton)");
+                s.forward_method = value;
+            } else if (key == GLIDE_TUNE_NEWTON_SWITCH_EXP10) {
+                if (value < 0 || value > 15) fail(GLIDE_ERR_ARG, "Newton switch exponent must be in [0, 15]");
+                s.newton_switch = std::pow(10.0, -double(value));
+            } else if (key == GLIDE_TUNE_TANGENT_VCYCLES) {
+                if (value < 1 || value > 16) fail(GLIDE_ERR_ARG, "tangent V-cycles must be in [1, 16]");
+                s.tangent_vcycles = value;
             } else {
                 fail(GLIDE_ERR_ARG, "unknown tuning key");
             }
@@ -957,11 +1259,25 @@ int glide_vjp(glide_handle h, int level, double dt, void* stream) {
     });
 }
 
+int glide_jvp(glide_handle h, int level, double dt, int reference_rows, void* stream) {
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            using SolverT = std::remove_reference_t<decltype(s)>;
+            typename SolverT::Lin L = SolverT::tan_sys();
+            L.x[0] = GLIDE_VAR_U; L.x[1] = GLIDE_VAR_V; L.x[2] = GLIDE_VAR_H;
+            const int out[3] = {GLIDE_JVP_U, GLIDE_JVP_V, GLIDE_JVP_H};
+            s.lin_op(level, dt, L, out, nullptr, false, false, reference_rows != 0, S(stream));
+        });
+    });
+}
+
 int glide_adjoint_sweep(glide_handle h, int level, double dt, int n, void* stream) {
     return guarded([&] {
         if (n < 0) fail(GLIDE_ERR_ARG, "negative sweep count");
         dispatch(h, [&](auto& s) {
             s.check_level(level);
+            s.ensure_blocks();
             s.adj_sweeps(level, dt, n, S(stream));
         });
     });

@@ -1,0 +1,220 @@
+// tangent_kernels.cuh -- Jacobian-vector product of the coupled operator.
+//
+// r_lin = J(x) e - f over one level: the exact directional derivative of the
+// residual rows along e = (e_u, e_v, e_H), the grounded fraction held fixed
+// (as the reference's forward-mode kernel does, residuals.cu:341-660), with
+// the rows the solver pins written as identity rows: Dirichlet faces
+// (u on x = 0, nx; v on y = 0, ny) and active-set cells (mask = 1) give
+// r_lin = e - f there.  With `ref_rows` the pinned rows follow the reference
+// kernel instead (zero on Dirichlet faces, (1 - mask) times the mass row).
+#pragma once
+
+#include "adjoint_kernels.cuh"
+
+namespace glide {
+
+template <class R>
+struct TanView {
+    const AdjTile<R>& a;  // lu/lv hold e_u/e_v, etad holds d(eta) along e
+    const Arr<R>* eH;
+    int i0, j0, ny, nx;
+    static constexpr int A = 2;
+    __device__ R U(int i, int j) const { return a.t.u[i - (i0 - A - 1)][j - (j0 - A)]; }
+    __device__ R V(int i, int j) const { return a.t.v[i - (i0 - A)][j - (j0 - A - 1)]; }
+    __device__ R LU(int i, int j) const { return a.lu[i - (i0 - A - 1)][j - (j0 - A)]; }
+    __device__ R LV(int i, int j) const { return a.lv[i - (i0 - A)][j - (j0 - A - 1)]; }
+    __device__ R Hc(int i, int j) const { return a.t.H[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R PHI(int i, int j) const { return a.t.phi[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R BED(int i, int j) const { return a.t.bed[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R BETA(int i, int j) const { return a.t.beta[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R ETA(int i, int j) const { return a.t.eta[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R ETAD(int i, int j) const { return a.etad[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R EH(int i, int j) const { return eH->at(clampi(i, 0, ny - 1), clampi(j, 0, nx - 1)); }
+};
+
+// d(mass row of cell (i,j)) . e before masking (residuals.cu:391-439)
+template <class R, class S>
+__device__ __forceinline__ R mass_jvp(const S& s, const PhysR<R>& p, int i, int j) {
+    const int ny = s.ny, nx = s.nx;
+    const R dxi = p.dxi;
+    const R Hc = s.Hc(i, j), phc = s.PHI(i, j), eHc = s.EH(i, j);
+    R dc, d = eHc * p.dti;
+    FluxT<R> f = lflux(s.U(i, j), s.Hc(i, j - 1), Hc, j, nx);
+    d -= (f.d_w * s.LU(i, j) + f.d_H0 * s.EH(i, j - 1) + f.d_H1 * eHc) * dxi;
+    calve(Hc, phc, s.PHI(i, j - 1), p.calving_rate, dc); d += dc * eHc * dxi;
+    f = lflux(s.U(i, j + 1), Hc, s.Hc(i, j + 1), j + 1, nx);
+    d += (f.d_w * s.LU(i, j + 1) + f.d_H0 * eHc + f.d_H1 * s.EH(i, j + 1)) * dxi;
+    calve(Hc, phc, s.PHI(i, j + 1), p.calving_rate, dc); d += dc * eHc * dxi;
+    f = lflux(s.V(i, j), Hc, s.Hc(i - 1, j), i, ny);
+    d += (f.d_w * s.LV(i, j) + f.d_H0 * eHc + f.d_H1 * s.EH(i - 1, j)) * dxi;
+    calve(Hc, phc, s.PHI(i - 1, j), p.calving_rate, dc); d += dc * eHc * dxi;
+    f = lflux(s.V(i + 1, j), s.Hc(i + 1, j), Hc, i + 1, ny);
+    d -= (f.d_w * s.LV(i + 1, j) + f.d_H0 * s.EH(i + 1, j) + f.d_H1 * eHc) * dxi;
+    calve(Hc, phc, s.PHI(i + 1, j), p.calving_rate, dc); d += dc * eHc * dxi;
+    return d;
+}
+
+// d(x-momentum row on u face (i,j)) . e (residuals.cu:441-548), interior rows
+template <class R, class S>
+__device__ __forceinline__ R umom_jvp(const S& s, const PhysR<R>& p, int i, int j) {
+    const int ny = s.ny, nx = s.nx;
+    const R dxi = p.dxi;
+    const R Hc = s.Hc(i, j), Hl = s.Hc(i, j - 1), ul = s.U(i, j);
+    R d = 0;
+    {
+        NormalT<R> a = sxx(ul, s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.ETA(i, j) * Hc, dxi, j, nx);
+        d += (a.d_ul * s.LU(i, j) + a.d_ur * s.LU(i, j + 1) + a.d_vt * s.LV(i, j) + a.d_vb * s.LV(i + 1, j) +
+              a.d_eH * (s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j))) * dxi;
+    }
+    {
+        NormalT<R> a = sxx(s.U(i, j - 1), ul, s.V(i, j - 1), s.V(i + 1, j - 1), s.ETA(i, j - 1) * Hl, dxi, j - 1, nx);
+        d -= (a.d_ul * s.LU(i, j - 1) + a.d_ur * s.LU(i, j) + a.d_vt * s.LV(i, j - 1) +
+              a.d_vb * s.LV(i + 1, j - 1) + a.d_eH * (s.ETAD(i, j - 1) * Hl + s.ETA(i, j - 1) * s.EH(i, j - 1))) * dxi;
+    }
+    {
+        R eH = vertex_eH(s.ETA(i - 1, j - 1), s.ETA(i - 1, j), s.ETA(i, j - 1), s.ETA(i, j), s.Hc(i - 1, j - 1),
+                         s.Hc(i - 1, j), Hl, Hc);
+        R deH = R(0.25) * (s.ETAD(i - 1, j - 1) * s.Hc(i - 1, j - 1) + s.ETA(i - 1, j - 1) * s.EH(i - 1, j - 1) +
+                           s.ETAD(i - 1, j) * s.Hc(i - 1, j) + s.ETA(i - 1, j) * s.EH(i - 1, j) +
+                           s.ETAD(i, j - 1) * Hl + s.ETA(i, j - 1) * s.EH(i, j - 1) +
+                           s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j));
+        ShearT<R> a = sxy(s.U(i - 1, j), ul, s.V(i, j - 1), s.V(i, j), eH, dxi, i, j, ny, nx);
+        d += (a.d_ut * s.LU(i - 1, j) + a.d_ub * s.LU(i, j) + a.d_vl * s.LV(i, j - 1) + a.d_vr * s.LV(i, j) +
+              a.d_eH * deH) * dxi;
+    }
+    {
+        R eH = vertex_eH(s.ETA(i, j - 1), s.ETA(i, j), s.ETA(i + 1, j - 1), s.ETA(i + 1, j), Hl, Hc,
+                         s.Hc(i + 1, j - 1), s.Hc(i + 1, j));
+        R deH = R(0.25) * (s.ETAD(i, j - 1) * Hl + s.ETA(i, j - 1) * s.EH(i, j - 1) + s.ETAD(i, j) * Hc +
+                           s.ETA(i, j) * s.EH(i, j) + s.ETAD(i + 1, j - 1) * s.Hc(i + 1, j - 1) +
+                           s.ETA(i + 1, j - 1) * s.EH(i + 1, j - 1) + s.ETAD(i + 1, j) * s.Hc(i + 1, j) +
+                           s.ETA(i + 1, j) * s.EH(i + 1, j));
+        ShearT<R> a = sxy(ul, s.U(i + 1, j), s.V(i + 1, j - 1), s.V(i + 1, j), eH, dxi, i + 1, j, ny, nx);
+        d -= (a.d_ut * s.LU(i, j) + a.d_ub * s.LU(i + 1, j) + a.d_vl * s.LV(i + 1, j - 1) +
+              a.d_vr * s.LV(i + 1, j) + a.d_eH * deH) * dxi;
+    }
+    {
+        BasalT<R> b = basal(ul, s.V(i, j - 1), s.V(i, j), s.V(i + 1, j - 1), s.V(i + 1, j), s.PHI(i, j - 1),
+                            s.PHI(i, j), s.BETA(i, j - 1), s.BETA(i, j), p);
+        d += b.d_w * s.LU(i, j) + b.d_a * s.LV(i, j - 1) + b.d_b * s.LV(i, j) + b.d_c * s.LV(i + 1, j - 1) +
+             b.d_d * s.LV(i + 1, j);
+    }
+    {
+        DriveT<R> dr = driving(Hl, Hc, s.BED(i, j - 1), s.BED(i, j), s.PHI(i, j - 1), s.PHI(i, j), dxi, j, nx);
+        d -= dr.d_H0 * s.EH(i, j - 1) + dr.d_H1 * s.EH(i, j);
+    }
+    return d;
+}
+
+// d(y-momentum row on v face (i,j)) . e (residuals.cu:551-658), interior rows
+template <class R, class S>
+__device__ __forceinline__ R vmom_jvp(const S& s, const PhysR<R>& p, int i, int j) {
+    const int ny = s.ny, nx = s.nx;
+    const R dxi = p.dxi;
+    const R Hc = s.Hc(i, j), Ht = s.Hc(i - 1, j), vt = s.V(i, j);
+    R d = 0;
+    {
+        NormalT<R> a = syy(s.U(i - 1, j), s.U(i - 1, j + 1), s.V(i - 1, j), vt, s.ETA(i - 1, j) * Ht, dxi, i - 1, ny);
+        d += (a.d_ul * s.LU(i - 1, j) + a.d_ur * s.LU(i - 1, j + 1) + a.d_vt * s.LV(i - 1, j) +
+              a.d_vb * s.LV(i, j) + a.d_eH * (s.ETAD(i - 1, j) * Ht + s.ETA(i - 1, j) * s.EH(i - 1, j))) * dxi;
+    }
+    {
+        NormalT<R> a = syy(s.U(i, j), s.U(i, j + 1), vt, s.V(i + 1, j), s.ETA(i, j) * Hc, dxi, i, ny);
+        d -= (a.d_ul * s.LU(i, j) + a.d_ur * s.LU(i, j + 1) + a.d_vt * s.LV(i, j) + a.d_vb * s.LV(i + 1, j) +
+              a.d_eH * (s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j))) * dxi;
+    }
+    {
+        R eH = vertex_eH(s.ETA(i - 1, j - 1), s.ETA(i - 1, j), s.ETA(i, j - 1), s.ETA(i, j), s.Hc(i - 1, j - 1), Ht,
+                         s.Hc(i, j - 1), Hc);
+        R deH = R(0.25) * (s.ETAD(i - 1, j - 1) * s.Hc(i - 1, j - 1) + s.ETA(i - 1, j - 1) * s.EH(i - 1, j - 1) +
+                           s.ETAD(i - 1, j) * Ht + s.ETA(i - 1, j) * s.EH(i - 1, j) +
+                           s.ETAD(i, j - 1) * s.Hc(i, j - 1) + s.ETA(i, j - 1) * s.EH(i, j - 1) +
+                           s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j));
+        ShearT<R> a = sxy(s.U(i - 1, j), s.U(i, j), s.V(i, j - 1), vt, eH, dxi, i, j, ny, nx);
+        d -= (a.d_ut * s.LU(i - 1, j) + a.d_ub * s.LU(i, j) + a.d_vl * s.LV(i, j - 1) + a.d_vr * s.LV(i, j) +
+              a.d_eH * deH) * dxi;
+    }
+    {
+        R eH = vertex_eH(s.ETA(i - 1, j), s.ETA(i - 1, j + 1), s.ETA(i, j), s.ETA(i, j + 1), Ht, s.Hc(i - 1, j + 1),
+                         Hc, s.Hc(i, j + 1));
+        R deH = R(0.25) * (s.ETAD(i - 1, j) * Ht + s.ETA(i - 1, j) * s.EH(i - 1, j) +
+                           s.ETAD(i - 1, j + 1) * s.Hc(i - 1, j + 1) + s.ETA(i - 1, j + 1) * s.EH(i - 1, j + 1) +
+                           s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j) + s.ETAD(i, j + 1) * s.Hc(i, j + 1) +
+                           s.ETA(i, j + 1) * s.EH(i, j + 1));
+        ShearT<R> a = sxy(s.U(i - 1, j + 1), s.U(i, j + 1), vt, s.V(i, j + 1), eH, dxi, i, j + 1, ny, nx);
+        d += (a.d_ut * s.LU(i - 1, j + 1) + a.d_ub * s.LU(i, j + 1) + a.d_vl * s.LV(i, j) +
+              a.d_vr * s.LV(i, j + 1) + a.d_eH * deH) * dxi;
+    }
+    {
+        BasalT<R> b = basal(vt, s.U(i - 1, j), s.U(i - 1, j + 1), s.U(i, j), s.U(i, j + 1), s.PHI(i - 1, j),
+                            s.PHI(i, j), s.BETA(i - 1, j), s.BETA(i, j), p);
+        d += b.d_w * s.LV(i, j) + b.d_a * s.LU(i - 1, j) + b.d_b * s.LU(i - 1, j + 1) + b.d_c * s.LU(i, j) +
+             b.d_d * s.LU(i, j + 1);
+    }
+    {
+        DriveT<R> dr = driving(Hc, Ht, s.BED(i, j), s.BED(i - 1, j), s.PHI(i, j), s.PHI(i - 1, j), dxi, i, ny);
+        d -= dr.d_H0 * s.EH(i, j) + dr.d_H1 * s.EH(i - 1, j);
+    }
+    return d;
+}
+
+// r_lin = J e - f (- sub) over one level, optional per-block sums of squares.
+// Uses VjpArgs with lu/lv/lH carrying e and f_* the right-hand side.
+template <class R>
+__global__ void __launch_bounds__(kTileA * kTileA) k_jvp(VjpArgs<R> a, int ref_rows) {
+    constexpr int NC = AdjTile<R>::NC;
+    __shared__ AdjTile<R> T;
+    __shared__ double red[3][kTileA * kTileA / 32];
+    const int i0 = blockIdx.y * kTileA, j0 = blockIdx.x * kTileA;
+    const int ny = a.ny, nx = a.nx;
+    stage_adjoint(T, i0, j0, a);
+    __syncthreads();
+    TanView<R> s{T, &a.lH, i0, j0, ny, nx};
+    for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
+        int r = k / NC, c = k % NC;
+        int gi = i0 - 2 + r, gj = j0 - 2 + c;
+        R Bc = a.B.at(clampi(gi, 0, ny - 1), clampi(gj, 0, nx - 1));
+        T.t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+        T.etad[r][c] = eta_dot_at<R>(s, Bc, a.p, gi, gj);
+    }
+    __syncthreads();
+    const int I = i0 + threadIdx.x / kTileA, J = j0 + threadIdx.x % kTileA;
+    double ssu = 0, ssv = 0, ssh = 0;
+    const bool f = a.use_forcing != 0;
+    auto emit = [&](Arr<R> o, const Arr<R>& fa, const Arr<R>& sa, int i, int j, R val, double& ss) {
+        R r = f ? val - fa.at(i, j) : val;
+        if (sa.p) r = r - sa.at(i, j);
+        o.at(i, j) = r;
+        ss += double(r) * double(r);
+    };
+    if (I < ny && J < nx) {
+        const R mk = a.mask.at(I, J);
+        R dH = mass_jvp<R>(s, a.p, I, J);
+        if (ref_rows) dH = (R(1) - mk) * dH;
+        else if (mk > R(0.5)) dH = s.EH(I, J);
+        emit(a.o_H, a.f_H, a.s_H, I, J, dH, ssh);
+        R du = (J == 0) ? (ref_rows ? R(0) : s.LU(I, 0)) : umom_jvp<R>(s, a.p, I, J);
+        emit(a.o_u, a.f_u, a.s_u, I, J, du, ssu);
+        if (J == nx - 1) emit(a.o_u, a.f_u, a.s_u, I, nx, ref_rows ? R(0) : s.LU(I, nx), ssu);
+        R dv = (I == 0) ? (ref_rows ? R(0) : s.LV(0, J)) : vmom_jvp<R>(s, a.p, I, J);
+        emit(a.o_v, a.f_v, a.s_v, I, J, dv, ssv);
+        if (I == ny - 1) emit(a.o_v, a.f_v, a.s_v, ny, J, ref_rows ? R(0) : s.LV(ny, J), ssv);
+    }
+    if (a.partial) {
+        for (int o = 16; o > 0; o >>= 1) {
+            ssu += __shfl_down_sync(0xffffffffu, ssu, o);
+            ssv += __shfl_down_sync(0xffffffffu, ssv, o);
+            ssh += __shfl_down_sync(0xffffffffu, ssh, o);
+        }
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0) { red[0][w] = ssu; red[1][w] = ssv; red[2][w] = ssh; }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double acc = 0;
+            for (int q = 0; q < kTileA * kTileA / 32; ++q) acc += red[threadIdx.x][q];
+            a.partial[size_t(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = acc;
+        }
+    }
+}
+
+}  // namespace glide

@@ -154,6 +154,68 @@ __global__ void k_axpby(Arr<R> a, Arr<R> b, Arr<R> c, R s, int rows, int cols) {
     if (i < rows && j < cols) a.at(i, j) = s * b.at(i, j) + (c.p ? c.at(i, j) : R(0));
 }
 
+// d = scale * src, converting the element type
+template <class D, class S>
+__global__ void k_convert(Arr<D> d, Arr<S> src, double scale, int rows, int cols) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < rows && j < cols) {
+        D v = D(src.at(i, j));
+        d.at(i, j) = scale == 1.0 ? v : D(scale) * v;
+    }
+}
+
+// d += src (src converted to d's type)
+template <class D, class S>
+__global__ void k_add_converted(Arr<D> d, Arr<S> src, int rows, int cols) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < rows && j < cols) d.at(i, j) = d.at(i, j) + D(src.at(i, j));
+}
+
+// Mixed-precision defect correction update of the state: x += y - fl(x) with
+// y the low-precision solution started from fl(x); the active set comes from
+// the low-precision smoother and masked thicknesses sit exactly on the floor.
+template <class D, class S>
+__global__ void k_defect_update(Arr<D> u, Arr<D> v, Arr<D> H, Arr<D> mask, Arr<D> gamma, Arr<S> uy,
+                                Arr<S> vy, Arr<S> Hy, Arr<S> masky, int ny, int nx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < ny && j <= nx) {
+        D x = u.at(i, j);
+        u.at(i, j) = x + (D(uy.at(i, j)) - D(S(x)));
+    }
+    if (i <= ny && j < nx) {
+        D x = v.at(i, j);
+        v.at(i, j) = x + (D(vy.at(i, j)) - D(S(x)));
+    }
+    if (i < ny && j < nx) {
+        const D m = D(masky.at(i, j));
+        D x = H.at(i, j);
+        H.at(i, j) = m > D(0.5) ? gamma.at(i, j) : x + (D(Hy.at(i, j)) - D(S(x)));
+        mask.at(i, j) = m;
+    }
+}
+
+// Right-hand side of the Newton correction, -r, in the tangent system's
+// precision; active cells take -(H - gamma) so that H + e_H = gamma.
+template <class T, class R>
+__global__ void k_tangent_rhs(Arr<T> fu, Arr<T> fv, Arr<T> fH, Arr<R> ru, Arr<R> rv, Arr<R> rH, Arr<R> H,
+                              Arr<R> gamma, Arr<R> mask, int ny, int nx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < ny && j <= nx) fu.at(i, j) = T(-ru.at(i, j));
+    if (i <= ny && j < nx) fv.at(i, j) = T(-rv.at(i, j));
+    if (i < ny && j < nx)
+        fH.at(i, j) = T(mask.at(i, j) > R(0.5) ? -(H.at(i, j) - gamma.at(i, j)) : -rH.at(i, j));
+}
+
+// Newton update x += e (e possibly in lower precision), thickness floored at gamma.
+template <class D, class S>
+__global__ void k_newton_update(Arr<D> u, Arr<D> v, Arr<D> H, Arr<D> gamma, Arr<S> eu, Arr<S> ev, Arr<S> eH,
+                                int ny, int nx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (i < ny && j <= nx) u.at(i, j) = u.at(i, j) + D(eu.at(i, j));
+    if (i <= ny && j < nx) v.at(i, j) = v.at(i, j) + D(ev.at(i, j));
+    if (i < ny && j < nx) H.at(i, j) = fmax(H.at(i, j) + D(eH.at(i, j)), gamma.at(i, j));
+}
+
 template <class R>
 __global__ void k_fill(Arr<R> a, R val, int rows, int cols) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;

@@ -36,18 +36,24 @@ class _DeviceBuffer:
 
 class Hierarchy:
     def __init__(self, ny: int, nx: int, dx: float, n_levels: int, dtype=torch.float64,
-                 reference_quirks: bool = True, use_graphs: bool = True):
+                 reference_quirks: bool = True, use_graphs: bool = True, precision: str | None = None):
+        """precision: "fp64" (default for float64), "fp32", or "mixed" (binary64
+        fields and residuals, binary32 smoother and coarse levels)."""
         if not torch.cuda.is_available():
             raise _lib.GlideError(_lib.GLIDE_ERR_STATE, "glide_b200 needs a CUDA device (sm_100a)")
-        if dtype not in (torch.float64, torch.float32):
-            raise TypeError("dtype must be torch.float64 or torch.float32")
+        if precision is None:
+            precision = "fp64" if dtype == torch.float64 else "fp32"
+        codes = {"fp64": _lib.GLIDE_F64, "fp32": _lib.GLIDE_F32, "mixed": _lib.GLIDE_MIXED}
+        if precision not in codes:
+            raise ValueError("precision must be 'fp64', 'fp32' or 'mixed'")
+        dtype = torch.float32 if precision == "fp32" else torch.float64
         self.dtype = dtype
+        self.precision = precision
         self.n_levels = n_levels
         lib = _lib.load()
         h = ctypes.c_void_p()
         torch.cuda.init()
-        _lib.check(lib.glide_create(int(ny), int(nx), float(dx), int(n_levels),
-                                    _lib.GLIDE_F64 if dtype == torch.float64 else _lib.GLIDE_F32,
+        _lib.check(lib.glide_create(int(ny), int(nx), float(dx), int(n_levels), codes[precision],
                                     ctypes.byref(h)))
         self._h = h
         self._views = {}
@@ -155,9 +161,23 @@ class Hierarchy:
     def set_use_graphs(self, on: bool):
         call("glide_set_use_graphs", self._h, int(bool(on)))
 
-    def set_tuning(self, sweep_blocks_per_sm: int | None = None):
+    def set_tuning(self, sweep_blocks_per_sm: int | None = None, mixed_inner_vcycles: int | None = None,
+                   forward_method: str | None = None, newton_switch_exp10: int | None = None,
+                   tangent_vcycles: int | None = None):
+        """Solver knobs with no counterpart in the reference (see glide_set_tuning).
+        forward_method: "fascd" (the reference's V-cycles only) or "newton"
+        (FASCD until 10^-newton_switch_exp10, then Newton steps whose correction
+        comes from the tangent linear multigrid)."""
         if sweep_blocks_per_sm is not None:
             call("glide_set_tuning", self._h, 1, int(sweep_blocks_per_sm))
+        if mixed_inner_vcycles is not None:
+            call("glide_set_tuning", self._h, 2, int(mixed_inner_vcycles))
+        if forward_method is not None:
+            call("glide_set_tuning", self._h, 3, {"fascd": 0, "newton": 1}[forward_method])
+        if newton_switch_exp10 is not None:
+            call("glide_set_tuning", self._h, 4, int(newton_switch_exp10))
+        if tangent_vcycles is not None:
+            call("glide_set_tuning", self._h, 5, int(tangent_vcycles))
 
     def launch_count(self) -> int:
         c = ctypes.c_longlong()
@@ -192,6 +212,9 @@ class Hierarchy:
 
     def vjp(self, level: int, dt: float):
         call("glide_vjp", self._h, int(level), float(dt), _stream_ptr())
+
+    def jvp(self, level: int, dt: float, reference_rows: bool = True):
+        call("glide_jvp", self._h, int(level), float(dt), int(bool(reference_rows)), _stream_ptr())
 
     def adjoint_sweep(self, level: int, dt: float, n: int):
         call("glide_adjoint_sweep", self._h, int(level), float(dt), int(n), _stream_ptr())

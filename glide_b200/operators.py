@@ -93,6 +93,19 @@ class ForwardOperators:
     F_v = property(lambda s: s._v("F_v"))
     F_H = property(lambda s: s._v("F_H"))
     gamma = property(lambda s: s._v("gamma"))
+    var_u = property(lambda s: s._v("var_u"))
+    var_v = property(lambda s: s._v("var_v"))
+    var_H = property(lambda s: s._v("var_H"))
+    jvp_u = property(lambda s: s._v("jvp_u"))
+    jvp_v = property(lambda s: s._v("jvp_v"))
+    jvp_H = property(lambda s: s._v("jvp_H"))
+
+    def compute_jvp(self, dt, use_mask=True, freeze_calving=False, freeze_phi=False, return_norms=False):
+        """jvp = J(x) var with the reference's row conventions
+        (glide/operators.py:129-171); phi is recomputed first unless frozen."""
+        if not freeze_phi:
+            self.compute_phi()
+        self._h.jvp(self._l, dt, reference_rows=True)
 
     def compute_residual(self, dt, use_mask=True, operator_only=False, freeze_calving=False,
                          freeze_phi=False, return_norms=False):

@@ -46,12 +46,16 @@ extern "C" {
 
 #define GLIDE_F64 0
 #define GLIDE_F32 1
+/* binary64 fields and residuals, binary32 smoother and coarse levels
+ * (nonlinear defect correction); fields are accessed as binary64 */
+#define GLIDE_MIXED 2
 
 /* Field identifiers.  Face fields: U (ny, nx+1), V (ny+1, nx); all others are
  * cell fields (ny, nx).  ADJ_* are the adjoint operators' arrays, GRAD_* the
  * gradients written by glide_gradients / glide_backward, VJP_* the plain
  * transpose product written by glide_vjp, FOP_* the operator without forcing
- * written by glide_residual(GLIDE_OPERATOR_ONLY). */
+ * written by glide_residual(GLIDE_OPERATOR_ONLY), VAR_* the direction and
+ * JVP_* the Jacobian-vector product of glide_jvp. */
 enum glide_field {
     GLIDE_U = 0, GLIDE_V, GLIDE_H, GLIDE_H_PREV, GLIDE_PHI, GLIDE_MASK,
     GLIDE_BED, GLIDE_B, GLIDE_BETA, GLIDE_SMB, GLIDE_GAMMA,
@@ -63,6 +67,8 @@ enum glide_field {
     GLIDE_GRAD_BETA, GLIDE_GRAD_BED, GLIDE_GRAD_H_PREV, GLIDE_GRAD_SMB,
     GLIDE_VJP_U, GLIDE_VJP_V, GLIDE_VJP_H,
     GLIDE_FOP_U, GLIDE_FOP_V, GLIDE_FOP_H,
+    GLIDE_VAR_U, GLIDE_VAR_V, GLIDE_VAR_H,
+    GLIDE_JVP_U, GLIDE_JVP_V, GLIDE_JVP_H,
     GLIDE_N_PUBLIC_FIELDS
 };
 
@@ -126,10 +132,12 @@ int glide_fill_field(glide_handle h, int field, int level, double value, int res
 int glide_restrict_field(glide_handle h, int field, int level, void* stream);
 int glide_set_phys(glide_handle h, int level, const glide_phys* p);
 int glide_get_phys(glide_handle h, int level, glide_phys* p);
-int glide_set_fas_config(glide_handle h, int adjoint, const glide_fas_config* c);
-int glide_get_fas_config(glide_handle h, int adjoint, glide_fas_config* c);
-int glide_set_vanka_config(glide_handle h, int adjoint, int level, const glide_vanka_config* c);
-int glide_get_vanka_config(glide_handle h, int adjoint, int level, glide_vanka_config* c);
+/* `which`: 0 forward FASCD, 1 FASAdjoint, 2 tangent linear multigrid of the
+ * Newton correction (no counterpart in the reference). */
+int glide_set_fas_config(glide_handle h, int which, const glide_fas_config* c);
+int glide_get_fas_config(glide_handle h, int which, glide_fas_config* c);
+int glide_set_vanka_config(glide_handle h, int which, int level, const glide_vanka_config* c);
+int glide_get_vanka_config(glide_handle h, int which, int level, glide_vanka_config* c);
 /* on = 1 reproduces the reference's v-face prolongation (its u-face kernel
  * run on v arrays, glide/multigrid.py:212-235; square grids only). */
 int glide_set_reference_quirks(glide_handle h, int on);
@@ -139,8 +147,20 @@ int glide_set_use_graphs(glide_handle h, int use_graphs);
  * every kernel node).  No counterpart in the reference: instrumentation. */
 int glide_launch_count(glide_handle h, long long* count);
 /* Kernel tuning knobs (no counterpart in the reference).
- * GLIDE_TUNE_SWEEP_BLOCKS_PER_SM: 1 or 2 resident Vanka-sweep blocks per SM. */
+ * GLIDE_TUNE_SWEEP_BLOCKS_PER_SM: 1 or 2 resident Vanka-sweep blocks per SM.
+ * GLIDE_TUNE_MIXED_INNER_VCYCLES: binary32 V-cycles per defect correction
+ * of a GLIDE_MIXED handle (default 1). */
 #define GLIDE_TUNE_SWEEP_BLOCKS_PER_SM 1
+#define GLIDE_TUNE_MIXED_INNER_VCYCLES 2
+/* GLIDE_TUNE_FORWARD_METHOD: 0 = FASCD V-cycles only (the reference's
+ * method); 1 = FASCD until the relative residual reaches 10^-k
+ * (GLIDE_TUNE_NEWTON_SWITCH_EXP10 = k, default 2), then Newton steps whose
+ * correction is solved by GLIDE_TUNE_TANGENT_VCYCLES V-cycles (default 1) of
+ * the tangent linear multigrid (schedule and smoother: config selector 2).
+ * GLIDE_MIXED handles default to 1. */
+#define GLIDE_TUNE_FORWARD_METHOD 3
+#define GLIDE_TUNE_NEWTON_SWITCH_EXP10 4
+#define GLIDE_TUNE_TANGENT_VCYCLES 5
 int glide_set_tuning(glide_handle h, int key, int value);
 
 int glide_set_rhs(glide_handle h, int level, double dt, void* stream);
@@ -152,6 +172,12 @@ int glide_forward(glide_handle h, double dt, int start_level, glide_stats* stats
 
 int glide_adjoint_residual(glide_handle h, int level, double dt, double* norms3, void* stream);
 int glide_vjp(glide_handle h, int level, double dt, void* stream);
+/* JVP_* = J(x) VAR_* at the level's state with the grounded fraction held
+ * fixed.  reference_rows = 1 follows ForwardOperators.compute_jvp
+ * (glide/operators.py:129-171, glide/cuda/residuals.cu:341-660): zero on the
+ * Dirichlet faces, (1 - mask) times the mass rows.  reference_rows = 0 gives
+ * the Jacobian the Newton iteration uses (identity rows there). */
+int glide_jvp(glide_handle h, int level, double dt, int reference_rows, void* stream);
 int glide_adjoint_sweep(glide_handle h, int level, double dt, int n, void* stream);
 int glide_gradients(glide_handle h, int level, double dt, int grad_mask, void* stream);
 int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, glide_stats* stats,

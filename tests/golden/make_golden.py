@@ -114,6 +114,23 @@ def random_cases(glide):
         out[f"out_{k}"] = np.array(getattr(g.state, k).data)
     np.savez_compressed(HERE / "random_vanka_f64.npz", **out)
 
+    # forward-mode derivative (ForwardOperators.compute_jvp)
+    rng = np.random.default_rng(5)
+    ny, nx = st["H"].shape
+    var = dict(var_u=rng.normal(0, 1, (ny, nx + 1)), var_v=rng.normal(0, 1, (ny + 1, nx)),
+               var_H=rng.normal(0, 10, (ny, nx)))
+    out = {f"in_{k}": v for k, v in {**st, **var}.items()}
+    g = random_grid(glide, st)
+    ops = g.forward_operators
+    ops.set_rhs(dt)
+    for k, v in var.items():
+        getattr(ops, k)[:, :] = v
+    ops.compute_jvp(dt)
+    for k in ("jvp_u", "jvp_v", "jvp_H"):
+        out[f"out_{k}"] = np.array(getattr(ops, k))
+    out["out_phi"] = np.array(g.state.phi.data)
+    np.savez_compressed(HERE / "random_jvp_f64.npz", **out)
+
     rng = np.random.default_rng(11)
     ny, nx = st["H"].shape
     lam = dict(lambda_u=rng.normal(0, 1, (ny, nx + 1)), lambda_v=rng.normal(0, 1, (ny + 1, nx)),
