@@ -123,6 +123,9 @@ SIGNATURES = {
     "glide_adjoint_sweep": ([_H, _I, _D, _I, _P], _I),
     "glide_gradients": ([_H, _I, _D, _I, _P], _I),
     "glide_backward": ([_H, _D, _I, _I, ctypes.POINTER(Stats), _P], _I),
+    "glide_residual_norms_noalloc": ([_I, _I, _D, _D, ctypes.POINTER(Phys), _P, _I, _P, _I, _P, _P, _P,
+                                      _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P], _I),
+    "glide_noalloc_last_error": ([], ctypes.c_char_p),
 }
 
 _LIB = None

@@ -20,6 +20,7 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libglide_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+UNITS = ["runtime.cu", "noalloc.cu"]
 
 
 def nvcc() -> str:
@@ -44,7 +45,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     OUT_DIR.mkdir(exist_ok=True)
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
            "-Xcompiler", "-fPIC", "-shared", "-I", str(ROOT / "include"), "-I", str(CSRC),
-           str(CSRC / "runtime.cu"), "-o", str(LIB) + ".tmp", "-lcudart"]
+           *[str(CSRC / f) for f in UNITS], "-o", str(LIB) + ".tmp", "-lcudart"]
     if verbose_ptxas:
         cmd.insert(1, "-Xptxas=-v")
     print(" ".join(cmd), flush=True)
