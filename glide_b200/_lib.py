@@ -128,6 +128,43 @@ SIGNATURES = {
     "glide_noalloc_last_error": ([], ctypes.c_char_p),
 }
 
+class EnthalpyConfig(ctypes.Structure):
+    _fields_ = [("omega", ctypes.c_double), ("n_newton", ctypes.c_int), ("relaxation", ctypes.c_double),
+                ("relative_tolerance", ctypes.c_double), ("absolute_tolerance", ctypes.c_double),
+                ("lf_c", ctypes.c_double), ("drain_rate", ctypes.c_double), ("h_thin", ctypes.c_double),
+                ("term_flags", ctypes.c_int)]
+
+
+class EnthalpyInputs(ctypes.Structure):
+    _fields_ = [("H", ctypes.c_void_p), ("ld_H", ctypes.c_int), ("u", ctypes.c_void_p), ("ld_u", ctypes.c_int),
+                ("u_layer", ctypes.c_longlong), ("v", ctypes.c_void_p), ("ld_v", ctypes.c_int),
+                ("v_layer", ctypes.c_longlong), ("vel_div", ctypes.c_double)]
+
+
+class EnthalpyStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("initial_norm", ctypes.c_double), ("final_norm", ctypes.c_double),
+                ("history", ctypes.c_double * 256)]
+
+
+SIGNATURES.update({
+    "glide_enthalpy_last_error": ([], ctypes.c_char_p),
+    "glide_enthalpy_create": ([_I, _I, _I, _D, ctypes.POINTER(_H)], _I),
+    "glide_enthalpy_destroy": ([_H], _I),
+    "glide_enthalpy_field_ptr": ([_H, _I, ctypes.POINTER(_P)], _I),
+    "glide_enthalpy_set_config": ([_H, ctypes.POINTER(EnthalpyConfig)], _I),
+    "glide_enthalpy_get_config": ([_H, ctypes.POINTER(EnthalpyConfig)], _I),
+    "glide_enthalpy_set_inputs": ([_H, ctypes.POINTER(EnthalpyInputs)], _I),
+    "glide_enthalpy_snapshot": ([_H, _P], _I),
+    "glide_enthalpy_set_rhs": ([_H, _P], _I),
+    "glide_enthalpy_residual": ([_H, _D, _I, ctypes.POINTER(_D), _P], _I),
+    "glide_enthalpy_column_smooth": ([_H, _D, _P], _I),
+    "glide_enthalpy_layer_smooth": ([_H, _D, _P], _I),
+    "glide_enthalpy_column_sweep": ([_H, _D, _I, _I, ctypes.POINTER(EnthalpyStats), _P], _I),
+    "glide_enthalpy_compute_omega": ([_H, _P, _I, _P, _I, _D, _D, _P], _I),
+    "glide_enthalpy_frictional_heating": ([_H, _P, _I, _D, _D, _P], _I),
+    "glide_enthalpy_arrhenius": ([_H, _D, _D, _P, _I, _P], _I),
+})
+
 _LIB = None
 
 

@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libglide_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-UNITS = ["runtime.cu", "noalloc.cu"]
+UNITS = ["runtime.cu", "noalloc.cu", "enthalpy.cu"]
 
 
 def nvcc() -> str:

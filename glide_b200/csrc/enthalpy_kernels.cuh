@@ -1,0 +1,530 @@
+// enthalpy_kernels.cuh -- the conservative enthalpy column solver
+// (glide/cuda/enthalpy.cu and glide/enthalpy.py of JacobDowns/glide), binary64.
+//
+// Layout in HBM: every 3-D node array is layer-major, node (k, i, j) at
+// k * plane + i * nx + j (plane = ny * nx).  One thread owns one column
+// (i, j) and walks k, so each k step of a warp reads 32 consecutive columns:
+// coalesced for every array.  Layer velocities are read with a layer stride;
+// stride 0 reads one 2-D field for all layers (the SSA depth-averaged
+// velocity, which the reference copies into nz layers).
+//
+// The reference compiles these kernels with its constants injected as binary32
+// literals (glide/enthalpy.py:229-246); products of those literals fold in
+// binary32.  The constants below are those binary32 values widened, and the
+// folded products are formed in binary32 the same way.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace glide {
+namespace enth {
+
+constexpr int kMaxNz = 64;
+constexpr int kColThreads = 128;
+
+constexpr float fRHO_I = 910.0f, fRHO_W = 1000.0f, fC_I = 2009.0f, fK_I = 2.1f, fL_HEAT = 334000.0f;
+constexpr float fT_REF = 223.15f, fT_MELT = 273.15f, fBETA_CC = 7.9e-08f, fGRAVITY = 9.81f;
+constexpr float fK_TEMP_FACTOR = 0.1f, fMASS_FLUX_REG = 1.00413490930961e-14f, fMASS_FLUX_REG_YR = 10.0f;
+
+constexpr double kRhoI = fRHO_I, kRhoW = fRHO_W, kCI = fC_I, kL = fL_HEAT, kTRef = fT_REF, kTMelt = fT_MELT;
+constexpr double kKTF = fK_TEMP_FACTOR, kReg = fMASS_FLUX_REG, kRegYr = fMASS_FLUX_REG_YR;
+constexpr double kKCold = double(fK_I / fC_I);                    // (K_I/C_I)
+constexpr double kEScale = double(fC_I * (fT_MELT - fT_REF));     // (C_I * (T_MELT - T_REF))
+constexpr double kCcRhoG = double(fBETA_CC * fRHO_I * fGRAVITY);  // BETA_CC * RHO_I * GRAVITY
+constexpr double kSharp = double(0.01f);                          // K(E) and drainage sharpness
+
+enum { kTermHorizAdv = 1, kTermSigmaDot = 2, kTermDrainage = 4 };
+
+struct EnthArgs {
+    const double* E;       // state read (layer-major)
+    const double* E_prev;
+    const double* f_E;
+    const double* omega;
+    const double* u;       // layer velocity, u[k * u_layer + i * ld_u + j]
+    const double* v;
+    const double* H;       // (ny, nx) with leading dimension ld_h
+    const double* H_prev;  // (ny, nx) contiguous
+    const double* E_s;     // (ny, nx) contiguous
+    long long u_layer, v_layer;
+    int ld_u, ld_v, ld_h;
+    double vel_div;        // velocities are divided by this on read
+    double dx, dt, drain, h_thin, lf_c;
+    double omega_relax;    // smoother update weight (ColumnSmootherConfig.omega)
+    double relaxation;     // Newton step length
+    int flags, ny, nx, nz, n_newton;
+    const int* done;       // sweep stop flag (nullptr: always run)
+};
+
+// ---------------------------------------------------------------- terms
+// enthalpy.cu:49-56
+__device__ __forceinline__ double e_pmp(double sigma, double H) {
+    double depth = (1.0 - sigma) * H;
+    double T_pmp = kTMelt - kCcRhoG * depth;
+    return kCI * (T_pmp - kTRef) / kEScale;
+}
+
+// enthalpy.cu:60-66
+__device__ __forceinline__ double k_diff(double E, double Ep) {
+    double z = (E - Ep) * kEScale * kSharp;
+    z = fmin(fmax(z, -20.0), 20.0);
+    double s = 1.0 / (1.0 + exp(-z));
+    return kKCold * (1.0 - s + kKTF * s);
+}
+
+// drainage residual and derivative (enthalpy.cu:71-91, :598-640)
+struct Drain { double res, d; };
+__device__ __forceinline__ Drain drainage(double Ek, double Ep, double drain, double h) {
+    double x = (Ek - Ep) * kEScale;
+    double ax = fmin(fmax(kSharp * x, -20.0), 20.0);
+    double sp = (ax > 10.0) ? x : log(1.0 + exp(ax)) / kSharp;
+    double z = fmin(fmax(kSharp * (Ek - Ep) * kEScale, -20.0), 20.0);
+    double s = 1.0 / (1.0 + exp(-z));
+    return {h * kRhoW * kL * (drain * (sp / kL)) / kEScale, h * kRhoW * kL * drain * (s / kL)};
+}
+
+// Lax-Friedrichs enthalpy flux through a face with mass flux q (enthalpy.cu:573-592)
+struct Flux { double res, dl, dr; };
+__device__ __forceinline__ Flux face_flux(double q, double El, double Er, double lf_c) {
+    double alpha = fabs(q) * sqrt(1.0 + lf_c);
+    return {0.5 * q * (El + Er) - 0.5 * alpha * (Er - El), 0.5 * (q + alpha), 0.5 * (q - alpha)};
+}
+
+// Per-column horizontal context: thicknesses of the column and its four
+// neighbours and which faces are interior.
+struct ColumnCtx {
+    int i, j;
+    size_t c;              // column offset i * nx + j
+    double h, h_prev, h_inv;
+    double Hxm, Hxp, Hym, Hyp;
+};
+
+__device__ __forceinline__ ColumnCtx column_ctx(const EnthArgs& a, int i, int j) {
+    ColumnCtx x;
+    x.i = i; x.j = j;
+    x.c = size_t(i) * a.nx + j;
+    const double* H = a.H;
+    x.h = H[size_t(i) * a.ld_h + j];
+    x.h_prev = a.H_prev[x.c];
+    x.h_inv = 1.0 / x.h;
+    x.Hxm = j > 0 ? H[size_t(i) * a.ld_h + j - 1] : 0.0;
+    x.Hxp = j < a.nx - 1 ? H[size_t(i) * a.ld_h + j + 1] : 0.0;
+    x.Hym = i > 0 ? H[size_t(i - 1) * a.ld_h + j] : 0.0;
+    x.Hyp = i < a.ny - 1 ? H[size_t(i + 1) * a.ld_h + j] : 0.0;
+    return x;
+}
+
+// Conservative horizontal advection at (i, j, k) with centre value Ec; the
+// neighbours come from the state array (enthalpy.cu:667-759).
+struct HAdv { double res, diag; };
+__device__ __forceinline__ HAdv horiz(const EnthArgs& a, const ColumnCtx& x, int k, double Ec) {
+    const size_t plane = size_t(a.ny) * a.nx;
+    const double* Ek = a.E + size_t(k) * plane;
+    const double* uk = a.u + k * a.u_layer + size_t(x.i) * a.ld_u;
+    const double* vk = a.v + k * a.v_layer;
+    Flux fl{0, 0, 0}, fr{0, 0, 0}, ft{0, 0, 0}, fb{0, 0, 0};
+    if (x.j > 0) {
+        double ul = uk[x.j] / a.vel_div;
+        double q = 0.5 * (x.Hxm + x.h) * ul - 0.5 * sqrt(ul * ul + kReg) * (x.h - x.Hxm);
+        fl = face_flux(q, Ek[x.c - 1], Ec, a.lf_c);
+    } else {
+        fl = face_flux(0.0, Ec, Ec, a.lf_c);
+    }
+    if (x.j < a.nx - 1) {
+        double ur = uk[x.j + 1] / a.vel_div;
+        double q = 0.5 * (x.h + x.Hxp) * ur - 0.5 * sqrt(ur * ur + kReg) * (x.Hxp - x.h);
+        fr = face_flux(q, Ec, Ek[x.c + 1], a.lf_c);
+    } else {
+        fr = face_flux(0.0, Ec, Ec, a.lf_c);
+    }
+    if (x.i > 0) {
+        double vt = vk[size_t(x.i) * a.ld_v + x.j] / a.vel_div;
+        double q = 0.5 * (x.Hym + x.h) * vt - 0.5 * sqrt(vt * vt + kReg) * (x.Hym - x.h);
+        ft = face_flux(q, Ec, Ek[x.c - a.nx], a.lf_c);
+    } else {
+        ft = face_flux(0.0, Ec, Ec, a.lf_c);
+    }
+    if (x.i < a.ny - 1) {
+        double vb = vk[size_t(x.i + 1) * a.ld_v + x.j] / a.vel_div;
+        double q = 0.5 * (x.h + x.Hyp) * vb - 0.5 * sqrt(vb * vb + kReg) * (x.h - x.Hyp);
+        fb = face_flux(q, Ek[x.c + a.nx], Ec, a.lf_c);
+    } else {
+        fb = face_flux(0.0, Ec, Ec, a.lf_c);
+    }
+    const double dx_inv = 1.0 / a.dx;
+    return {kRhoI * ((fr.res - fl.res) + (ft.res - fb.res)) * dx_inv,
+            kRhoI * ((fr.dl - fl.dr) + (ft.dl - fb.dr)) * dx_inv};
+}
+
+// Vertical terms of row k < nz - 1: sigma advection, diffusion, drainage with
+// their tridiagonal coefficients (enthalpy.cu:217-509).  K_lo / K_up are the
+// diffusivities of the interfaces below and above node k, which the caller
+// carries from row to row (the reference evaluates each twice, from the same
+// arguments).
+struct Vert { double adv, dif, drn; double a, b_dif, b_adv, b_drn, c; };
+
+__device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, double Ek, double Ekp1,
+                                         double Epk, double K_lo, double K_up, double om_m, double om_k,
+                                         double om_p, double h, double h_inv, double dsig) {
+    Vert r{0, 0, 0, 0, 0, 0, 0, 0};
+    if (k == 0) {
+        const double dsh = 0.5 * dsig, dsh_inv = 1.0 / dsh;
+        if (a.flags & kTermSigmaDot) {
+            double wh = 0.5 * (om_k + om_p);
+            double wp = fmax(wh, 0.0), wn = fmin(wh, 0.0);
+            double Fu = wp * Ek + wn * Ekp1, Fb = om_k * Ek;
+            r.adv = kRhoI * (Fu - Fb) * dsh_inv;
+            r.b_adv = kRhoI * (wp - om_k) * dsh_inv;
+            r.c = kRhoI * wn * dsh_inv;
+        }
+        r.dif = (-h_inv * K_up * (Ekp1 - Ek) / dsig - 0.0) / dsh;
+        double coeff = h_inv * K_up / (dsig * dsh);
+        r.b_dif = coeff;
+        r.c += -coeff;
+    } else {
+        const double di = 1.0 / dsig;
+        if (a.flags & kTermSigmaDot) {
+            double wu = 0.5 * (om_k + om_p), wl = 0.5 * (om_m + om_k);
+            double up = fmax(wu, 0.0), un = fmin(wu, 0.0), lp = fmax(wl, 0.0), ln = fmin(wl, 0.0);
+            double Fu = up * Ek + un * Ekp1, Fl = lp * Ekm1 + ln * Ek;
+            r.adv = kRhoI * (Fu - Fl) * di;
+            r.a = -kRhoI * lp * di;
+            r.c = kRhoI * un * di;
+            r.b_adv = kRhoI * (up - ln) * di;
+        }
+        const double d2 = 1.0 / (dsig * dsig);
+        r.dif = -h_inv * d2 * (K_up * (Ekp1 - Ek) - K_lo * (Ek - Ekm1));
+        double dl = h_inv * d2 * K_lo, du = h_inv * d2 * K_up;
+        r.a += -dl;
+        r.c += -du;
+        r.b_dif = dl + du;
+    }
+    if (a.flags & kTermDrainage) {
+        Drain d = drainage(Ek, Epk, a.drain, h);
+        r.drn = d.res;
+        r.b_drn = d.d;
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool stopped(const int* done) { return done && *(volatile const int*)done; }
+
+// ------------------------------------------------------------- residual
+// enthalpy.cu:784-893.  out (layer-major) = F(E) - f_E, or F(E) without
+// forcing; partial[block] = max |out| over the block's nodes.
+__global__ void __launch_bounds__(kColThreads) k_enth_residual(EnthArgs a, double* out, int use_forcing,
+                                                                  double* partial) {
+    __shared__ double red[kColThreads / 32];
+    if (stopped(a.done)) return;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    double mx = 0.0;
+    if (col < a.ny * a.nx) {
+        const int i = col / a.nx, j = col % a.nx;
+        const ColumnCtx x = column_ctx(a, i, j);
+        if (x.h < a.h_thin) {
+            for (int k = 0; k < nz; ++k) out[k * plane + x.c] = 0.0;
+        } else {
+            const double dsig = 1.0 / double(nz - 1), inv_dt = 1.0 / a.dt;
+            const double* E = a.E + x.c;
+            const double* om = a.omega + x.c;
+            double Ekm1 = 0.0, Ek = E[0], Ekp1 = E[plane];
+            double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
+            double K_lo = 0.0;
+            double om_m = 0.0, om_k = om[0];
+            for (int k = 0; k < nz - 1; ++k) {
+                const double om_p = om[size_t(k + 1) * plane];
+                const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp));
+                double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[k * plane + x.c]) * inv_dt;
+                if (a.flags & kTermHorizAdv) r += horiz(a, x, k, Ek).res;
+                Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig);
+                r += vt.adv;
+                r += vt.dif;
+                r += vt.drn;
+                if (use_forcing) r = r - a.f_E[k * plane + x.c];
+                out[k * plane + x.c] = r;
+                mx = fmax(mx, fabs(r));
+                // slide the window
+                Ekm1 = Ek; Ek = Ekp1;
+                Ekp1 = (k + 2 < nz) ? E[size_t(k + 2) * plane] : 0.0;
+                Epk = Epp;
+                Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
+                K_lo = K_up;
+                om_m = om_k; om_k = om_p;
+            }
+            out[size_t(nz - 1) * plane + x.c] = 0.0;
+        }
+    }
+    if (partial) {
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = red[0];
+            for (int q = 1; q < kColThreads / 32; ++q) m = fmax(m, red[q]);
+            partial[blockIdx.x] = m;
+        }
+    }
+}
+
+// --------------------------------------------------------- column smoother
+// enthalpy.cu:933-1112: per column, n_newton damped Newton steps on the
+// column with the horizontal neighbours frozen, each a tridiagonal (Thomas)
+// solve.  mode 0 writes delta_E = E_col - E; mode 1 writes the updated state
+// E + omega_relax (E_col - E).  Rows are assembled and eliminated in one
+// upward pass (Thomas in its c', d' form), then back-substituted.
+__global__ void __launch_bounds__(kColThreads) k_enth_column(EnthArgs a, double* out, int mode) {
+    if (stopped(a.done)) return;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ny * a.nx) return;
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    const int i = col / a.nx, j = col % a.nx;
+    const ColumnCtx x = column_ctx(a, i, j);
+    const double* E = a.E + x.c;
+    const double dsig = 1.0 / double(nz - 1);
+    const double Es = a.E_s[x.c];
+    double El[kMaxNz], cp[kMaxNz], dp[kMaxNz];
+    if (x.h < a.h_thin) {
+        // thin ice: driven to min(E_surface, E_pmp) (enthalpy.cu:963-973)
+        for (int k = 0; k < nz; ++k) {
+            double Ek = E[size_t(k) * plane];
+            double d = fmin(Es, e_pmp(k * dsig, x.h)) - Ek;
+            out[size_t(k) * plane + x.c] = mode ? Ek + a.omega_relax * d : d;
+        }
+        return;
+    }
+    for (int k = 0; k < nz; ++k) El[k] = E[size_t(k) * plane];
+    const double inv_dt = 1.0 / a.dt;
+    const double* om = a.omega + x.c;
+    const double bt = kRhoI * x.h * inv_dt;  // time-term diagonal
+    for (int it = 0; it < a.n_newton; ++it) {
+        double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
+        double K_lo = 0.0, om_m = 0.0, om_k = om[0];
+        double c_prev = 0.0, d_prev = 0.0;
+        for (int k = 0; k < nz - 1; ++k) {
+            const double Ek = El[k], Ekp1 = El[k + 1], Ekm1 = k > 0 ? El[k - 1] : 0.0;
+            const double om_p = om[size_t(k + 1) * plane];
+            const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp));
+            const size_t n = size_t(k) * plane + x.c;
+            double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[n]) * inv_dt - a.f_E[n];
+            double hd = 0.0;
+            if (a.flags & kTermHorizAdv) {
+                HAdv ha = horiz(a, x, k, Ek);
+                r += ha.res;
+                hd = ha.diag;
+            }
+            Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig);
+            r += vt.adv;
+            r += vt.dif;
+            r += vt.drn;
+            const double b = bt + vt.b_dif + vt.b_adv + vt.b_drn + hd;
+            // elimination: b' = b - a c'_{k-1}; c'_k = c / b'; d'_k = (rhs - a d'_{k-1}) / b'
+            const double bp = b - vt.a * c_prev;
+            const double inv = 1.0 / bp;
+            c_prev = vt.c * inv;
+            d_prev = (-r - vt.a * d_prev) * inv;
+            cp[k] = c_prev;
+            dp[k] = d_prev;
+            Epk = Epp;
+            Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
+            K_lo = K_up;
+            om_m = om_k; om_k = om_p;
+        }
+        // surface Dirichlet row: E = E_surface (a = c = 0, b = 1)
+        double xk = -(El[nz - 1] - Es);
+        El[nz - 1] += a.relaxation * xk;
+        for (int k = nz - 2; k >= 0; --k) {
+            xk = dp[k] - cp[k] * xk;
+            El[k] += a.relaxation * xk;
+        }
+    }
+    for (int k = 0; k < nz; ++k) {
+        const double Ek = E[size_t(k) * plane];
+        const double d = El[k] - Ek;
+        out[size_t(k) * plane + x.c] = mode ? Ek + a.omega_relax * d : d;
+    }
+}
+
+// ---------------------------------------------------------- layer smoother
+// enthalpy.cu:1129-1258: pointwise Jacobi, delta = -r / J_kk.  One thread per
+// column walking k.  mode 0 writes delta_E, mode 1 the updated state.
+__global__ void __launch_bounds__(kColThreads) k_enth_layer(EnthArgs a, double* out, int mode) {
+    if (stopped(a.done)) return;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ny * a.nx) return;
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    const int i = col / a.nx, j = col % a.nx;
+    const ColumnCtx x = column_ctx(a, i, j);
+    const double* E = a.E + x.c;
+    if (x.h < a.h_thin) {
+        for (int k = 0; k < nz; ++k) out[size_t(k) * plane + x.c] = mode ? E[size_t(k) * plane] : 0.0;
+        return;
+    }
+    const double dsig = 1.0 / double(nz - 1), inv_dt = 1.0 / a.dt;
+    const double* om = a.omega + x.c;
+    double Ekm1 = 0.0, Ek = E[0], Ekp1 = E[plane];
+    double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
+    double K_lo = 0.0, om_m = 0.0, om_k = om[0];
+    for (int k = 0; k < nz - 1; ++k) {
+        const double om_p = om[size_t(k + 1) * plane];
+        const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp));
+        const size_t n = size_t(k) * plane + x.c;
+        double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[n]) * inv_dt - a.f_E[n];
+        double diag = kRhoI * x.h * inv_dt;
+        if (a.flags & kTermHorizAdv) {
+            HAdv ha = horiz(a, x, k, Ek);
+            r += ha.res;
+            diag += ha.diag;
+        }
+        Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig);
+        r += vt.adv;
+        r += vt.dif;
+        r += vt.drn;
+        diag += vt.b_dif + vt.b_adv + vt.b_drn;
+        const double d = (fabs(diag) > 1e-30) ? (-r / diag) : 0.0;
+        out[n] = mode ? Ek + a.omega_relax * d : d;
+        Ekm1 = Ek; Ek = Ekp1;
+        Ekp1 = (k + 2 < nz) ? E[size_t(k + 2) * plane] : 0.0;
+        Epk = Epp;
+        Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
+        K_lo = K_up;
+        om_m = om_k; om_k = om_p;
+    }
+    const size_t top = size_t(nz - 1) * plane + x.c;
+    out[top] = mode ? E[size_t(nz - 1) * plane] : 0.0;
+}
+
+// ------------------------------------------------------------ omega
+// enthalpy.cu:1277-1372: omega = H sigma_dot integrated upward from
+// omega(0) = -bmb.  dh_dt: explicit array, or (H - H_prev) / dh_div when
+// dh_dt is null (glide/model.py:237-258).  Velocities are read undivided
+// (the reference evaluates this in m/a); omega is divided by omega_div.
+__global__ void __launch_bounds__(kColThreads) k_enth_omega(EnthArgs a, double* omega, const double* dh_dt,
+                                                               int ld_dh, const double* bmb, int ld_bmb,
+                                                               double dh_div, double omega_div) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ny * a.nx) return;
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    const int i = col / a.nx, j = col % a.nx;
+    const double* H = a.H;
+    const double h = H[size_t(i) * a.ld_h + j];
+    const size_t c = size_t(i) * a.nx + j;
+    if (h < double(1e-3f)) {
+        for (int k = 0; k < nz; ++k) omega[size_t(k) * plane + c] = 0.0;
+        return;
+    }
+    auto Hc = [&](int ii, int jj) {
+        ii = ii < 0 ? 0 : (ii > a.ny - 1 ? a.ny - 1 : ii);
+        jj = jj < 0 ? 0 : (jj > a.nx - 1 ? a.nx - 1 : jj);
+        return H[size_t(ii) * a.ld_h + jj];
+    };
+    const double Hxm = Hc(i, j - 1), Hxp = Hc(i, j + 1), Hym = Hc(i - 1, j), Hyp = Hc(i + 1, j);
+    const double dx_inv = 1.0 / a.dx, dsig = 1.0 / double(nz - 1);
+    const double dh = dh_dt ? dh_dt[size_t(i) * ld_dh + j] : (h - a.H_prev[c]) / dh_div;
+    double w = bmb ? -bmb[size_t(i) * ld_bmb + j] : -0.0;
+    omega[c] = w / omega_div;
+    double div_prev = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const double* uk = a.u + k * a.u_layer + size_t(i) * a.ld_u;
+        const double* vk = a.v + k * a.v_layer;
+        const double ul = uk[j], ur = uk[j + 1];
+        const double vt = vk[size_t(i) * a.ld_v + j], vb = vk[size_t(i + 1) * a.ld_v + j];
+        double fr = 0.0, fl = 0.0, fb = 0.0, ft = 0.0;
+        if (j < a.nx - 1) fr = 0.5 * (h + Hxp) * ur - 0.5 * sqrt(ur * ur + kRegYr) * (Hxp - h);
+        if (j > 0) fl = 0.5 * (Hxm + h) * ul - 0.5 * sqrt(ul * ul + kRegYr) * (h - Hxm);
+        if (i < a.ny - 1) fb = 0.5 * (h + Hyp) * vb - 0.5 * sqrt(vb * vb + kRegYr) * (h - Hyp);
+        if (i > 0) ft = 0.5 * (Hym + h) * vt - 0.5 * sqrt(vt * vt + kRegYr) * (Hym - h);
+        const double div = (fr - fl + ft - fb) * dx_inv;
+        if (k > 0) {
+            w = w - dsig * (dh + 0.5 * (div_prev + div));
+            omega[size_t(k) * plane + c] = w / omega_div;
+        }
+        div_prev = div;
+    }
+}
+
+// ------------------------------------------------------------- forcing
+// EnthalpyOperators.set_rhs (glide/enthalpy.py:473-519): f_E = H phi_strain /
+// E_SCALE below the surface, plus (Q_geo + Q_fh) / (dsig/2 E_SCALE) at the bed,
+// 0 at the surface.  e_scale is the host-side E_SCALE of glide/enthalpy.py.
+__global__ void __launch_bounds__(kColThreads) k_enth_set_rhs(EnthArgs a, double* f_E, const double* phi_strain,
+                                                                 const double* Q_geo, const double* Q_fh,
+                                                                 double e_scale) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ny * a.nx) return;
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    const int i = col / a.nx, j = col % a.nx;
+    const size_t c = size_t(i) * a.nx + j;
+    const double h = a.H[size_t(i) * a.ld_h + j];
+    const double dsig_half = 0.5 * (1.0 / double(nz - 1));
+    for (int k = 0; k < nz - 1; ++k) {
+        double f = h * phi_strain[size_t(k) * plane + c] / e_scale;
+        if (k == 0) f += (Q_geo[c] + Q_fh[c]) / (dsig_half * e_scale);
+        f_E[size_t(k) * plane + c] = f;
+    }
+    f_E[size_t(nz - 1) * plane + c] = 0.0;
+}
+
+// Q_fh = beta |u_b|^(m+1) from the bed-layer velocity (glide/model.py:224-235)
+__global__ void k_enth_friction(EnthArgs a, double* Q_fh, const double* beta, int ld_beta, double m,
+                                double u_reg) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ny * a.nx) return;
+    const int i = col / a.nx, j = col % a.nx;
+    const double* u0 = a.u + size_t(i) * a.ld_u;
+    const double uc = 0.5 * (u0[j + 1] / a.vel_div + u0[j] / a.vel_div);
+    const double vc = 0.5 * (a.v[size_t(i + 1) * a.ld_v + j] / a.vel_div + a.v[size_t(i) * a.ld_v + j] / a.vel_div);
+    const double speed = sqrt(uc * uc + vc * vc + u_reg * u_reg);
+    Q_fh[size_t(i) * a.nx + j] = beta[size_t(i) * ld_beta + j] * pow(speed, m + 1.0);
+}
+
+// Depth-averaged rate factor B = mean_k(A)^(-1/n) / scale (Paterson-Budd with
+// water-content enhancement, glide/enthalpy.py:600-643).  Host-side constants
+// of glide/enthalpy.py (binary64), sigma as numpy.linspace gives it.
+__global__ void __launch_bounds__(kColThreads) k_enth_arrhenius(EnthArgs a, double* B, int ld_B, double n_glen,
+                                                                   double scale) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ny * a.nx) return;
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    const int i = col / a.nx, j = col % a.nx;
+    const size_t c = size_t(i) * a.nx + j;
+    const double h = a.H[size_t(i) * a.ld_h + j];
+    const double step = 1.0 / double(nz - 1);
+    const double E_SCALE = 2009.0 * (273.15 - 223.15), cc = 7.9e-8 * 910.0 * 9.81;
+    auto rate = [&](int k) {
+        const double sig = (k == nz - 1) ? 1.0 : k * step;
+        const double depth = (1.0 - sig) * h;
+        const double T_pmp = 273.15 - cc * depth;
+        const double Ek = a.E[size_t(k) * plane + c];
+        const double T = fmin(Ek * E_SCALE / 2009.0 + 223.15, T_pmp);
+        const bool cold = T < 263.15;
+        const double Af = cold ? 3.985e-13 : 1.916e3, Qf = cold ? 60e3 : 139e3;
+        double A = Af * exp(-Qf / (8.314 * fmax(T, 1.0)));
+        const double w = fmax(Ek * E_SCALE - 2009.0 * (T_pmp - 223.15), 0.0) / 334000.0;
+        return A * (1.0 + 181.25 * w);
+    };
+    // numpy's pairwise sum of a short contiguous axis: below 8 terms in order;
+    // else 8 interleaved partial sums combined pairwise, then the rest in order
+    double sum = 0.0;
+    if (nz < 8) {
+        for (int k = 0; k < nz; ++k) sum += rate(k);
+    } else {
+        double r[8];
+        for (int q = 0; q < 8; ++q) r[q] = rate(q);
+        const int n8 = nz - nz % 8;
+        for (int k = 8; k < n8; k += 8)
+            for (int q = 0; q < 8; ++q) r[q] += rate(k + q);
+        sum = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (int k = n8; k < nz; ++k) sum += rate(k);
+    }
+    const double A_avg = sum / double(nz);
+    B[size_t(i) * ld_B + j] = pow(A_avg, -1.0 / n_glen) / scale;
+}
+
+}  // namespace enth
+}  // namespace glide

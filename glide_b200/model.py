@@ -69,3 +69,83 @@ class IceDynamics:
         mask = ((_lib.GRAD_BETA if compute_beta_grad else 0) | (_lib.GRAD_BED if compute_bed_grad else 0) |
                 (_lib.GRAD_H_PREV if compute_H_prev_grad else 0) | (_lib.GRAD_SMB if compute_smb_grad else 0))
         return self.adjoint_solver.solve(dt, start_level=top, grad_mask=mask)
+
+
+class ThermalModel:
+    """Enthalpy solver coupled to the momentum solve (mirror of glide/model.py:97-281).
+
+    step(dt): omega from the realised thickness change, frictional heating,
+    forcing, column sweeps, then the depth-averaged rate factor fed back into
+    the finest grid's B (coarser levels keep theirs, as in the reference).
+    The SSA velocity is read in place for every sigma layer (no layer copies);
+    the m/a -> m/s conversion is applied by the kernels as they read it.
+    """
+
+    SEC_PER_YR = 365.25 * 86400.0
+
+    def __init__(self, grid, nz=21, n_smooth=10, update_rheology=True, frictional_heating=True, rho_i=917.0):
+        from .enthalpy import EnthalpyOperators
+        self.ops = EnthalpyOperators(grid, nz=nz)
+        self.n_smooth = n_smooth
+        self.update_rheology = update_rheology
+        self.frictional_heating = frictional_heating
+        self.rho_i = rho_i
+        self.g = 9.81
+
+    def initialize(self, T_surface, T_field=None, Q_geo=None):
+        """Initial temperature, surface Dirichlet data and geothermal flux (glide/model.py:134-153)."""
+        if T_field is None:
+            T_field = T_surface
+        self.ops.initialize_from_temperature(T_field)
+        self.ops.set_surface_enthalpy_from_temperature(T_surface)
+        if Q_geo is not None:
+            self.ops.enthalpy_forcing.Q_geo[:] = torch.as_tensor(Q_geo, dtype=torch.float64, device="cuda")
+
+    def pre_momentum(self):
+        """Snapshot E and H before the momentum step (glide/model.py:155-164)."""
+        self.ops.snapshot()
+
+    def step(self, dt):
+        """Advance enthalpy by dt seconds (glide/model.py:166-222)."""
+        from .enthalpy import _ecall, _stream
+        import ctypes
+        ops = self.ops
+        sec = self.SEC_PER_YR
+        ops._push_config()
+        ops.broadcast_velocity()
+        # omega in m/a from (H - H_prev) / dt_yr, then converted to m/s
+        dt_yr = dt / sec
+        _ecall("glide_enthalpy_compute_omega", ops._h, None, 0, None, 0, float(dt_yr), float(sec), _stream())
+        ops._bind(vel_div=sec)
+        if self.frictional_heating:
+            sl = ops.grid.sliding
+            beta = sl.beta.data
+            _ecall("glide_enthalpy_frictional_heating", ops._h, ctypes.c_void_p(beta.data_ptr()), beta.stride(0),
+                   float(sl.m.value), float(sl.u_reg.value), _stream())
+        ops.set_rhs(snapshot=False)
+        ops.column_sweep(dt, self.n_smooth)
+        if self.update_rheology:
+            n = float(ops.grid.rheology.n.value)
+            scale = self.rho_i * self.g * sec ** (1.0 / n)
+            ops.get_arrhenius_factor(out=ops.grid.rheology.B.data, scale=scale)
+
+    @property
+    def B_scale(self):
+        n = float(self.ops.grid.rheology.n.value)
+        return self.rho_i * self.g * self.SEC_PER_YR ** (1.0 / n)
+
+    @property
+    def temperature(self):
+        return self.ops.get_temperature()
+
+    @property
+    def water_content(self):
+        return self.ops.get_water_content()
+
+    @property
+    def enthalpy(self):
+        return self.ops.enthalpy_state.E
+
+    @property
+    def sigma(self):
+        return self.ops.sigma

@@ -4,7 +4,8 @@ Outputs:
   oracle/libglide_oracle.so      -- this project's C++ restatement of the
                                     reference's discrete operator and solver
                                     sequencing (binary64 and binary32 entry
-                                    points), OpenMP over rows.
+                                    points), OpenMP over rows, and of its
+                                    enthalpy column solver (binary64).
   oracle/_ref/libglide_ref32.so  -- the reference's own kernel sources
   oracle/_ref/libglide_ref64.so     (glide/cuda/*.cu) compiled as host C++ from
                                     the reference checkout and executed by the
@@ -17,6 +18,7 @@ from __future__ import annotations
 
 import argparse
 import os
+import re
 import subprocess
 import sys
 from pathlib import Path
@@ -44,11 +46,39 @@ def _run(cmd: list[str]) -> None:
 
 def build_oracle(force: bool = False) -> Path:
     out = HERE / "libglide_oracle.so"
-    srcs = [HERE / "glide_oracle.cpp", HERE / "glide_oracle.hpp"]
+    srcs = [HERE / "glide_oracle.cpp", HERE / "glide_oracle.hpp", HERE / "enthalpy_oracle.cpp"]
     if force or _stale(out, srcs):
         _run([CXX, *BASE_FLAGS, "-march=x86-64-v2", str(HERE / "glide_oracle.cpp"),
-              "-o", str(out)])
+              str(HERE / "enthalpy_oracle.cpp"), "-o", str(out)])
     return out
+
+
+# Constants the reference injects into its enthalpy kernels, in the order of
+# glide/enthalpy.py:231-238; K_COLD and E_SCALE follow as expressions.
+ENTHALPY_CONSTANTS = ["RHO_I", "RHO_W", "C_I", "K_I", "L_HEAT", "T_REF", "T_MELT", "BETA_CC", "GRAVITY",
+                      "K_TEMP_FACTOR", "MASS_FLUX_REG", "MASS_FLUX_REG_YR"]
+
+
+def enthalpy_defines(reference: str) -> str:
+    """The #define block the reference prepends to enthalpy.cu
+    (glide/enthalpy.py:229-246): each constant as a binary32 literal of its
+    Python value.  The numeric module-level assignments of glide/enthalpy.py
+    are evaluated in order, with no builtins."""
+    src = (Path(reference) / "glide" / "enthalpy.py").read_text()
+    ns: dict[str, float] = {}
+    for line in src.splitlines():
+        m = re.match(r"^([A-Z][A-Z0-9_]*)\s*=\s*([0-9A-Z_.+\-*/() e]+?)\s*(#.*)?$", line)
+        if m:
+            try:
+                ns[m.group(1)] = float(eval(m.group(2), {"__builtins__": {}}, dict(ns)))
+            except Exception:
+                pass
+    missing = [k for k in ENTHALPY_CONSTANTS if k not in ns]
+    if missing:
+        raise RuntimeError(f"constants not found in glide/enthalpy.py: {missing}")
+    lines = [f"#define {k} {ns[k]}f" for k in ENTHALPY_CONSTANTS]
+    lines += ["#define K_COLD (K_I/C_I)", "#define E_SCALE (C_I * (T_MELT - T_REF))"]
+    return "\n".join(lines) + "\n"
 
 
 def build_reference(reference: str, force: bool = False) -> list[Path]:
@@ -57,13 +87,17 @@ def build_reference(reference: str, force: bool = False) -> list[Path]:
         print(f"reference kernels not found under {cuda_dir}; skipping oracle/_ref", flush=True)
         return []
     REF_OUT.mkdir(exist_ok=True)
-    srcs = [HERE / "ref_harness.cpp", HERE / "simt_host.cpp", HERE / "simt_host.hpp",
+    defines = REF_OUT / "enthalpy_defines.h"
+    text = enthalpy_defines(reference)
+    if not defines.exists() or defines.read_text() != text:
+        defines.write_text(text)
+    srcs = [HERE / "ref_harness.cpp", HERE / "simt_host.cpp", HERE / "simt_host.hpp", defines,
             *sorted(cuda_dir.glob("*.cu"))]
     outs = []
     for bits, defs in ((32, []), (64, ["-DGLIDE_REF_FP64"])):
         out = REF_OUT / f"libglide_ref{bits}.so"
         if force or _stale(out, srcs):
-            _run([CXX, *BASE_FLAGS, "-w", f"-I{cuda_dir}", f"-I{HERE}", *defs,
+            _run([CXX, *BASE_FLAGS, "-w", f"-I{cuda_dir}", f"-I{HERE}", f"-I{REF_OUT}", *defs,
                   str(HERE / "ref_harness.cpp"), str(HERE / "simt_host.cpp"), "-o", str(out)])
         outs.append(out)
     return outs

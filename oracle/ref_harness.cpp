@@ -32,6 +32,11 @@
 #include "vanka.cu"
 #include "grad.cu"
 #include "transfer.cu"
+// The enthalpy module is compiled by the reference with its physical constants
+// injected as #define lines (glide/enthalpy.py:229-246); build_oracle.py writes
+// the same lines into oracle/_ref/enthalpy_defines.h.
+#include "enthalpy_defines.h"
+#include "enthalpy.cu"
 
 #ifdef GLIDE_REF_FP64
 #undef float
@@ -184,5 +189,43 @@ GREF_TRANSFER(prolongate_hfacet_injection)
 GREF_TRANSFER(prolongate_hfacet_bilinear)
 GREF_TRANSFER(prolongate_cell_injection)
 GREF_TRANSFER(prolongate_cell_bilinear)
+
+#define GREF_ENTHALPY_ARRAYS                                                          \
+    const ref_real *E, const ref_real *E_prev, const ref_real *f_E, const ref_real *u3d,  \
+        const ref_real *v3d, const ref_real *omega, const ref_real *H,                    \
+        const ref_real *H_prev, const ref_real *E_surface, ref_real dx, ref_real dt,      \
+        ref_real drain_rate, ref_real h_thin, ref_real lf_c, int term_flags
+
+void gref_enthalpy_compute_residual(int gx, int bx, ref_real* out, GREF_ENTHALPY_ARRAYS,
+                                    int use_forcing, int ny, int nx, int nz) {
+    simt::launch(d3(gx, 1, 1), d3(bx, 1, 1), [&] {
+        enthalpy_compute_residual(out, E, E_prev, f_E, u3d, v3d, omega, H, H_prev, E_surface, dx, dt,
+                                  drain_rate, h_thin, lf_c, term_flags, use_forcing, ny, nx, nz);
+    });
+}
+
+void gref_enthalpy_column_smooth(int gx, int bx, ref_real* delta_E, GREF_ENTHALPY_ARRAYS, int ny,
+                                 int nx, int nz, int n_newton, ref_real relaxation) {
+    simt::launch(d3(gx, 1, 1), d3(bx, 1, 1), [&] {
+        enthalpy_column_smooth(delta_E, E, E_prev, f_E, u3d, v3d, omega, H, H_prev, E_surface, dx, dt,
+                               drain_rate, h_thin, lf_c, term_flags, ny, nx, nz, n_newton, relaxation);
+    });
+}
+
+void gref_enthalpy_layer_smooth(int gx, int bx, ref_real* delta_E, GREF_ENTHALPY_ARRAYS, int ny,
+                                int nx, int nz) {
+    simt::launch(d3(gx, 1, 1), d3(bx, 1, 1), [&] {
+        enthalpy_layer_smooth(delta_E, E, E_prev, f_E, u3d, v3d, omega, H, H_prev, E_surface, dx, dt,
+                              drain_rate, h_thin, lf_c, term_flags, ny, nx, nz);
+    });
+}
+
+void gref_compute_omega(int gx, int bx, ref_real* omega, const ref_real* u3d, const ref_real* v3d,
+                        const ref_real* H, const ref_real* dh_dt, const ref_real* bmb, ref_real dx, int ny,
+                        int nx, int nz) {
+    simt::launch(d3(gx, 1, 1), d3(bx, 1, 1), [&] {
+        compute_omega(omega, u3d, v3d, H, dh_dt, bmb, dx, ny, nx, nz);
+    });
+}
 
 }  // extern "C"

@@ -45,6 +45,12 @@ _SIGS = {
     "compute_gradient_beta": ("2d", "p" * 13 + _PHYS + "iiii"),
     "compute_gradient_bed": ("2d", "p" * 13 + _PHYS + "iiii"),
 }
+_SIGS.update({
+    "enthalpy_compute_residual": ("1d", "p" * 10 + "r" * 5 + "ii" + "iii"),
+    "enthalpy_column_smooth": ("1d", "p" * 10 + "r" * 5 + "i" + "iii" + "ir"),
+    "enthalpy_layer_smooth": ("1d", "p" * 10 + "r" * 5 + "i" + "iii"),
+    "compute_omega": ("1d", "p" * 6 + "r" + "iii"),
+})
 for _name in ("restrict_vfacet", "restrict_hfacet", "restrict_cell_avg", "restrict_cell_max",
               "restrict_cell_min", "restrict_cell_var", "prolongate_vfacet_injection",
               "prolongate_vfacet_bilinear", "prolongate_hfacet_injection",
@@ -165,7 +171,7 @@ def load_reference(fp64: bool = True, reference: str = DEFAULT_REFERENCE):
     if reference not in sys.path:
         sys.path.insert(0, reference)
     glide = importlib.import_module("glide")
-    for sub in ("field", "grid", "operators", "multigrid", "model"):
+    for sub in ("field", "grid", "operators", "multigrid", "model", "enthalpy"):
         importlib.import_module("glide." + sub)
     glide._kernels = kernels
     return glide

@@ -77,3 +77,41 @@ def random_state(ny, nx, seed=1, thin_frac=0.2):
     f_v = rng.normal(0, 1e-2, (ny + 1, nx))
     H_prev = H * rng.uniform(0.95, 1.05, (ny, nx))
     return dict(u=u, v=v, H=H, H_prev=H_prev, bed=bed, B=B, beta=beta, smb=smb, mask=mask, f_u=f_u, f_v=f_v)
+
+
+SEC_PER_YR = 365.25 * 86400.0
+E_SCALE_HOST = 2009.0 * (273.15 - 223.15)  # C_I (T_MELT - T_REF), J/kg
+
+
+def enthalpy_state(ny, nx, nz, seed=1, thin_frac=0.15):
+    """A rough enthalpy state exercising every branch of the column solver:
+    cold and temperate nodes on both sides of the pressure-melting point,
+    thin columns below h_thin, random layer velocities (m/s) and omega."""
+    rng = np.random.default_rng(seed)
+    H = rng.uniform(100.0, 3000.0, (ny, nx))
+    H[rng.random((ny, nx)) < thin_frac] = rng.uniform(1.0, 20.0)
+    sigma = np.linspace(0.0, 1.0, nz)
+    depth = (1.0 - sigma)[None, None, :] * H[:, :, None]
+    E_pmp = 2009.0 * (273.15 - 7.9e-8 * 910.0 * 9.81 * depth - 223.15) / E_SCALE_HOST
+    # offsets from -0.5 (cold) to +0.02 (temperate, ~2 kJ/kg above pmp)
+    E = E_pmp + rng.uniform(-0.5, 0.02, (ny, nx, nz))
+    E_prev = E + rng.normal(0.0, 0.01, E.shape)
+    u3d = rng.normal(0.0, 100.0, (nz, ny, nx + 1)) / SEC_PER_YR
+    v3d = rng.normal(0.0, 100.0, (nz, ny + 1, nx)) / SEC_PER_YR
+    omega = rng.normal(0.0, 0.3, (ny, nx, nz)) / SEC_PER_YR
+    f_E = rng.normal(0.0, 1e-6, (ny, nx, nz))
+    f_E[:, :, -1] = 0.0
+    E_surface = E_pmp[:, :, -1] - rng.uniform(0.1, 0.4, (ny, nx))
+    H_prev = H * rng.uniform(0.98, 1.02, (ny, nx))
+    return dict(E=E, E_prev=E_prev, f_E=f_E, u3d=u3d, v3d=v3d, omega=omega, H=H, H_prev=H_prev,
+                E_surface=E_surface)
+
+
+def enthalpy_config(**kw):
+    """ColumnSmootherConfig / EnthalpyForcing defaults of the reference
+    (glide/enthalpy.py:108-203) as binary64 numbers."""
+    cfg = dict(dx=2000.0, dt=10.0 * SEC_PER_YR, drain_rate=0.01 / SEC_PER_YR, h_thin=25.0,
+               lf_c=1e-12, term_flags=7, omega=1.0, n_newton=3, relaxation=1.0,
+               relative_tolerance=1e-5, absolute_tolerance=1e-2)
+    cfg.update(kw)
+    return cfg

@@ -25,7 +25,7 @@ ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(HERE.parent))
 
-from cases import random_state, slab_c1  # noqa: E402
+from cases import SEC_PER_YR, enthalpy_config, enthalpy_state, random_state, slab_c1  # noqa: E402
 from oracle.refpy import load_reference  # noqa: E402
 
 
@@ -163,13 +163,99 @@ def random_cases(glide):
     np.savez_compressed(HERE / "random_adjoint_f64.npz", **out)
 
 
+def enthalpy_cases(glide):
+    """EnthalpyOperators (glide/enthalpy.py) on a rough random state: residual,
+    one column smooth, one layer smooth, omega, and column sweeps; then one
+    ThermalModel step (glide/model.py:97-281) on a random grid."""
+    from glide.enthalpy import EnthalpyOperators
+    from glide.grid import Grid
+    from glide.model import ThermalModel
+    ny, nx, nz = 6, 9, 11
+    st = enthalpy_state(ny, nx, nz, seed=5)
+    cfg = enthalpy_config()
+    dt = cfg["dt"]
+
+    def make_ops():
+        g = Grid(ny, nx, cfg["dx"])
+        g.state.H.set(st["H"])
+        ops = EnthalpyOperators(g, nz=nz)
+        es, ev, ef = ops.enthalpy_state, ops.enthalpy_velocity, ops.enthalpy_forcing
+        es.E[:] = st["E"]
+        es.E_prev[:] = st["E_prev"]
+        ops.f_E[:] = st["f_E"]
+        ev.u3d[:] = st["u3d"]
+        ev.v3d[:] = st["v3d"]
+        ev.omega[:] = st["omega"]
+        ops.H_prev[:] = st["H_prev"]
+        ef.E_surface[:] = st["E_surface"]
+        return ops
+
+    out = {f"in_{k}": v for k, v in st.items()}
+    ops = make_ops()
+    out["out_rmax"] = np.array(ops.compute_residual(dt))
+    out["out_r_E"] = np.array(ops.r_E)
+    ops.column_smooth(dt)
+    out["out_column_delta"] = np.array(ops.delta_E)
+    ops.layer_smooth(dt)
+    out["out_layer_delta"] = np.array(ops.delta_E)
+    rng = np.random.default_rng(17)
+    dh = rng.normal(0.0, 0.5, (ny, nx))
+    out["in_dh_dt"] = dh
+    ev = ops.enthalpy_velocity
+    ev.u3d[:] = st["u3d"] * SEC_PER_YR
+    ev.v3d[:] = st["v3d"] * SEC_PER_YR
+    ops.compute_omega(dh)
+    out["out_omega"] = np.array(ev.omega)
+    for tag, alternating, n in (("alt", True, 4), ("col", False, 3)):
+        ops = make_ops()
+        ops.smoother_config.relative_tolerance = 1e-30
+        ops.smoother_config.absolute_tolerance = 0.0
+        ops.column_sweep(dt, n, alternating=alternating)
+        out[f"out_sweep_{tag}_E"] = np.array(ops.enthalpy_state.E)
+    np.savez_compressed(HERE / "enthalpy_ops_f64.npz", **out)
+
+    # one coupled thermal step
+    ny, nx, nz = 8, 10, 9
+    rng = np.random.default_rng(23)
+    g = Grid(ny, nx, 1500.0)
+    u = rng.normal(0.0, 80.0, (ny, nx + 1))
+    v = rng.normal(0.0, 80.0, (ny + 1, nx))
+    H0 = rng.uniform(200.0, 2500.0, (ny, nx))
+    H0[0, :3] = 10.0
+    beta = rng.uniform(0.05, 0.5, (ny, nx))
+    T_s = rng.uniform(238.0, 268.0, (ny, nx))
+    g.state.u.set(u)
+    g.state.v.set(v)
+    g.state.H.set(H0)
+    g.sliding.beta.set(beta)
+    tm = ThermalModel(g, nz=nz, n_smooth=4)
+    tm.initialize(T_s, Q_geo=0.05)
+    tm.pre_momentum()
+    H1 = H0 * rng.uniform(0.99, 1.01, (ny, nx))
+    g.state.H.set(H1)
+    dt_s = 10.0 * SEC_PER_YR
+    tm.step(dt_s)
+    out = dict(in_u=u, in_v=v, in_H0=H0, in_H1=H1, in_beta=beta, in_T_s=T_s, in_dt=np.array(dt_s))
+    out["out_E"] = np.array(tm.enthalpy)
+    out["out_omega"] = np.array(tm.ops.enthalpy_velocity.omega)
+    out["out_Q_fh"] = np.array(tm.ops.enthalpy_forcing.Q_fh)
+    out["out_B"] = np.array(g.rheology.B.data)
+    out["out_T"] = np.array(tm.temperature)
+    np.savez_compressed(HERE / "thermal_step_f64.npz", **out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None, help="enthalpy: only the enthalpy fixtures")
     a = ap.parse_args(argv)
+    if a.only == "enthalpy":
+        enthalpy_cases(load_reference(fp64=True, reference=a.reference))
+        return
     glide = load_reference(fp64=True, reference=a.reference)
     c1_forward_and_adjoint(glide, "f64")
     random_cases(glide)
+    enthalpy_cases(glide)
     glide32 = load_reference(fp64=False, reference=a.reference)
     c1_forward_and_adjoint(glide32, "f32")
     for p in sorted(HERE.glob("*.npz")):
