@@ -29,17 +29,19 @@ struct ResidualArgs {
     int active_set;              // Newton mode (see the mass row below)
 };
 
+// Each warp computes a 4 x 8 patch of the 16 x 16 tile; rows are padded to 24
+// entries so that the patch's stencil reads are bank-conflict free.
 template <class R>
 __global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a) {
-    using TileT = Tile<R, kTile, 1, 1>;
+    using TileT = Tile<R, kTile, 1, 1, 24>;
     constexpr int NC = TileT::NC;
     __shared__ TileT t;
     __shared__ double red[3][8];
     const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
     const int ny = a.ny, nx = a.nx;
-    stage_tile<R, kTile, 1, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
+    stage_tile<R, kTile, 1, 1, 24>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
     __syncthreads();
-    TileView<R, kTile, 1, 1> s{t, i0, j0, ny, nx};
+    TileView<R, kTile, 1, 1, 24> s{t, i0, j0, ny, nx};
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
         int gi = i0 - 1 + r, gj = j0 - 1 + c;
@@ -47,7 +49,8 @@ __global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a) {
         t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
     }
     __syncthreads();
-    const int i = i0 + threadIdx.x / kTile, j = j0 + threadIdx.x % kTile;
+    const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    const int i = i0 + 4 * (wp >> 1) + (ln >> 3), j = j0 + 8 * (wp & 1) + (ln & 7);
     double ssu = 0, ssv = 0, ssh = 0;
     if (i < ny && j < nx) {
         const bool f = a.use_forcing != 0;

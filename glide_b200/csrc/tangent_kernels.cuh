@@ -13,25 +13,6 @@
 
 namespace glide {
 
-template <class R>
-struct TanView {
-    const AdjTile<R>& a;  // lu/lv hold e_u/e_v, etad holds d(eta) along e
-    const Arr<R>* eH;
-    int i0, j0, ny, nx;
-    static constexpr int A = 2;
-    __device__ R U(int i, int j) const { return a.t.u[i - (i0 - A - 1)][j - (j0 - A)]; }
-    __device__ R V(int i, int j) const { return a.t.v[i - (i0 - A)][j - (j0 - A - 1)]; }
-    __device__ R LU(int i, int j) const { return a.lu[i - (i0 - A - 1)][j - (j0 - A)]; }
-    __device__ R LV(int i, int j) const { return a.lv[i - (i0 - A)][j - (j0 - A - 1)]; }
-    __device__ R Hc(int i, int j) const { return a.t.H[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R PHI(int i, int j) const { return a.t.phi[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R BED(int i, int j) const { return a.t.bed[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R BETA(int i, int j) const { return a.t.beta[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R ETA(int i, int j) const { return a.t.eta[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R ETAD(int i, int j) const { return a.etad[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R EH(int i, int j) const { return eH->at(clampi(i, 0, ny - 1), clampi(j, 0, nx - 1)); }
-};
-
 // d(mass row of cell (i,j)) . e before masking (residuals.cu:391-439)
 template <class R, class S>
 __device__ __forceinline__ R mass_jvp(const S& s, const PhysR<R>& p, int i, int j) {
@@ -158,27 +139,115 @@ __device__ __forceinline__ R vmom_jvp(const S& s, const PhysR<R>& p, int i, int 
     return d;
 }
 
+// Staged tile of the JVP: the state and e with a one-cell halo, eta and
+// eta-dot.  Rows are padded to 24 entries: with the 4 x 8 cell patch each warp
+// computes (see jvp_cell), every stencil access of a warp then hits distinct
+// shared-memory banks, for 4- and 8-byte values alike.
+template <class R>
+struct JvpTile {
+    static constexpr int T = kTileA, A = 1, NC = T + 2, P = 24;
+    R u[NC + 2][P], v[NC + 1][P], eu[NC + 2][P], ev[NC + 1][P];
+    R H[NC][P], phi[NC][P], bed[NC][P], beta[NC][P], eta[NC][P], etad[NC][P], eH[NC][P];
+};
+
+template <class R>
+struct JvpView {
+    const JvpTile<R>& t;
+    int i0, j0, ny, nx;
+    static constexpr int A = 1;
+    __device__ R U(int i, int j) const { return t.u[i - (i0 - A - 1)][j - (j0 - A)]; }
+    __device__ R V(int i, int j) const { return t.v[i - (i0 - A)][j - (j0 - A - 1)]; }
+    __device__ R LU(int i, int j) const { return t.eu[i - (i0 - A - 1)][j - (j0 - A)]; }
+    __device__ R LV(int i, int j) const { return t.ev[i - (i0 - A)][j - (j0 - A - 1)]; }
+    __device__ R Hc(int i, int j) const { return t.H[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R PHI(int i, int j) const { return t.phi[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R BED(int i, int j) const { return t.bed[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R BETA(int i, int j) const { return t.beta[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R ETA(int i, int j) const { return t.eta[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R ETAD(int i, int j) const { return t.etad[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R EH(int i, int j) const { return t.eH[i - (i0 - A)][j - (j0 - A)]; }
+};
+
+// Viscosity and its derivative along e at one cell, sharing the strain rates
+// and one power: eta = B/2 eII^q, eta-dot = eta q eII'/eII (viscosity.cu:63-168).
+template <class R, class S>
+__device__ __forceinline__ void eta_and_dot(const S& s, R Bc, const PhysR<R>& p, int i, int j, R& eta, R& etad) {
+    const R dxi = p.dxi;
+    const int ny = s.ny, nx = s.nx;
+    R ul = s.U(i, j), ur = s.U(i, j + 1), vt = s.V(i, j), vb = s.V(i + 1, j);
+    R dul = s.LU(i, j), dur = s.LU(i, j + 1), dvt = s.LV(i, j), dvb = s.LV(i + 1, j);
+    R ux = (ur - ul) * dxi, vy = (vt - vb) * dxi;
+    R dux = (dur - dul) * dxi, dvy = (dvt - dvb) * dxi;
+    R m_tl = (i > 0 && j > 0), m_tr = (i > 0 && j < nx - 1);
+    R m_bl = (i < ny - 1 && j > 0), m_br = (i < ny - 1 && j < nx - 1);
+    R e1 = R(0.5) * ((s.U(i - 1, j) - ul) * dxi + (vt - s.V(i, j - 1)) * dxi) * m_tl;
+    R d1 = R(0.5) * ((s.LU(i - 1, j) - dul) * dxi + (dvt - s.LV(i, j - 1)) * dxi) * m_tl;
+    R e2 = R(0.5) * ((s.U(i - 1, j + 1) - ur) * dxi + (s.V(i, j + 1) - vt) * dxi) * m_tr;
+    R d2 = R(0.5) * ((s.LU(i - 1, j + 1) - dur) * dxi + (s.LV(i, j + 1) - dvt) * dxi) * m_tr;
+    R e3 = R(0.5) * ((ul - s.U(i + 1, j)) * dxi + (vb - s.V(i + 1, j - 1)) * dxi) * m_bl;
+    R d3 = R(0.5) * ((dul - s.LU(i + 1, j)) * dxi + (dvb - s.LV(i + 1, j - 1)) * dxi) * m_bl;
+    R e4 = R(0.5) * ((ur - s.U(i + 1, j + 1)) * dxi + (s.V(i + 1, j + 1) - vb) * dxi) * m_br;
+    R d4 = R(0.5) * ((dur - s.LU(i + 1, j + 1)) * dxi + (s.LV(i + 1, j + 1) - dvb) * dxi) * m_br;
+    R shear = R(0.25) * (e1 * e1 + e2 * e2 + e3 * e3 + e4 * e4);
+    R dshear = R(0.25) * (R(2) * e1 * d1 + R(2) * e2 * d2 + R(2) * e3 * d3 + R(2) * e4 * d4);
+    R eII = ux * ux + vy * vy + ux * vy + shear + p.eps_reg;
+    R deII = R(2) * ux * dux + R(2) * vy * dvy + (ux * dvy + dux * vy) + dshear;
+    eta = R(0.5) * Bc * glen_pow(eII, p);
+    etad = eta * p.gexp * deII / eII;
+}
+
+template <class R>
+__device__ void stage_jvp(JvpTile<R>& t, int i0, int j0, const VjpArgs<R>& a) {
+    using TT = JvpTile<R>;
+    constexpr int NC = TT::NC, A = TT::A;
+    const int ny = a.ny, nx = a.nx, tid = threadIdx.x, nt = blockDim.x;
+    for (int k = tid; k < (NC + 2) * (NC + 1); k += nt) {
+        int r = k / (NC + 1), c = k % (NC + 1);
+        int gi = clampi(i0 - A - 1 + r, 0, ny - 1), gj = clampi(j0 - A + c, 0, nx);
+        t.u[r][c] = ldg(&a.u.p[size_t(gi) * a.u.pitch + gj]);
+        t.eu[r][c] = ldg(&a.lu.p[size_t(gi) * a.lu.pitch + gj]);
+    }
+    for (int k = tid; k < (NC + 1) * (NC + 2); k += nt) {
+        int r = k / (NC + 2), c = k % (NC + 2);
+        int gi = clampi(i0 - A + r, 0, ny), gj = clampi(j0 - A - 1 + c, 0, nx - 1);
+        t.v[r][c] = ldg(&a.v.p[size_t(gi) * a.v.pitch + gj]);
+        t.ev[r][c] = ldg(&a.lv.p[size_t(gi) * a.lv.pitch + gj]);
+    }
+    for (int k = tid; k < NC * NC; k += nt) {
+        int r = k / NC, c = k % NC;
+        int gi = clampi(i0 - A + r, 0, ny - 1), gj = clampi(j0 - A + c, 0, nx - 1);
+        size_t o = size_t(gi) * a.H.pitch + gj;  // all cell arrays share one pitch
+        t.H[r][c] = ldg(&a.H.p[o]);
+        t.bed[r][c] = ldg(&a.bed.p[o]);
+        t.beta[r][c] = ldg(&a.beta.p[o]);
+        t.phi[r][c] = ldg(&a.phi.p[o]);
+        t.eH[r][c] = ldg(&a.lH.p[o]);
+    }
+}
+
 // r_lin = J e - f (- sub) over one level, optional per-block sums of squares.
-// Uses VjpArgs with lu/lv/lH carrying e and f_* the right-hand side.
+// Uses VjpArgs with lu/lv/lH carrying e and f_* the right-hand side.  Each
+// warp computes a 4 x 8 patch of the 16 x 16 tile.
 template <class R>
 __global__ void __launch_bounds__(kTileA * kTileA) k_jvp(VjpArgs<R> a, int ref_rows) {
-    constexpr int NC = AdjTile<R>::NC;
-    __shared__ AdjTile<R> T;
+    using TT = JvpTile<R>;
+    constexpr int NC = TT::NC;
+    __shared__ TT T;
     __shared__ double red[3][kTileA * kTileA / 32];
     const int i0 = blockIdx.y * kTileA, j0 = blockIdx.x * kTileA;
     const int ny = a.ny, nx = a.nx;
-    stage_adjoint(T, i0, j0, a);
+    stage_jvp(T, i0, j0, a);
     __syncthreads();
-    TanView<R> s{T, &a.lH, i0, j0, ny, nx};
+    JvpView<R> s{T, i0, j0, ny, nx};
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
-        int gi = i0 - 2 + r, gj = j0 - 2 + c;
+        int gi = i0 - 1 + r, gj = j0 - 1 + c;
         R Bc = a.B.at(clampi(gi, 0, ny - 1), clampi(gj, 0, nx - 1));
-        T.t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
-        T.etad[r][c] = eta_dot_at<R>(s, Bc, a.p, gi, gj);
+        eta_and_dot<R>(s, Bc, a.p, gi, gj, T.eta[r][c], T.etad[r][c]);
     }
     __syncthreads();
-    const int I = i0 + threadIdx.x / kTileA, J = j0 + threadIdx.x % kTileA;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int I = i0 + 4 * (w >> 1) + (l >> 3), J = j0 + 8 * (w & 1) + (l & 7);
     double ssu = 0, ssv = 0, ssh = 0;
     const bool f = a.use_forcing != 0;
     auto emit = [&](Arr<R> o, const Arr<R>& fa, const Arr<R>& sa, int i, int j, R val, double& ss) {
@@ -206,7 +275,6 @@ __global__ void __launch_bounds__(kTileA * kTileA) k_jvp(VjpArgs<R> a, int ref_r
             ssv += __shfl_down_sync(0xffffffffu, ssv, o);
             ssh += __shfl_down_sync(0xffffffffu, ssh, o);
         }
-        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
         if (l == 0) { red[0][w] = ssu; red[1][w] = ssv; red[2][w] = ssh; }
         __syncthreads();
         if (threadIdx.x < 3) {

@@ -13,21 +13,24 @@
 
 namespace glide {
 
-template <class R, int T, int A, int B>
+// P > 0 pads every row to P entries (P = 8 mod 16 makes a 4 x 8 cell patch
+// per warp bank-conflict free for 4- and 8-byte values).
+template <class R, int T, int A, int B, int P = 0>
 struct Tile {
     static constexpr int NC = T + A + B;
-    R u[NC + 2][NC + 1];
-    R v[NC + 1][NC + 2];
-    R H[NC][NC];
-    R phi[NC][NC];
-    R bed[NC][NC];
-    R beta[NC][NC];
-    R eta[NC][NC];
+    static constexpr int WU = P ? P : NC + 1, WV = P ? P : NC + 2, WC = P ? P : NC;
+    R u[NC + 2][WU];
+    R v[NC + 1][WV];
+    R H[NC][WC];
+    R phi[NC][WC];
+    R bed[NC][WC];
+    R beta[NC][WC];
+    R eta[NC][WC];
 };
 
-template <class R, int T, int A, int B>
+template <class R, int T, int A, int B, int P = 0>
 struct TileView {
-    const Tile<R, T, A, B>& t;
+    const Tile<R, T, A, B, P>& t;
     int i0, j0, ny, nx;
     __device__ R U(int i, int j) const { return t.u[i - (i0 - A - 1)][j - (j0 - A)]; }
     __device__ R V(int i, int j) const { return t.v[i - (i0 - A)][j - (j0 - A - 1)]; }
@@ -39,11 +42,11 @@ struct TileView {
 };
 
 // Stage u, v, H, bed, beta (and phi when `phi` is non-null) for the tile.
-template <class R, int T, int A, int B>
-__device__ void stage_tile(Tile<R, T, A, B>& t, int i0, int j0, int ny, int nx, const Arr<R>& u,
+template <class R, int T, int A, int B, int P = 0>
+__device__ void stage_tile(Tile<R, T, A, B, P>& t, int i0, int j0, int ny, int nx, const Arr<R>& u,
                            const Arr<R>& v, const Arr<R>& H, const Arr<R>& bed, const Arr<R>& beta,
                            const Arr<R>* phi) {
-    constexpr int NC = Tile<R, T, A, B>::NC;
+    constexpr int NC = Tile<R, T, A, B, P>::NC;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int k = tid; k < (NC + 2) * (NC + 1); k += nt) {
         int r = k / (NC + 1), c = k % (NC + 1);

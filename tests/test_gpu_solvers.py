@@ -112,7 +112,8 @@ def test_reference_dot_product_identity():
     assert abs(t1 - t2) <= 2e-2 * 0.5 * (abs(t1) + abs(t2)), (t1, t2)
 
 
-def _solve_c1(precision="fp64", quirks=True, method=None, schedule=None, relax=None, omega=None, rtol=1e-11):
+def _solve_c1(precision="fp64", quirks=True, method=None, schedule=None, relax=None, omega=None, rtol=1e-11,
+              newton_steps=None, switch=None):
     from cases import slab_c1
     f = slab_c1()
     h = _hier(64, 64, 1000.0, levels=4, precision=precision, quirks=quirks)
@@ -125,12 +126,16 @@ def _solve_c1(precision="fp64", quirks=True, method=None, schedule=None, relax=N
     kw = {}
     if relax is not None:
         kw["relaxation"] = relax
+    if newton_steps is not None:
+        kw["newton_steps"] = newton_steps
     if omega is not None:
         kw["omega"] = omega
     if kw:
         h.set_vanka(False, -1, **kw)
     if method:
         h.set_tuning(forward_method=method)
+    if switch is not None:
+        h.set_tuning(newton_switch_exp10=switch)
     st = h.forward(10.0, 0)
     return h, st
 
@@ -161,3 +166,35 @@ def test_mixed_precision_reaches_reference_solution(c1_reference_solution):
     assert st["final_norm"] <= 1e-11 * st["initial_norm"]
     for k, ref in c1_reference_solution.items():
         assert rel_err(_np(h.view(k, 0)), ref) <= 1e-8, k
+
+
+def test_fast_form_reaches_reference_solution(c1_reference_solution):
+    """The benchmark's fast form: mixed precision, corrected transfers,
+    FASCD (4/4/0/200, local Newton capped at 3) to 1e-2, then Newton."""
+    h, st = _solve_c1(precision="mixed", quirks=False, schedule=(4, 4, 0, 200), method="newton",
+                      newton_steps=3, switch=2)
+    assert st["final_norm"] <= 1e-11 * st["initial_norm"]
+    for k, ref in c1_reference_solution.items():
+        assert rel_err(_np(h.view(k, 0)), ref) <= 1e-8, k
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_adjoint_converges_to_reference_adjoint(precision):
+    """Converged adjoint of C1 (binary64 reference form) against the fast
+    forms: lambda to 1e-8 relative, gradients to 1e-7."""
+    def run(prec, quirks):
+        h, st = _solve_c1(precision=prec, quirks=quirks)
+        u, v = h.get("u", 0), h.get("v", 0)
+        h.set("adj_f_u", 0, -(u - 1.1 * u))
+        h.set("adj_f_v", 0, -(v - 0.9 * v))
+        h.set("adj_f_H", 0, 0.0)
+        h.set_fas(True, maximum_vcycles=100, relative_tolerance=1e-11, absolute_tolerance=0.0)
+        ast = h.backward(10.0, 0)
+        assert ast["final_norm"] <= 1e-11 * ast["initial_norm"], ast
+        return {k: _np(h.view(k, 0)).copy() for k in ("lambda_u", "lambda_v", "lambda_H", "grad_beta", "grad_bed")}
+    ref = run("fp64", True)
+    got = run(precision, True)
+    for k in ("lambda_u", "lambda_v", "lambda_H"):
+        assert rel_err(got[k], ref[k]) <= 1e-8, k
+    for k in ("grad_beta", "grad_bed"):
+        assert rel_err(got[k], ref[k]) <= 1e-7, k
