@@ -71,7 +71,12 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare-plain", action="store_true", help="skip timing the binary64 reference form")
     ap.add_argument("--no-grads", action="store_true", help="skip timing the adjoint (gradient) solve")
-    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels"],
+    ap.add_argument("--no-thermal", action="store_true", help="skip timing the enthalpy (thermal) step")
+    ap.add_argument("--nz", type=int, default=41, help="sigma levels of the enthalpy columns")
+    ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
+    ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
+    ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
+    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels", "thermal"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -482,6 +487,8 @@ def run_ours(a, rank, world):
                  "final_relative_residual": float(np.max([s["final_norm"] / s["initial_norm"] for s in pst])),
                  "what": "reference algorithm (FASCD 10/20/50/200, 30 local Newton iterations, quirks) in binary64"}
 
+    thermal = None if a.no_thermal else thermal_leg(a, h, f, stream, dev, world)
+
     dom = "k_vanka_sweep"
     kd = kernels[dom]
     res = {
@@ -509,7 +516,7 @@ def run_ours(a, rank, world):
                    "schedule": {k: fas[k] for k in ("pre_steps", "post_steps", "finest_steps", "coarsest_steps")},
                    "parallelism": f"replicas x{world} (one domain per GPU)",
                    "l2": "inputs larger than L2 (2048^2 state and parameters: ~0.5 GB per fine-level pass)",
-                   "plain_fp64": plain, "grads": grads},
+                   "plain_fp64": plain, "grads": grads, "thermal": thermal},
         "gpu_launches": int(launches),
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -522,6 +529,74 @@ def run_ours(a, rank, world):
         "clocks": clocks,
     }
     return res, plain
+
+
+def run_thermal(a):
+    """Profiling case: the thermal leg alone on the dome at --size with a
+    uniform velocity (50, 20) m/a in place of the SSA solution."""
+    import torch
+    from cases import dome
+    from glide_b200.hierarchy import Hierarchy
+    f = dome(a.size, a.dx, a.radius, seed=0)
+    h = Hierarchy(a.size, a.size, a.dx, 1, precision="fp64")
+    load_dome(h, f)
+    h.set("u", 0, 50.0)
+    h.set("v", 0, 20.0)
+    dev = torch.device("cuda", 0)
+    out = thermal_leg(a, h, f, torch.cuda.current_stream(), dev, 1)
+    print(json.dumps({"mode": "thermal", "size": a.size, **out}), flush=True)
+
+
+def thermal_leg(a, h, f, stream, dev, world):
+    """The enthalpy column solve coupled to the solved state: ThermalModel
+    steps (omega, frictional heating, forcing, up to 10 column/layer sweeps
+    with the device-side stop test, B feedback) on the 2048^2 grid with nz
+    sigma levels, binary64; then each enthalpy kernel alone.  Surface
+    temperature -30 + 6e-3 (2000 - s) C, geothermal flux 0.05 W m^-2."""
+    import torch
+    from glide_b200.grid import Grid
+    from glide_b200.model import ThermalModel
+    sec = 365.25 * 86400.0
+    g = Grid(hierarchy=h, level=0)
+    tm = ThermalModel(g, nz=a.nz, n_smooth=10)
+    tm.ops.set_tuning(point_blocks_per_sm=a.enth_point_blocks, column_blocks_per_sm=a.enth_column_blocks,
+                      column_prefers_l1=a.enth_column_l1)
+    H = np.asarray(f["H"])
+    surf = np.maximum(f["bed"] + H, (1.0 - 0.917) * H)
+    T_s = 273.15 + (-30.0 + 6e-3 * (2000.0 - surf))
+    tm.initialize(torch.as_tensor(T_s), Q_geo=0.05)
+    dt_s = a.dt * sec
+
+    def tstep():
+        tm.pre_momentum()
+        tm.step(dt_s)
+    tstep()
+    t_ms = event_time(tstep, 3, stream)
+    tt = torch.tensor([t_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    t_ms = float(tt.item())
+    ops = tm.ops
+    ops._push_config()
+    ops._bind(vel_div=sec)
+    ncol = a.size * a.size
+    nbytes = (5 * a.nz + 7) * 8 * ncol
+    peak, _ = measured_peaks()
+    kern = {}
+    for name, fn in (("k_enth_column", lambda: ops.column_smooth(dt_s)),
+                     ("k_enth_layer", lambda: ops.layer_smooth(dt_s)),
+                     ("k_enth_residual", lambda: ops.compute_residual(dt_s))):
+        fn()
+        ms = event_time(fn, 5, stream)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        kern[name] = {"launch_ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
+    # the residual call also reads the norm back (one small copy and a sync)
+    st = getattr(ops, "last_stats", None)
+    return {"ms_per_step": t_ms, "steps_per_s": world * 1000.0 / t_ms, "nz": a.nz, "columns": ncol,
+            "sweeps_last_step": int(st.iterations) if st is not None else None,
+            "what": "ThermalModel.step at 2048^2 x nz (binary64), coupled to the solved SSA state",
+            "kernels": kern}
 
 
 # -------------------------------------------------------------- CPU legs
@@ -637,6 +712,9 @@ def main():
         return 0
     if a.mode == "kernels":
         run_kernels(a)
+        return 0
+    if a.mode == "thermal":
+        run_thermal(a)
         return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))

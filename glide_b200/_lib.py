@@ -154,6 +154,7 @@ SIGNATURES.update({
     "glide_enthalpy_set_config": ([_H, ctypes.POINTER(EnthalpyConfig)], _I),
     "glide_enthalpy_get_config": ([_H, ctypes.POINTER(EnthalpyConfig)], _I),
     "glide_enthalpy_set_inputs": ([_H, ctypes.POINTER(EnthalpyInputs)], _I),
+    "glide_enthalpy_set_tuning": ([_H, _I, _I], _I),
     "glide_enthalpy_snapshot": ([_H, _P], _I),
     "glide_enthalpy_set_rhs": ([_H, _P], _I),
     "glide_enthalpy_residual": ([_H, _D, _I, ctypes.POINTER(_D), _P], _I),

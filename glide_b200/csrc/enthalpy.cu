@@ -119,6 +119,8 @@ struct Handle {
     int nblocks = 0;
     glide_enthalpy_config cfg;
     glide_enthalpy_inputs in;
+    int point_blocks = 5;   // resident blocks per SM of the residual / layer kernels (4, 5, 6)
+    int column_blocks = 6;  // of the column kernel (2 to 6)
 
     Handle(int ny_, int nx_, int nz_, double dx_) : ny(ny_), nx(nx_), nz(nz_), dx(dx_) {
         plane = size_t(ny) * nx;
@@ -204,8 +206,24 @@ struct Handle {
     dim3 col_grid() const { return dim3(unsigned(nblocks)); }
 
     void residual(const EnthArgs& a, int use_forcing, cudaStream_t s) {
-        k_enth_residual<<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
+        if (point_blocks == 4) k_enth_residual<4><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
+        else if (point_blocks == 6) k_enth_residual<6><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
+        else k_enth_residual<5><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
         check_launch("enthalpy residual");
+    }
+    void column(const EnthArgs& a, double* out, int mode, cudaStream_t s) {
+        if (column_blocks == 2) k_enth_column<2><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else if (column_blocks == 3) k_enth_column<3><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else if (column_blocks == 5) k_enth_column<5><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else if (column_blocks == 6) k_enth_column<6><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else k_enth_column<4><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        check_launch("enthalpy column smooth");
+    }
+    void layer(const EnthArgs& a, double* out, int mode, cudaStream_t s) {
+        if (point_blocks == 4) k_enth_layer<4><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else if (point_blocks == 6) k_enth_layer<6><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else k_enth_layer<5><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        check_launch("enthalpy layer smooth");
     }
     void finish(int mode, cudaStream_t s) {
         k_enth_finish<<<1, 1024, 0, s>>>(partial, nblocks, ctl, mode, cfg.relative_tolerance,
@@ -289,6 +307,28 @@ int glide_enthalpy_get_config(glide_enthalpy_handle h, glide_enthalpy_config* c)
     });
 }
 
+int glide_enthalpy_set_tuning(glide_enthalpy_handle h, int key, int value) {
+    return guarded([&] {
+        Handle* e = H(h);
+        if (key == GLIDE_ENTH_TUNE_POINT_BLOCKS) {
+            if (value < 4 || value > 6) fail(GLIDE_ERR_ARG, "point blocks per SM must be 4, 5 or 6");
+            e->point_blocks = value;
+        } else if (key == GLIDE_ENTH_TUNE_COLUMN_BLOCKS) {
+            if (value < 2 || value > 6) fail(GLIDE_ERR_ARG, "column blocks per SM must lie in [2, 6]");
+            e->column_blocks = value;
+        } else if (key == GLIDE_ENTH_TUNE_COLUMN_L1) {
+            const int carve = value ? int(cudaSharedmemCarveoutMaxL1) : int(cudaSharedmemCarveoutDefault);
+            ECU(cudaFuncSetAttribute(k_enth_column<2>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+            ECU(cudaFuncSetAttribute(k_enth_column<3>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+            ECU(cudaFuncSetAttribute(k_enth_column<4>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+            ECU(cudaFuncSetAttribute(k_enth_column<5>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+            ECU(cudaFuncSetAttribute(k_enth_column<6>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        } else {
+            fail(GLIDE_ERR_ARG, "unknown enthalpy tuning key");
+        }
+    });
+}
+
 int glide_enthalpy_set_inputs(glide_enthalpy_handle h, const glide_enthalpy_inputs* in) {
     return guarded([&] {
         Handle* e = H(h);
@@ -342,8 +382,7 @@ int glide_enthalpy_column_smooth(glide_enthalpy_handle h, double dt, void* strea
         Handle* e = H(h);
         if (!(dt > 0)) fail(GLIDE_ERR_ARG, "dt must be positive");
         EnthArgs a = e->args(dt, e->f[GLIDE_ENTH_E], false);
-        k_enth_column<<<e->col_grid(), kColThreads, 0, S(stream)>>>(a, e->f[GLIDE_ENTH_DELTA_E], 0);
-        check_launch("enthalpy column smooth");
+        e->column(a, e->f[GLIDE_ENTH_DELTA_E], 0, S(stream));
     });
 }
 
@@ -352,8 +391,7 @@ int glide_enthalpy_layer_smooth(glide_enthalpy_handle h, double dt, void* stream
         Handle* e = H(h);
         if (!(dt > 0)) fail(GLIDE_ERR_ARG, "dt must be positive");
         EnthArgs a = e->args(dt, e->f[GLIDE_ENTH_E], false);
-        k_enth_layer<<<e->col_grid(), kColThreads, 0, S(stream)>>>(a, e->f[GLIDE_ENTH_DELTA_E], 0);
-        check_launch("enthalpy layer smooth");
+        e->layer(a, e->f[GLIDE_ENTH_DELTA_E], 0, S(stream));
     });
 }
 
@@ -373,11 +411,9 @@ int glide_enthalpy_column_sweep(glide_enthalpy_handle h, double dt, int n_iter, 
         e->residual(first, 1, s);
         e->finish(0, s);
         for (int it = 0; it < n_iter; ++it) {
-            k_enth_column<<<e->col_grid(), kColThreads, 0, s>>>(home, e->E_alt, 1);
-            check_launch("enthalpy column smooth");
+            e->column(home, e->E_alt, 1, s);
             if (alternating) {
-                k_enth_layer<<<e->col_grid(), kColThreads, 0, s>>>(alt, E, 1);
-                check_launch("enthalpy layer smooth");
+                e->layer(alt, E, 1, s);
             } else {
                 k_enth_copy<<<1184, 256, 0, s>>>(E, e->E_alt, e->n3, &e->ctl->done);
                 check_launch("enthalpy copy");

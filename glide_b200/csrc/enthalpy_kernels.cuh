@@ -63,29 +63,49 @@ __device__ __forceinline__ double e_pmp(double sigma, double H) {
     return kCI * (T_pmp - kTRef) / kEScale;
 }
 
+// Values of the smoothed switches where their argument is clamped at -20 or
+// +20 (ice colder or warmer than ~2 K / ~2 kJ kg^-1 from the melting point).
+// They are evaluated once per thread from the same expressions, so the
+// clamped branches below return exactly what the general path would.
+struct Clamped {
+    double s_lo, s_hi, sp_lo;
+    __device__ Clamped()
+        : s_lo(1.0 / (1.0 + exp(20.0))), s_hi(1.0 / (1.0 + exp(-20.0))),
+          sp_lo(log(1.0 + exp(-20.0)) / kSharp) {}
+};
+
+// logistic switch 1 / (1 + exp(-z)) with z clamped to [-20, 20]
+__device__ __forceinline__ double switch_of(double z, const Clamped& c) {
+    if (z <= -20.0) return c.s_lo;
+    if (z >= 20.0) return c.s_hi;
+    return 1.0 / (1.0 + exp(-z));
+}
+
 // enthalpy.cu:60-66
-__device__ __forceinline__ double k_diff(double E, double Ep) {
+__device__ __forceinline__ double k_diff(double E, double Ep, const Clamped& c) {
     double z = (E - Ep) * kEScale * kSharp;
-    z = fmin(fmax(z, -20.0), 20.0);
-    double s = 1.0 / (1.0 + exp(-z));
+    double s = switch_of(z, c);
     return kKCold * (1.0 - s + kKTF * s);
 }
 
 // drainage residual and derivative (enthalpy.cu:71-91, :598-640)
 struct Drain { double res, d; };
-__device__ __forceinline__ Drain drainage(double Ek, double Ep, double drain, double h) {
+__device__ __forceinline__ Drain drainage(double Ek, double Ep, double drain, double h, const Clamped& c) {
     double x = (Ek - Ep) * kEScale;
-    double ax = fmin(fmax(kSharp * x, -20.0), 20.0);
-    double sp = (ax > 10.0) ? x : log(1.0 + exp(ax)) / kSharp;
-    double z = fmin(fmax(kSharp * (Ek - Ep) * kEScale, -20.0), 20.0);
-    double s = 1.0 / (1.0 + exp(-z));
+    double ax = kSharp * x;
+    double sp;
+    if (ax <= -20.0) sp = c.sp_lo;
+    else if (ax > 10.0) sp = x;
+    else sp = log(1.0 + exp(ax)) / kSharp;
+    double s = switch_of(kSharp * (Ek - Ep) * kEScale, c);
     return {h * kRhoW * kL * (drain * (sp / kL)) / kEScale, h * kRhoW * kL * drain * (s / kL)};
 }
 
-// Lax-Friedrichs enthalpy flux through a face with mass flux q (enthalpy.cu:573-592)
+// Lax-Friedrichs enthalpy flux through a face with mass flux q; sq = sqrt(1 + lf_c)
+// (enthalpy.cu:573-592)
 struct Flux { double res, dl, dr; };
-__device__ __forceinline__ Flux face_flux(double q, double El, double Er, double lf_c) {
-    double alpha = fabs(q) * sqrt(1.0 + lf_c);
+__device__ __forceinline__ Flux face_flux(double q, double El, double Er, double sq) {
+    double alpha = fabs(q) * sq;
     return {0.5 * q * (El + Er) - 0.5 * alpha * (Er - El), 0.5 * (q + alpha), 0.5 * (q - alpha)};
 }
 
@@ -113,47 +133,66 @@ __device__ __forceinline__ ColumnCtx column_ctx(const EnthArgs& a, int i, int j)
     return x;
 }
 
-// Conservative horizontal advection at (i, j, k) with centre value Ec; the
-// neighbours come from the state array (enthalpy.cu:667-759).
-struct HAdv { double res, diag; };
-__device__ __forceinline__ HAdv horiz(const EnthArgs& a, const ColumnCtx& x, int k, double Ec) {
-    const size_t plane = size_t(a.ny) * a.nx;
-    const double* Ek = a.E + size_t(k) * plane;
+// Mass fluxes H u through the four faces of a column at layer k, with the
+// Lax-Friedrichs thickness flux of the momentum solver (enthalpy.cu:690-745);
+// boundary faces carry none.  With a layer-independent velocity they are
+// the same for every k and are evaluated once per column.
+struct FaceQ { double l, r, t, b; };
+__device__ __forceinline__ FaceQ face_q(const EnthArgs& a, const ColumnCtx& x, int k) {
     const double* uk = a.u + k * a.u_layer + size_t(x.i) * a.ld_u;
     const double* vk = a.v + k * a.v_layer;
-    Flux fl{0, 0, 0}, fr{0, 0, 0}, ft{0, 0, 0}, fb{0, 0, 0};
+    FaceQ q{0.0, 0.0, 0.0, 0.0};
     if (x.j > 0) {
         double ul = uk[x.j] / a.vel_div;
-        double q = 0.5 * (x.Hxm + x.h) * ul - 0.5 * sqrt(ul * ul + kReg) * (x.h - x.Hxm);
-        fl = face_flux(q, Ek[x.c - 1], Ec, a.lf_c);
-    } else {
-        fl = face_flux(0.0, Ec, Ec, a.lf_c);
+        q.l = 0.5 * (x.Hxm + x.h) * ul - 0.5 * sqrt(ul * ul + kReg) * (x.h - x.Hxm);
     }
     if (x.j < a.nx - 1) {
         double ur = uk[x.j + 1] / a.vel_div;
-        double q = 0.5 * (x.h + x.Hxp) * ur - 0.5 * sqrt(ur * ur + kReg) * (x.Hxp - x.h);
-        fr = face_flux(q, Ec, Ek[x.c + 1], a.lf_c);
-    } else {
-        fr = face_flux(0.0, Ec, Ec, a.lf_c);
+        q.r = 0.5 * (x.h + x.Hxp) * ur - 0.5 * sqrt(ur * ur + kReg) * (x.Hxp - x.h);
     }
     if (x.i > 0) {
         double vt = vk[size_t(x.i) * a.ld_v + x.j] / a.vel_div;
-        double q = 0.5 * (x.Hym + x.h) * vt - 0.5 * sqrt(vt * vt + kReg) * (x.Hym - x.h);
-        ft = face_flux(q, Ec, Ek[x.c - a.nx], a.lf_c);
-    } else {
-        ft = face_flux(0.0, Ec, Ec, a.lf_c);
+        q.t = 0.5 * (x.Hym + x.h) * vt - 0.5 * sqrt(vt * vt + kReg) * (x.Hym - x.h);
     }
     if (x.i < a.ny - 1) {
         double vb = vk[size_t(x.i + 1) * a.ld_v + x.j] / a.vel_div;
-        double q = 0.5 * (x.h + x.Hyp) * vb - 0.5 * sqrt(vb * vb + kReg) * (x.h - x.Hyp);
-        fb = face_flux(q, Ek[x.c + a.nx], Ec, a.lf_c);
-    } else {
-        fb = face_flux(0.0, Ec, Ec, a.lf_c);
+        q.b = 0.5 * (x.h + x.Hyp) * vb - 0.5 * sqrt(vb * vb + kReg) * (x.h - x.Hyp);
     }
-    const double dx_inv = 1.0 / a.dx;
+    return q;
+}
+
+// Conservative horizontal advection at (i, j, k) with centre value Ec; the
+// neighbours come from the state array (enthalpy.cu:667-759).  sq =
+// sqrt(1 + lf_c), dx_inv = 1 / dx.
+struct HAdv { double res, diag; };
+__device__ __forceinline__ HAdv horiz(const EnthArgs& a, const ColumnCtx& x, int k, double Ec, const FaceQ& q,
+                                      double sq, double dx_inv) {
+    const size_t plane = size_t(a.ny) * a.nx;
+    const double* Ek = a.E + size_t(k) * plane;
+    Flux fl = x.j > 0 ? face_flux(q.l, Ek[x.c - 1], Ec, sq) : face_flux(0.0, Ec, Ec, sq);
+    Flux fr = x.j < a.nx - 1 ? face_flux(q.r, Ec, Ek[x.c + 1], sq) : face_flux(0.0, Ec, Ec, sq);
+    Flux ft = x.i > 0 ? face_flux(q.t, Ec, Ek[x.c - a.nx], sq) : face_flux(0.0, Ec, Ec, sq);
+    Flux fb = x.i < a.ny - 1 ? face_flux(q.b, Ek[x.c + a.nx], Ec, sq) : face_flux(0.0, Ec, Ec, sq);
     return {kRhoI * ((fr.res - fl.res) + (ft.res - fb.res)) * dx_inv,
             kRhoI * ((fr.dl - fl.dr) + (ft.dl - fb.dr)) * dx_inv};
 }
+
+// Per-column horizontal-advection context: the hoisted face fluxes (valid
+// for every k when the velocity is layer-independent) and the constants.
+struct HCtx {
+    FaceQ q;
+    bool flat;  // velocity independent of the layer
+    double sq, dx_inv;
+    __device__ HCtx(const EnthArgs& a, const ColumnCtx& x) {
+        flat = a.u_layer == 0 && a.v_layer == 0;
+        sq = sqrt(1.0 + a.lf_c);
+        dx_inv = 1.0 / a.dx;
+        q = flat ? face_q(a, x, 0) : FaceQ{0.0, 0.0, 0.0, 0.0};
+    }
+    __device__ HAdv at(const EnthArgs& a, const ColumnCtx& x, int k, double Ec) const {
+        return horiz(a, x, k, Ec, flat ? q : face_q(a, x, k), sq, dx_inv);
+    }
+};
 
 // Vertical terms of row k < nz - 1: sigma advection, diffusion, drainage with
 // their tridiagonal coefficients (enthalpy.cu:217-509).  K_lo / K_up are the
@@ -164,7 +203,7 @@ struct Vert { double adv, dif, drn; double a, b_dif, b_adv, b_drn, c; };
 
 __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, double Ek, double Ekp1,
                                          double Epk, double K_lo, double K_up, double om_m, double om_k,
-                                         double om_p, double h, double h_inv, double dsig) {
+                                         double om_p, double h, double h_inv, double dsig, const Clamped& cl) {
     Vert r{0, 0, 0, 0, 0, 0, 0, 0};
     if (k == 0) {
         const double dsh = 0.5 * dsig, dsh_inv = 1.0 / dsh;
@@ -199,7 +238,7 @@ __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, 
         r.b_dif = dl + du;
     }
     if (a.flags & kTermDrainage) {
-        Drain d = drainage(Ek, Epk, a.drain, h);
+        Drain d = drainage(Ek, Epk, a.drain, h, cl);
         r.drn = d.res;
         r.b_drn = d.d;
     }
@@ -211,7 +250,8 @@ __device__ __forceinline__ bool stopped(const int* done) { return done && *(vola
 // ------------------------------------------------------------- residual
 // enthalpy.cu:784-893.  out (layer-major) = F(E) - f_E, or F(E) without
 // forcing; partial[block] = max |out| over the block's nodes.
-__global__ void __launch_bounds__(kColThreads) k_enth_residual(EnthArgs a, double* out, int use_forcing,
+template <int MINB>
+__global__ void __launch_bounds__(kColThreads, MINB) k_enth_residual(EnthArgs a, double* out, int use_forcing,
                                                                   double* partial) {
     __shared__ double red[kColThreads / 32];
     if (stopped(a.done)) return;
@@ -225,6 +265,8 @@ __global__ void __launch_bounds__(kColThreads) k_enth_residual(EnthArgs a, doubl
         if (x.h < a.h_thin) {
             for (int k = 0; k < nz; ++k) out[k * plane + x.c] = 0.0;
         } else {
+            const Clamped cl;
+            const HCtx hc(a, x);
             const double dsig = 1.0 / double(nz - 1), inv_dt = 1.0 / a.dt;
             const double* E = a.E + x.c;
             const double* om = a.omega + x.c;
@@ -234,10 +276,10 @@ __global__ void __launch_bounds__(kColThreads) k_enth_residual(EnthArgs a, doubl
             double om_m = 0.0, om_k = om[0];
             for (int k = 0; k < nz - 1; ++k) {
                 const double om_p = om[size_t(k + 1) * plane];
-                const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp));
+                const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
                 double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[k * plane + x.c]) * inv_dt;
-                if (a.flags & kTermHorizAdv) r += horiz(a, x, k, Ek).res;
-                Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig);
+                if (a.flags & kTermHorizAdv) r += hc.at(a, x, k, Ek).res;
+                Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
                 r += vt.adv;
                 r += vt.dif;
                 r += vt.drn;
@@ -273,7 +315,8 @@ __global__ void __launch_bounds__(kColThreads) k_enth_residual(EnthArgs a, doubl
 // solve.  mode 0 writes delta_E = E_col - E; mode 1 writes the updated state
 // E + omega_relax (E_col - E).  Rows are assembled and eliminated in one
 // upward pass (Thomas in its c', d' form), then back-substituted.
-__global__ void __launch_bounds__(kColThreads) k_enth_column(EnthArgs a, double* out, int mode) {
+template <int MINB>
+__global__ void __launch_bounds__(kColThreads, MINB) k_enth_column(EnthArgs a, double* out, int mode) {
     if (stopped(a.done)) return;
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= a.ny * a.nx) return;
@@ -295,6 +338,8 @@ __global__ void __launch_bounds__(kColThreads) k_enth_column(EnthArgs a, double*
         return;
     }
     for (int k = 0; k < nz; ++k) El[k] = E[size_t(k) * plane];
+    const Clamped cl;
+    const HCtx hc(a, x);
     const double inv_dt = 1.0 / a.dt;
     const double* om = a.omega + x.c;
     const double bt = kRhoI * x.h * inv_dt;  // time-term diagonal
@@ -305,16 +350,16 @@ __global__ void __launch_bounds__(kColThreads) k_enth_column(EnthArgs a, double*
         for (int k = 0; k < nz - 1; ++k) {
             const double Ek = El[k], Ekp1 = El[k + 1], Ekm1 = k > 0 ? El[k - 1] : 0.0;
             const double om_p = om[size_t(k + 1) * plane];
-            const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp));
+            const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
             const size_t n = size_t(k) * plane + x.c;
             double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[n]) * inv_dt - a.f_E[n];
             double hd = 0.0;
             if (a.flags & kTermHorizAdv) {
-                HAdv ha = horiz(a, x, k, Ek);
+                HAdv ha = hc.at(a, x, k, Ek);
                 r += ha.res;
                 hd = ha.diag;
             }
-            Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig);
+            Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
             r += vt.adv;
             r += vt.dif;
             r += vt.drn;
@@ -349,7 +394,8 @@ __global__ void __launch_bounds__(kColThreads) k_enth_column(EnthArgs a, double*
 // ---------------------------------------------------------- layer smoother
 // enthalpy.cu:1129-1258: pointwise Jacobi, delta = -r / J_kk.  One thread per
 // column walking k.  mode 0 writes delta_E, mode 1 the updated state.
-__global__ void __launch_bounds__(kColThreads) k_enth_layer(EnthArgs a, double* out, int mode) {
+template <int MINB>
+__global__ void __launch_bounds__(kColThreads, MINB) k_enth_layer(EnthArgs a, double* out, int mode) {
     if (stopped(a.done)) return;
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= a.ny * a.nx) return;
@@ -362,6 +408,8 @@ __global__ void __launch_bounds__(kColThreads) k_enth_layer(EnthArgs a, double* 
         for (int k = 0; k < nz; ++k) out[size_t(k) * plane + x.c] = mode ? E[size_t(k) * plane] : 0.0;
         return;
     }
+    const Clamped cl;
+    const HCtx hc(a, x);
     const double dsig = 1.0 / double(nz - 1), inv_dt = 1.0 / a.dt;
     const double* om = a.omega + x.c;
     double Ekm1 = 0.0, Ek = E[0], Ekp1 = E[plane];
@@ -369,16 +417,16 @@ __global__ void __launch_bounds__(kColThreads) k_enth_layer(EnthArgs a, double* 
     double K_lo = 0.0, om_m = 0.0, om_k = om[0];
     for (int k = 0; k < nz - 1; ++k) {
         const double om_p = om[size_t(k + 1) * plane];
-        const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp));
+        const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
         const size_t n = size_t(k) * plane + x.c;
         double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[n]) * inv_dt - a.f_E[n];
         double diag = kRhoI * x.h * inv_dt;
         if (a.flags & kTermHorizAdv) {
-            HAdv ha = horiz(a, x, k, Ek);
+            HAdv ha = hc.at(a, x, k, Ek);
             r += ha.res;
             diag += ha.diag;
         }
-        Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig);
+        Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
         r += vt.adv;
         r += vt.dif;
         r += vt.drn;

@@ -253,6 +253,15 @@ class EnthalpyOperators:
         inp.vel_div = self._vel_div
         _ecall("glide_enthalpy_set_inputs", self._h, ctypes.byref(inp))
 
+    def set_tuning(self, point_blocks_per_sm=None, column_blocks_per_sm=None, column_prefers_l1=None):
+        """Launch shapes of the kernels (no counterpart in the reference)."""
+        if point_blocks_per_sm is not None:
+            _ecall("glide_enthalpy_set_tuning", self._h, 1, int(point_blocks_per_sm))
+        if column_blocks_per_sm is not None:
+            _ecall("glide_enthalpy_set_tuning", self._h, 2, int(column_blocks_per_sm))
+        if column_prefers_l1 is not None:
+            _ecall("glide_enthalpy_set_tuning", self._h, 3, int(bool(column_prefers_l1)))
+
     def _materialize_velocity(self):
         if not self._broadcast:
             return

@@ -112,6 +112,14 @@ int glide_enthalpy_field_ptr(glide_enthalpy_handle h, int field, void** ptr);
 int glide_enthalpy_set_config(glide_enthalpy_handle h, const glide_enthalpy_config* c);
 int glide_enthalpy_get_config(glide_enthalpy_handle h, glide_enthalpy_config* c);
 int glide_enthalpy_set_inputs(glide_enthalpy_handle h, const glide_enthalpy_inputs* in);
+/* Launch shapes, no counterpart in the reference: resident blocks per SM the
+ * residual / layer kernels (4, 5 or 6; default 5) and the column kernel (2 to
+ * 6; default 6) are compiled for, and whether the column kernel prefers the
+ * largest L1 (value 1) for its per-column Thomas arrays. */
+#define GLIDE_ENTH_TUNE_POINT_BLOCKS 1
+#define GLIDE_ENTH_TUNE_COLUMN_BLOCKS 2
+#define GLIDE_ENTH_TUNE_COLUMN_L1 3
+int glide_enthalpy_set_tuning(glide_enthalpy_handle h, int key, int value);
 int glide_enthalpy_snapshot(glide_enthalpy_handle h, void* stream);
 int glide_enthalpy_set_rhs(glide_enthalpy_handle h, void* stream);
 /* max_abs (host, may be NULL) receives max |r_E| and synchronises `stream`. */
