@@ -266,6 +266,18 @@ def step_fn(h, dt):
     return step
 
 
+def reduce_max(value, device, world):
+    """Max of a per-rank figure over all ranks (the slowest replica sets the
+    job's time); identity for a single process."""
+    import torch
+    if world <= 1:
+        return float(value)
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def event_time(fn, n, stream):
     """Average device time of fn() over n calls, CUDA events on `stream`."""
     import torch
@@ -289,6 +301,12 @@ def run_kernels(a):
     f = dome(a.size, a.dx, a.radius, seed=0)
     out, peak, peak_kind, prec = kernel_roofline(a, None, torch.cuda.current_stream(), fields=f, probe=True)
     print(json.dumps({"mode": "kernels", "precision": prec, "peak_gbs": peak, "kernels": out}), flush=True)
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# binary32 fine-level kernels on the 2048^2 workload, from one ncu capture of
+# `python bench.py --mode kernels` on a B200.
+NCU_TRAFFIC_2048_FP32 = {"k_residual": 225.087e6, "k_jvp": 223.795e6, "k_vanka_sweep": 249.767e6}
 
 
 def kernel_roofline(a, h, stream, fields=None, probe=False):
@@ -340,7 +358,9 @@ def kernel_roofline(a, h, stream, fields=None, probe=False):
         fn()
         ms = event_time(fn, 10, stream)
         gbs = nbytes / (ms * 1e-3) / 1e9
-        out[name] = {"launch_ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
+        traffic = NCU_TRAFFIC_2048_FP32.get(name) if (a.size == 2048 and prec == "fp32") else None
+        out[name] = {"launch_ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak,
+                     "traffic": traffic}
     del k
     return out, peak, peak_kind, prec
 
@@ -390,11 +410,7 @@ def run_ours(a, rank, world):
     torch.cuda.synchronize()
     launches = h.launch_count() - l0
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1) / a.steps
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = reduce_max(e0.elapsed_time(e1) / a.steps, dev, world)
     vcyc = float(np.mean([s["vcycles"] for s in stats]))
     final_rel = float(np.max([s["final_norm"] / s["initial_norm"] for s in stats]))
     if a.quick:  # schedule exploration: the solve only
@@ -420,11 +436,7 @@ def run_ours(a, rank, world):
         grad()
         kg = max(1, min(a.steps, 2))
         gstats = []
-        g_ms = event_time(lambda: gstats.append(grad()), kg, stream)
-        tg = torch.tensor([g_ms], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(tg, op=dist.ReduceOp.MAX)
-        g_ms = float(tg.item())
+        g_ms = reduce_max(event_time(lambda: gstats.append(grad()), kg, stream), dev, world)
         grads = {"value": world * 1000.0 / g_ms, "unit": "grads/s", "ms_per_grad": g_ms,
                  "vcycles_per_grad": float(np.mean([s["vcycles"] for s in gstats])),
                  "what": "adjoint FAS solve to rel. residual 1e-8 plus gradients w.r.t. beta, bed, H_prev, smb"}
@@ -458,11 +470,7 @@ def run_ours(a, rank, world):
         out_u.copy_(h.view("u", 0), non_blocking=True)
         out_v.copy_(h.view("v", 0), non_blocking=True)
         out_H.copy_(h.view("H", 0), non_blocking=True)
-    e2e_ms = event_time(e2e_step, k_e2e, stream)
-    te = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te.item())
+    e2e_ms = reduce_max(event_time(e2e_step, k_e2e, stream), dev, world)
     itemsize = 4 if dtype == torch.float32 else 8
     h2d = sum(host[k].numel() * itemsize for k in ("bed", "beta", "smb")) + out_H.numel() * itemsize
     d2h = (out_u.numel() + out_v.numel() + out_H.numel()) * itemsize
@@ -477,11 +485,7 @@ def run_ours(a, rank, world):
         pstep = step_fn(hp_, ar.dt)
         pstep()
         pst = []
-        p_ms = event_time(lambda: pst.append(pstep()), 2, stream)
-        tp = torch.tensor([p_ms], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(tp, op=dist.ReduceOp.MAX)
-        p_ms = float(tp.item())
+        p_ms = reduce_max(event_time(lambda: pst.append(pstep()), 2, stream), dev, world)
         plain = {"ms_per_step": p_ms, "steps_per_s": world * 1000.0 / p_ms,
                  "vcycles_per_step": float(np.mean([s["vcycles"] for s in pst])),
                  "final_relative_residual": float(np.max([s["final_norm"] / s["initial_norm"] for s in pst])),
@@ -524,7 +528,7 @@ def run_ours(a, rank, world):
                         "memory, forward solve, u, v, H back to the host"},
         "roofline": {"bound": "hbm", "kernel": f"{dom} (fine level, {kprec}, step-start state)",
                      "achieved": kd["achieved_gbs"], "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": kd["frac"], "traffic": None, "launch_ms": kd["launch_ms"],
+                     "frac": kd["frac"], "traffic": kd["traffic"], "launch_ms": kd["launch_ms"],
                      "algorithmic_bytes_per_launch": kd["algorithmic_bytes"], "kernels": kernels},
         "clocks": clocks,
     }
@@ -571,12 +575,7 @@ def thermal_leg(a, h, f, stream, dev, world):
         tm.pre_momentum()
         tm.step(dt_s)
     tstep()
-    t_ms = event_time(tstep, 3, stream)
-    tt = torch.tensor([t_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    t_ms = float(tt.item())
+    t_ms = reduce_max(event_time(tstep, 3, stream), dev, world)
     ops = tm.ops
     ops._push_config()
     ops._bind(vel_div=sec)

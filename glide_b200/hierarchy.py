@@ -157,6 +157,7 @@ class Hierarchy:
 
     def set_reference_quirks(self, on: bool):
         call("glide_set_reference_quirks", self._h, int(bool(on)))
+        self.reference_quirks = bool(on)
 
     def set_use_graphs(self, on: bool):
         call("glide_set_use_graphs", self._h, int(bool(on)))

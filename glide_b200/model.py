@@ -58,9 +58,19 @@ class IceDynamics:
     def backward(self, t, dt, dJdu=None, dJdv=None, dJdH=None, compute_beta_grad=True,
                  compute_bed_grad=True, compute_H_prev_grad=True, compute_smb_grad=True):
         """Adjoint solve with forcing -dJ/dx, then the parameter gradients
-        (glide/model.py:74-94)."""
+        (glide/model.py:74-94).
+
+        The reference starts each adjoint solve from the previous lambda.  Its
+        lambda on the Dirichlet faces is left unconstrained by the adjoint
+        residual yet enters the gradient kernels, so a gradient depends on
+        which solve ran before it.  Reference mode keeps that; native mode
+        (reference_quirks=False) starts every solve from lambda = 0, which
+        makes each gradient a function of this step's inputs alone."""
         h = self.mg.hierarchy
         top = self.top_level
+        if not getattr(h, "reference_quirks", True):
+            for name in ("lambda_u", "lambda_v", "lambda_H"):
+                h.set(name, top, 0.0, restrict_down=True)
         for name, g in (("adj_f_u", dJdu), ("adj_f_v", dJdv), ("adj_f_H", dJdH)):
             if g is None:
                 h.set(name, top, 0.0)
