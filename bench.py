@@ -73,10 +73,14 @@ def parse(argv=None):
     ap.add_argument("--no-grads", action="store_true", help="skip timing the adjoint (gradient) solve")
     ap.add_argument("--no-thermal", action="store_true", help="skip timing the enthalpy (thermal) step")
     ap.add_argument("--nz", type=int, default=41, help="sigma levels of the enthalpy columns")
+    ap.add_argument("--members", type=int, default=64, help="ensemble mode: members")
+    ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
+    ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
+    ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
     ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
-    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels", "thermal"],
+    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels", "thermal", "ensemble"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -551,6 +555,66 @@ def run_thermal(a):
     print(json.dumps({"mode": "thermal", "size": a.size, **out}), flush=True)
 
 
+def run_ensemble(a):
+    """The batched-ensemble workload: `--members` independent domes of uneven
+    sizes drawn from {128, 192, 256, 384, 512, 768}^2 (dx 1500 m, levels down to
+    a coarsest grid >= 16^2, radius U(200, 600) km, log-normal beta, smb lapse
+    U(1e-3, 3e-3) /m), each step a forward solve and an adjoint solve to a
+    relative residual of 1e-8, the solver schedule autotuned per size class
+    among Newton, short FASCD and the classic FASCD schedule; members run
+    concurrently (see glide_b200.ensemble)."""
+    import torch
+    from cases import dome
+    from glide_b200.ensemble import Ensemble, member_specs
+    from glide_b200.model import IceDynamics
+    specs = member_specs(a.members, seed=0)
+    max_cycles = max(a.max_vcycles, 100)  # small steep domes need up to ~60 classic cycles
+    members = []
+    for sp in specs:
+        f = dome(sp.n, sp.dx, sp.radius, seed=sp.seed, lapse=sp.lapse)
+        m = IceDynamics(n_levels=sp.levels, ny=sp.n, nx=sp.n, dx=sp.dx, reference_quirks=False,
+                        precision=a.ens_precision)
+        mg = m.mg
+        for k, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
+            getattr(grp, k).set(torch.as_tensor(f[k]))
+        mg.state.H.set(torch.as_tensor(f["H"]))
+        mg.state.H_prev.set(torch.as_tensor(f["H_prev"]))
+        m.forward_solver.fas_options.set(maximum_vcycles=max_cycles, relative_tolerance=a.rtol,
+                                         absolute_tolerance=0.0, report_norms=False)
+        m.adjoint_solver.fas_options.set(maximum_vcycles=max_cycles, relative_tolerance=a.rtol,
+                                         absolute_tolerance=0.0, report_norms=False)
+        members.append(m)
+    ens = Ensemble(members, workers=a.ens_workers)
+    t0 = time.perf_counter()
+    chosen = ens.autotune(a.dt)
+    tune_s = time.perf_counter() - t0
+    dJ = lambda k, m: (0.05 * m.mg.levels[0].state.u.data, 0.05 * m.mg.levels[0].state.v.data, None)
+
+    def step(t):
+        fs = ens.forward(t, a.dt)
+        bs = ens.backward(t, a.dt, dJ)
+        return fs, bs
+    step(0.0)
+    stream = torch.cuda.current_stream()
+    stats = []
+    ms = event_time(lambda: stats.append(step(0.0)), a.ens_steps, stream)
+    ens.close()
+    cells = sum(sp.n * sp.n for sp in specs)
+    fv = [s["vcycles"] for fs, _ in stats for s in fs]
+    bv = [s["vcycles"] for _, bs in stats for s in bs]
+    rels = [s["final_norm"] / s["initial_norm"] for fs, _ in stats for s in fs if s["initial_norm"] > 0]
+    worst = max(rels)
+    converged = float(np.mean([r <= a.rtol for r in rels]))
+    return {"members": a.members, "steps": a.ens_steps, "ms_per_ensemble_step": ms,
+            "member_steps_per_s": a.members * 1000.0 / ms, "cells_total": cells,
+            "sizes": {str(n): sum(1 for sp in specs if sp.n == n) for n in sorted({sp.n for sp in specs})},
+            "schedules": {str(k): v for k, v in chosen.items()}, "autotune_s": tune_s,
+            "mean_forward_cycles": float(np.mean(fv)), "mean_adjoint_cycles": float(np.mean(bv)),
+            "worst_forward_relative_residual": worst, "forward_solves_converged": converged,
+            "max_cycles": max_cycles, "workers": ens.workers,
+            "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
+
+
 def thermal_leg(a, h, f, stream, dev, world):
     """The enthalpy column solve coupled to the solved state: ThermalModel
     steps (omega, frictional heating, forcing, up to 10 column/layer sweeps
@@ -714,6 +778,9 @@ def main():
         return 0
     if a.mode == "thermal":
         run_thermal(a)
+        return 0
+    if a.mode == "ensemble":
+        print(json.dumps({"mode": "ensemble", **run_ensemble(a)}), flush=True)
         return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))

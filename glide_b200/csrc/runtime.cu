@@ -646,14 +646,19 @@ struct Solver : SolverBase {
             st->history[0] = r0;
         }
         // Newton safeguard: two consecutive steps that fail to cut the residual
-        // by `newton_stall_ratio` hand the rest of the solve back to FASCD
+        // by `newton_stall_ratio` hand the rest of the solve back to FASCD.  On
+        // a mixed handle those FASCD cycles run in binary64: the binary32
+        // defect correction stops near the binary32 rounding level of the
+        // residual.
         bool newton_off = false;
         int stall = 0;
         double prev = ab;
         while (rel > c.relative_tolerance && ab > c.absolute_tolerance && it < c.maximum_vcycles) {
             // forward solves may finish with Newton steps once the FAS phase is close
             int k = kind;
-            if ((kind == 0 || kind == 2) && forward_method == 1 && rel <= newton_switch && !newton_off) k = 4;
+            const bool newton_phase = (kind == 0 || kind == 2) && forward_method == 1 && rel <= newton_switch;
+            if (newton_phase && !newton_off) k = 4;
+            else if (newton_phase && kind == 2) k = 0;
             if (k == 4 && !in_newton) {
                 newton_prologue(start, dt, s);
                 in_newton = true;

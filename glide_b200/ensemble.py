@@ -1,0 +1,180 @@
+"""Ensembles of independent ice-sheet members of uneven grid sizes.
+
+Each member is an `IceDynamics` on its own hierarchy (own device arena, own
+captured V-cycle graphs).  `Ensemble` drives them concurrently: members are
+dealt to a fixed pool of host workers, each worker owns a CUDA stream and
+always serves the same members (handles are single-threaded), and the C-ABI
+calls release the interpreter lock, so the GPU runs kernels of many members
+at once.  A member's convergence checks synchronise only its own stream.
+
+`Ensemble.autotune` picks, per size class, the fastest of a few solver
+schedules by timing one step of the class's first member on a copy of its
+state.
+
+No counterpart in the reference (its models run one grid at a time); the
+members themselves are the reference-compatible `IceDynamics`.
+"""
+from __future__ import annotations
+
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from .model import IceDynamics
+
+STATE = ("u", "v", "H", "H_prev", "phi", "mask")
+
+
+def levels_for(n: int, min_coarse: int = 16, max_levels: int = 8) -> int:
+    """Most levels such that n halves exactly down to a coarsest grid of at
+    least `min_coarse` cells."""
+    levels = 1
+    while levels < max_levels and n % (2 ** levels) == 0 and n // (2 ** levels) >= min_coarse:
+        levels += 1
+    return levels
+
+
+@dataclass
+class MemberSpec:
+    n: int
+    dx: float
+    levels: int
+    radius: float
+    seed: int
+    lapse: float
+
+
+def member_specs(n_members: int, seed: int = 0, sizes=(128, 192, 256, 384, 512, 768), dx: float = 1500.0,
+                 radius=(200e3, 600e3), lapse=(1e-3, 3e-3), min_coarse: int = 16) -> list[MemberSpec]:
+    """Seeded uneven ensemble: sizes drawn from `sizes`, dome radius and smb
+    lapse rate drawn uniformly, levels down to a coarsest grid >= min_coarse."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_members):
+        n = int(rng.choice(sizes))
+        R = float(rng.uniform(*radius))
+        # the dome must fit the domain
+        R = min(R, 0.45 * n * dx)
+        out.append(MemberSpec(n=n, dx=dx, levels=levels_for(n, min_coarse), radius=R,
+                              seed=int(rng.integers(1 << 30)), lapse=float(rng.uniform(*lapse))))
+    return out
+
+
+# solver schedules the autotuner chooses among (applied through the options API)
+CANDIDATES = {
+    "fast": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="newton", switch=2,
+                 tangent=(4, 4, 0, 20)),
+    "fascd": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="fascd", switch=None,
+                  tangent=None),
+    "classic": dict(quirks=False, schedule=(10, 20, 50, 200), newton_steps=30, method="fascd", switch=None,
+                    tangent=None),
+}
+FALLBACK = "classic"
+
+
+def apply_schedule(model: IceDynamics, cfg: dict):
+    h = model.mg.hierarchy
+    h.set_reference_quirks(cfg["quirks"])
+    pre, post, fin, coarse = cfg["schedule"]
+    h.set_fas(False, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
+    h.set_vanka(False, -1, newton_steps=cfg["newton_steps"])
+    h.set_tuning(forward_method=cfg["method"], newton_switch_exp10=cfg["switch"])
+    if cfg["tangent"]:
+        pre, post, fin, coarse = cfg["tangent"]
+        h.set_fas(2, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
+
+
+class Ensemble:
+    """Concurrent driver of independent members (see the module text)."""
+
+    def __init__(self, members: list[IceDynamics], workers: int | None = None):
+        self.members = list(members)
+        n = len(self.members)
+        self.workers = max(1, min(workers or min(n, 16), n))
+        # members dealt round-robin, largest first, so workers get even loads
+        order = sorted(range(n), key=lambda k: -self.members[k].mg.hierarchy.shapes[0][0] ** 2)
+        self._groups = [[] for _ in range(self.workers)]
+        for r, k in enumerate(order):
+            self._groups[r % self.workers].append(k)
+        self._pool = ThreadPoolExecutor(max_workers=self.workers)
+        self._streams = [None] * self.workers
+        self.schedules: dict[int, str] = {}
+
+    def close(self):
+        self._pool.shutdown(wait=True)
+
+    def _run(self, fn):
+        """fn(k, model) for every member, each worker on its own stream;
+        returns the results in member order."""
+        res = [None] * len(self.members)
+        caller = torch.cuda.current_stream()
+        start = torch.cuda.Event()
+        start.record(caller)
+
+        def work(w):
+            if self._streams[w] is None:
+                self._streams[w] = torch.cuda.Stream()
+            s = self._streams[w]
+            s.wait_event(start)
+            with torch.cuda.stream(s):
+                for k in self._groups[w]:
+                    res[k] = fn(k, self.members[k])
+            done = torch.cuda.Event()
+            done.record(s)
+            return done
+
+        events = list(self._pool.map(work, range(self.workers)))
+        for e in events:
+            caller.wait_event(e)
+        return res
+
+    def forward(self, t: float, dt: float, update_geometry: bool = True):
+        return self._run(lambda k, m: m.forward(t, dt, update_geometry=update_geometry))
+
+    def backward(self, t: float, dt: float, dJ):
+        """dJ(k, model) -> (dJdu, dJdv, dJdH) per member; returns the adjoint stats."""
+        def one(k, m):
+            du, dv, dH = dJ(k, m)
+            return m.backward(t, dt, dJdu=du, dJdv=dv, dJdH=dH)
+        return self._run(one)
+
+    def autotune(self, dt: float, candidates: dict | None = None) -> dict[int, str]:
+        """Per size class: time one forward step of the class's first member
+        from its current state with every candidate schedule (state restored
+        after each trial), keep the fastest for the whole class."""
+        candidates = candidates or CANDIDATES
+        classes: dict[int, list[int]] = {}
+        for k, m in enumerate(self.members):
+            classes.setdefault(m.mg.hierarchy.shapes[0][0], []).append(k)
+        chosen = {}
+        for n, ks in sorted(classes.items()):
+            m = self.members[ks[0]]
+            h = m.mg.hierarchy
+            saved = {f: h.get(f, 0) for f in STATE}
+            best, best_t = None, float("inf")
+            for name, cfg in candidates.items():
+                apply_schedule(m, cfg)
+                for trial in range(2):  # the first run captures the V-cycle graphs
+                    for f, v in saved.items():
+                        h.set(f, 0, v, restrict_down=True)
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    st = m.forward(0.0, dt, update_geometry=False)
+                    torch.cuda.synchronize()
+                    el = time.perf_counter() - t0
+                ok = st["final_norm"] <= max(h.get_fas(False)["relative_tolerance"] * st["initial_norm"],
+                                             h.get_fas(False)["absolute_tolerance"])
+                if ok and el < best_t:
+                    best, best_t = name, el
+            best = best or FALLBACK
+            for f, v in saved.items():
+                h.set(f, 0, v, restrict_down=True)
+            for k in ks:
+                apply_schedule(self.members[k], candidates[best])
+                self.schedules[k] = best
+            chosen[n] = best
+        return chosen
+

@@ -11,14 +11,16 @@ class IceDynamics:
     """Momentum + mass conservation (SSA) on a multigrid hierarchy."""
 
     def __init__(self, mg: Multigrid | None = None, n_levels=None, grid=None, ny=None, nx=None, dx=None,
-                 x0=0.0, y0=0.0, crs=None, dtype=torch.float64, reference_quirks=True):
+                 x0=0.0, y0=0.0, crs=None, dtype=torch.float64, reference_quirks=True, precision=None):
+        """precision: None (from dtype), "fp64", "fp32" or "mixed" (binary64
+        state and residual, binary32 smoother and tangent multigrid)."""
         if mg is not None:
             self.mg = mg
         elif grid is not None and n_levels is not None:
-            self.mg = Multigrid(n_levels, finest_grid=grid, reference_quirks=reference_quirks)
+            self.mg = Multigrid(n_levels, finest_grid=grid, reference_quirks=reference_quirks, precision=precision)
         elif ny and nx and dx and n_levels:
             self.mg = Multigrid(n_levels, ny=ny, nx=nx, dx=dx, x0=x0, y0=y0, crs=crs, dtype=dtype,
-                                reference_quirks=reference_quirks)
+                                reference_quirks=reference_quirks, precision=precision)
         else:
             raise ValueError("Must supply either (a) a multigrid object (b) a grid and number of levels "
                              "(c) ny/nx/dx and number of levels")

@@ -25,13 +25,13 @@ class Multigrid:
 
     def __init__(self, n_levels: int, finest_grid: Grid | None = None, ny=None, nx=None, dx=None,
                  x0=0.0, y0=0.0, crs=None, use_fast_math=True, dtype=torch.float64,
-                 reference_quirks: bool = True, use_graphs: bool = True):
+                 reference_quirks: bool = True, use_graphs: bool = True, precision: str | None = None):
         if finest_grid is not None:
             ny, nx, dx = finest_grid.ny, finest_grid.nx, finest_grid.dx
             x0, y0, crs = finest_grid.x0, finest_grid.y0, finest_grid.crs
             dtype = finest_grid._hier.dtype
         self.hierarchy = Hierarchy(ny, nx, dx, n_levels, dtype=dtype, reference_quirks=reference_quirks,
-                                   use_graphs=use_graphs)
+                                   use_graphs=use_graphs, precision=precision)
         self.n_levels = n_levels
         self.levels = []
         for l in range(n_levels):

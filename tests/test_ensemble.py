@@ -1,0 +1,76 @@
+"""Ensemble of uneven members: member layout on the CPU, and on the GPU the
+concurrent driver gives bit-identical results to running every member alone
+(members are independent; streams and threads change no arithmetic)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+
+def test_levels_for_reaches_coarsest_at_least_16():
+    from glide_b200.ensemble import levels_for
+    assert [levels_for(n) for n in (128, 192, 256, 384, 512, 768)] == [4, 4, 5, 5, 6, 6]
+    for n in (128, 192, 256, 384, 512, 768):
+        L = levels_for(n)
+        assert n % 2 ** (L - 1) == 0 and n // 2 ** (L - 1) >= 16
+        assert n % 2 ** L != 0 or n // 2 ** L < 16  # one more level would break the rule
+
+
+def test_member_specs_are_seeded_and_uneven():
+    from glide_b200.ensemble import member_specs
+    a, b = member_specs(64, seed=3), member_specs(64, seed=3)
+    assert a == b
+    assert len({m.n for m in a}) >= 5
+    for m in a:
+        assert 0 < m.radius <= 600e3 and 1e-3 <= m.lapse <= 3e-3
+        assert m.radius <= 0.45 * m.n * m.dx
+
+
+def _member(n, seed, levels=3, dx=4000.0):
+    from cases import dome
+    from glide_b200.model import IceDynamics
+    f = dome(n, dx, R=0.4 * n * dx, seed=seed)
+    m = IceDynamics(n_levels=levels, ny=n, nx=n, dx=dx, reference_quirks=False)
+    mg = m.mg
+    for k, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
+        getattr(grp, k).set(torch.as_tensor(f[k]))
+    mg.state.H.set(torch.as_tensor(f["H"]))
+    mg.state.H_prev.set(torch.as_tensor(f["H_prev"]))
+    m.forward_solver.fas_options.set(maximum_vcycles=6, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                     report_norms=False)
+    m.adjoint_solver.fas_options.set(maximum_vcycles=3, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                     report_norms=False)
+    return m
+
+
+@pytest.mark.gpu
+def test_concurrent_members_match_solo_runs():
+    from glide_b200.ensemble import Ensemble
+    sizes = [64, 96, 128, 64, 96]
+
+    def run(concurrent):
+        members = [_member(n, seed=10 + k) for k, n in enumerate(sizes)]
+        dJ = lambda k, m: (0.05 * m.mg.levels[0].state.u.data, 0.05 * m.mg.levels[0].state.v.data, None)
+        if concurrent:
+            ens = Ensemble(members, workers=3)
+            for step in range(2):
+                ens.forward(step * 10.0, 10.0)
+            ens.backward(20.0, 10.0, dJ)
+            torch.cuda.synchronize()
+            ens.close()
+        else:
+            for m in members:
+                for step in range(2):
+                    m.forward(step * 10.0, 10.0)
+                du, dv, _ = dJ(0, m)
+                m.backward(20.0, 10.0, dJdu=du, dJdv=dv)
+            torch.cuda.synchronize()
+        return [{k: m.mg.hierarchy.get(k, 0).cpu().numpy() for k in ("u", "v", "H", "lambda_u", "grad_beta")}
+                for m in members]
+
+    a, b = run(True), run(False)
+    for ma, mb in zip(a, b):
+        for k in ma:
+            np.testing.assert_array_equal(ma[k], mb[k], err_msg=k)
