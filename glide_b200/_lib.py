@@ -116,6 +116,7 @@ SIGNATURES = {
     "glide_compute_phi": ([_H, _I, _D, _P], _I),
     "glide_residual": ([_H, _I, _D, _I, ctypes.POINTER(_D), _P], _I),
     "glide_vanka_sweep": ([_H, _I, _D, _I, _I, _P, _P], _I),
+    "glide_vanka_dump": ([_H, _I, _D, _P, _P, _P], _I),
     "glide_forward": ([_H, _D, _I, ctypes.POINTER(Stats), _P], _I),
     "glide_adjoint_residual": ([_H, _I, _D, ctypes.POINTER(_D), _P], _I),
     "glide_vjp": ([_H, _I, _D, _P], _I),

@@ -119,6 +119,51 @@ __global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a) {
     }
 }
 
+// -------------------------------------------------------------------------
+// Local 5x5 Vanka systems of every cell for inspection (vanka.cu:801-908,
+// operators.py:253-273): the Newton matrix and residual of the cell's five
+// unknowns at the current state -- no damping terms -- with the Dirichlet and
+// active-set rows pinned as the smoother pins them.  J (ny*nx, 25) row-major,
+// r (ny*nx, 5), both contiguous.
+// -------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(256) k_vanka_dump(ResidualArgs<R> a, R* Jout, R* rout) {
+    using TileT = Tile<R, kTile, 1, 1>;
+    constexpr int NC = TileT::NC;
+    __shared__ TileT t;
+    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int ny = a.ny, nx = a.nx;
+    stage_tile<R, kTile, 1, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
+    __syncthreads();
+    TileView<R, kTile, 1, 1> s{t, i0, j0, ny, nx};
+    for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
+        int r = k / NC, c = k % NC;
+        int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        R Bc = ldg(&a.B.p[size_t(clampi(gi, 0, ny - 1)) * a.B.pitch + clampi(gj, 0, nx - 1)]);
+        t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x / kTile, j = j0 + threadIdx.x % kTile;
+    if (i >= ny || j >= nx) return;
+    R x[5] = {s.U(i, j), s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.Hc(i, j)};
+    R J[25], r[5];
+    local_system<R>(s, a.p, i, j, x, J, r);
+    r[0] -= a.f_u.at(i, j); r[1] -= a.f_u.at(i, j + 1);
+    r[2] -= a.f_v.at(i, j); r[3] -= a.f_v.at(i + 1, j);
+    r[4] -= a.f_H.at(i, j);
+    if (j == 0) { pin(J, 0); r[0] = x[0]; }
+    if (j == nx - 1) { pin(J, 1); r[1] = x[1]; }
+    if (i == 0) { pin(J, 2); r[2] = x[2]; }
+    if (i == ny - 1) { pin(J, 3); r[3] = x[3]; }
+    const R thk = a.gamma.at(i, j);
+    if ((x[4] - a.p.dt * r[4]) <= thk) { pin(J, 4); r[4] = x[4] - thk; }
+    const size_t c = size_t(i) * nx + j;
+#pragma unroll
+    for (int q = 0; q < 25; ++q) Jout[c * 25 + q] = J[q];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) rout[c * 5 + q] = r[q];
+}
+
 // Sum the per-block partials in a fixed order and take square roots:
 // out[0..2] = |r_u|, |r_v|, |r_H|; out[3] = sqrt of their squares' sum.
 __global__ void k_finish_norms(const double* partial, int nblocks, double* out);

@@ -332,6 +332,21 @@ struct Solver : SolverBase {
         }
     }
 
+    void vanka_dump(int l, double dt, R* J, R* r, cudaStream_t s) {
+        Level<R>& v = lv[l];
+        ResidualArgs<R> a;
+        a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
+        a.phi = v.a[GLIDE_PHI]; a.mask = v.a[GLIDE_MASK]; a.bed = v.a[GLIDE_BED]; a.B = v.a[GLIDE_B];
+        a.beta = v.a[GLIDE_BETA]; a.gamma = v.a[GLIDE_GAMMA];
+        a.f_u = v.a[GLIDE_F_U]; a.f_v = v.a[GLIDE_F_V]; a.f_H = v.a[GLIDE_F_H];
+        a.partial = nullptr;
+        a.p = physr(l, dt, false);
+        a.ny = v.ny; a.nx = v.nx;
+        a.use_forcing = 1; a.use_mask = 0; a.active_set = 0;
+        k_vanka_dump<R><<<dim3(v.blocks_x(), v.blocks_y()), 256, 0, s>>>(a, J, r);
+        counted("vanka_dump");
+    }
+
     void read_norms(double out[4], cudaStream_t s) {
         GCU(cudaMemcpyAsync(norms_host, norms_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
         GCU(cudaStreamSynchronize(s));
@@ -1233,6 +1248,17 @@ int glide_vanka_sweep(glide_handle h, int level, double dt, int n, int flags, in
             s.check_level(level);
             s.sweeps(level, dt, n, kGammaArray, (flags & GLIDE_FREEZE_CALVING) != 0,
                      (flags & GLIDE_FREEZE_PHI) != 0, newton_iters, S(stream));
+        });
+    });
+}
+
+int glide_vanka_dump(glide_handle h, int level, double dt, void* J, void* r, void* stream) {
+    return guarded([&] {
+        if (!J || !r) fail(GLIDE_ERR_ARG, "null output array");
+        dispatch(h, [&](auto& s) {
+            using RT = std::remove_pointer_t<decltype(s.lv[0].a[0].p)>;
+            s.check_level(level);
+            s.vanka_dump(level, dt, static_cast<RT*>(J), static_cast<RT*>(r), S(stream));
         });
     });
 }

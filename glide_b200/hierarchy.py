@@ -201,6 +201,15 @@ class Hierarchy:
         p = ctypes.c_void_p(newton_iters.data_ptr()) if newton_iters is not None else None
         call("glide_vanka_sweep", self._h, int(level), float(dt), int(n), int(flags), p, _stream_ptr())
 
+    def vanka_dump(self, level: int, dt: float):
+        """Local 5x5 Vanka systems (J (ny*nx, 25), r (ny*nx, 5)) of every cell."""
+        ny, nx, _ = self.shapes[level]
+        J = torch.empty((ny * nx, 25), dtype=self.dtype, device="cuda")
+        r = torch.empty((ny * nx, 5), dtype=self.dtype, device="cuda")
+        call("glide_vanka_dump", self._h, int(level), float(dt), ctypes.c_void_p(J.data_ptr()),
+             ctypes.c_void_p(r.data_ptr()), _stream_ptr())
+        return J, r
+
     def forward(self, dt: float, start_level: int = 0) -> dict:
         st = _lib.Stats()
         call("glide_forward", self._h, float(dt), int(start_level), ctypes.byref(st), _stream_ptr())

@@ -126,6 +126,12 @@ class ForwardOperators:
             self._h.vanka_sweep(self._l, dt, 1, flags, newton_iters)
             hook(i)
 
+    def vanka_dump(self, dt):
+        """Local 5x5 Vanka matrices and residuals of every cell at the current
+        state (glide/operators.py:253-273); returns new tensors J (ny*nx, 25)
+        and r (ny*nx, 5)."""
+        return self._h.vanka_dump(self._l, dt)
+
     def vanka_smooth(self, dt, freeze_calving=False, freeze_phi=False):
         """One smoother pass.  Unlike the reference, the update is applied in the
         same fused kernel (there are no separate delta buffers)."""

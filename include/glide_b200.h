@@ -168,6 +168,11 @@ int glide_compute_phi(glide_handle h, int level, double relaxation, void* stream
 int glide_residual(glide_handle h, int level, double dt, int flags, double* norms3, void* stream);
 int glide_vanka_sweep(glide_handle h, int level, double dt, int n, int flags, int* newton_iters,
                       void* stream);
+/* Local 5x5 Vanka systems of every cell of a level at its current state
+ * (ForwardOperators.vanka_dump, glide/operators.py:253-273, glide/cuda/vanka.cu:801-908):
+ * J (ny*nx x 25, row-major per cell) and r (ny*nx x 5), device arrays of the
+ * handle's value type (binary64 for GLIDE_F64 and GLIDE_MIXED). */
+int glide_vanka_dump(glide_handle h, int level, double dt, void* J, void* r, void* stream);
 int glide_forward(glide_handle h, double dt, int start_level, glide_stats* stats, void* stream);
 
 int glide_adjoint_residual(glide_handle h, int level, double dt, double* norms3, void* stream);

@@ -163,6 +163,14 @@ class OracleLevel:
             self.v += w * self.d_v
             self.H += w * self.d_H
 
+    def vanka_dump(self, dt):
+        """ForwardOperators.vanka_dump, glide/operators.py:253-273: the local
+        5x5 systems of every cell at the current state and phi."""
+        J = np.zeros((self.ny * self.nx, 25), self.dtype)
+        r = np.zeros((self.ny * self.nx, 5), self.dtype)
+        getattr(lib(), "go_vanka_dump_" + self.suf)(*self._level_args(dt), _p(J), _p(r))
+        return J, r
+
     def vjp(self, dt, lam, use_forcing, out, f=None):
         getattr(lib(), "go_vjp_" + self.suf)(
             *self._level_args(dt, f=f), *[_p(a) for a in lam], ctypes.c_int(1 if use_forcing else 0),

@@ -163,6 +163,24 @@ def random_cases(glide):
     np.savez_compressed(HERE / "random_adjoint_f64.npz", **out)
 
 
+def vanka_dump_case(glide):
+    """ForwardOperators.vanka_dump (glide/operators.py:253-273) on the random
+    state: the local 5x5 systems of every cell."""
+    st = random_state(40, 56, seed=7)
+    dt = 5.0
+    g = random_grid(glide, st, calving=1.0)
+    ops = g.forward_operators
+    ops.set_rhs(dt)
+    ops.compute_phi()
+    J, r = ops.vanka_dump(dt)
+    out = {f"in_{k}": v for k, v in st.items()}
+    out["in_phi"] = np.array(g.state.phi.data)
+    out["in_gamma"] = np.array(ops.gamma)
+    out["out_J"] = np.array(J)
+    out["out_r"] = np.array(r)
+    np.savez_compressed(HERE / "random_vanka_dump_f64.npz", **out)
+
+
 def enthalpy_cases(glide):
     """EnthalpyOperators (glide/enthalpy.py) on a rough random state: residual,
     one column smooth, one layer smooth, omega, and column sweeps; then one
@@ -247,15 +265,19 @@ def enthalpy_cases(glide):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", default=None, help="enthalpy: only the enthalpy fixtures")
+    ap.add_argument("--only", default=None, help="enthalpy | dump: only those fixtures")
     a = ap.parse_args(argv)
     if a.only == "enthalpy":
         enthalpy_cases(load_reference(fp64=True, reference=a.reference))
+        return
+    if a.only == "dump":
+        vanka_dump_case(load_reference(fp64=True, reference=a.reference))
         return
     glide = load_reference(fp64=True, reference=a.reference)
     c1_forward_and_adjoint(glide, "f64")
     random_cases(glide)
     enthalpy_cases(glide)
+    vanka_dump_case(glide)
     glide32 = load_reference(fp64=False, reference=a.reference)
     c1_forward_and_adjoint(glide32, "f32")
     for p in sorted(HERE.glob("*.npz")):

@@ -198,3 +198,17 @@ def test_adjoint_converges_to_reference_adjoint(precision):
         assert rel_err(got[k], ref[k]) <= 1e-8, k
     for k in ("grad_beta", "grad_bed"):
         assert rel_err(got[k], ref[k]) <= 1e-7, k
+
+
+def test_vanka_dump_matches_reference():
+    """ForwardOperators.vanka_dump: the local 5x5 Vanka systems of every cell."""
+    g = load_golden("random_vanka_dump_f64")
+    ny, nx = g["in_H"].shape
+    h = _hier(ny, nx, 1500.0)
+    for k in ("u", "v", "H", "H_prev", "bed", "B", "beta", "smb", "phi", "gamma", "f_u", "f_v"):
+        h.set(k, 0, torch.as_tensor(g[f"in_{k}"]))
+    h.set_phys(0, calving_rate=1.0)
+    h.set_rhs(0, DT)
+    J, r = h.vanka_dump(0, DT)
+    assert rel_err(_np(J), g["out_J"]) <= 1e-12
+    assert rel_err(_np(r), g["out_r"]) <= 1e-12

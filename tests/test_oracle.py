@@ -143,3 +143,18 @@ def test_oracle_matches_live_reference_on_new_seed():
     lev.vanka_sweep(2.0, 2)
     for k in ("u", "v", "H", "mask"):
         assert rel_err(getattr(lev, k), np.array(getattr(gr.state, k).data)) <= 1e-12, k
+
+
+def test_vanka_dump_matches_reference():
+    """ForwardOperators.vanka_dump on the random state (with calving)."""
+    from oracle.glide_oracle import OracleLevel
+    g = load_golden("random_vanka_dump_f64")
+    ny, nx = g["in_H"].shape
+    lev = OracleLevel(ny, nx, 1500.0, np.float64)
+    for k in ("u", "v", "H", "bed", "B", "beta", "phi", "gamma", "f_u", "f_v"):
+        getattr(lev, k)[...] = g[f"in_{k}"]
+    lev.phys["calving_rate"] = 1.0
+    lev.f_H[...] = g["in_H_prev"] / 5.0 + g["in_smb"]
+    J, r = lev.vanka_dump(5.0)
+    assert rel_err(J, g["out_J"]) <= 1e-12
+    assert rel_err(r, g["out_r"]) <= 1e-12
