@@ -21,6 +21,10 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libglide_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 UNITS = ["runtime.cu", "noalloc.cu", "enthalpy.cu"]
+# Fast single-precision math (approximate division, square root, reciprocal
+# cube root; flush-to-zero) for the binary32 smoother and tangent kernels, as
+# the reference compiles its own kernels.  Binary64 code is unaffected.
+EXTRA = os.environ.get("GLIDE_NVCC_EXTRA", "--use_fast_math").split()
 
 
 def nvcc() -> str:
@@ -43,7 +47,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     if not force and not stale():
         return LIB
     OUT_DIR.mkdir(exist_ok=True)
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", *EXTRA,
            "-Xcompiler", "-fPIC", "-shared", "-I", str(ROOT / "include"), "-I", str(CSRC),
            *[str(CSRC / f) for f in UNITS], "-o", str(LIB) + ".tmp", "-lcudart"]
     if verbose_ptxas:
