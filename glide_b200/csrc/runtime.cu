@@ -84,6 +84,8 @@ enum InternalField {
     // tangent (Newton correction) system: correction, right-hand side,
     // residual and the coarse-level snapshot of the correction
     F_E_U, F_E_V, F_E_H, F_TF_U, F_TF_V, F_TF_H, F_TR_U, F_TR_V, F_TR_H, F_TW_U, F_TW_V, F_TW_H,
+    // state before a Newton step, restored when the step is rejected
+    F_BK_U, F_BK_V, F_BK_H, F_BK_MASK,
     F_COUNT
 };
 
@@ -94,10 +96,12 @@ static Kind field_kind(int f) {
         case GLIDE_U: case GLIDE_F_U: case GLIDE_R_U: case GLIDE_LAMBDA_U: case GLIDE_ADJ_F_U:
         case GLIDE_ADJ_R_U: case GLIDE_VJP_U: case GLIDE_FOP_U: case F_U_ALT: case F_W_U: case F_WL_U:
         case F_E_U: case F_TF_U: case F_TR_U: case F_TW_U: case GLIDE_VAR_U: case GLIDE_JVP_U:
+        case F_BK_U:
             return KU;
         case GLIDE_V: case GLIDE_F_V: case GLIDE_R_V: case GLIDE_LAMBDA_V: case GLIDE_ADJ_F_V:
         case GLIDE_ADJ_R_V: case GLIDE_VJP_V: case GLIDE_FOP_V: case F_V_ALT: case F_W_V: case F_WL_V:
         case F_E_V: case F_TF_V: case F_TR_V: case F_TW_V: case GLIDE_VAR_V: case GLIDE_JVP_V:
+        case F_BK_V:
             return KV;
         default:
             return KC;
@@ -181,13 +185,21 @@ struct Solver : SolverBase {
     double* partial = nullptr;
     double* norms_dev = nullptr;
     double* norms_host = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    unsigned graph_version = 0;
-    double graph_dt = 0;
-    int graph_start = -1, graph_kind = -1;
+    // one captured V-cycle per cycle kind (0 FAS, 1 adjoint, 2 mixed FAS,
+    // 3 mixed adjoint, 4 Newton), each valid for the (version, dt, start) it
+    // was captured with, so that solves alternating kinds replay, not recapture
+    static constexpr int kKinds = 5;
+    struct CachedGraph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned version = 0;
+        double dt = 0;
+        int start = -1;
+        long long launches = 0;  // kernels inside the graph
+    };
+    CachedGraph graphs[kKinds];
     cudaStream_t own_stream = nullptr;
     long long launches = 0;        // kernels issued by this handle (graph replays included)
-    long long graph_launches = 0;  // kernels inside the captured graph
+    long long newton_rejects = 0;  // Newton steps undone by the growth guard
 
     void counted(const char* what) {
         check_launch(what);
@@ -246,7 +258,8 @@ struct Solver : SolverBase {
     }
 
     ~Solver() override {
-        if (graph) cudaGraphExecDestroy(graph);
+        for (CachedGraph& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
         for (R* b : blk) if (b) cudaFree(b);
         if (own_stream) cudaStreamDestroy(own_stream);
         if (norms_host) cudaFreeHost(norms_host);
@@ -500,8 +513,9 @@ struct Solver : SolverBase {
             if (!own_stream) GCU(cudaStreamCreate(&own_stream));
             s = own_stream;
         }
-        if (!graph || graph_version != version || graph_dt != dt || graph_start != start || graph_kind != kind) {
-            if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        CachedGraph& cg = graphs[kind];
+        if (!cg.exec || cg.version != version || cg.dt != dt || cg.start != start) {
+            if (cg.exec) { cudaGraphExecDestroy(cg.exec); cg.exec = nullptr; }
             cudaGraph_t g;
             const long long before = launches;
             GCU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -513,16 +527,16 @@ struct Solver : SolverBase {
                 launches = before;
                 throw;
             }
-            graph_launches = launches - before;
+            cg.launches = launches - before;
             launches = before;
             GCU(cudaStreamEndCapture(s, &g));
-            cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+            cudaError_t e = cudaGraphInstantiate(&cg.exec, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) fail(GLIDE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            graph_version = version; graph_dt = dt; graph_start = start; graph_kind = kind;
+            cg.version = version; cg.dt = dt; cg.start = start;
         }
-        GCU(cudaGraphLaunch(graph, s));
-        launches += graph_launches;
+        GCU(cudaGraphLaunch(cg.exec, s));
+        launches += cg.launches;
     }
 
     // ------------------------------------------------ mixed precision
@@ -660,31 +674,57 @@ struct Solver : SolverBase {
             st->initial_norm = r0;
             st->history[0] = r0;
         }
-        // Newton safeguard: two consecutive steps that fail to cut the residual
-        // by `newton_stall_ratio` hand the rest of the solve back to FASCD.  On
-        // a mixed handle those FASCD cycles run in binary64: the binary32
-        // defect correction stops near the binary32 rounding level of the
-        // residual.
+        // Newton guards.  Each Newton step starts from a saved state; a step
+        // whose residual grows (or is not finite) is undone, and Newton waits
+        // until FASCD has cut the residual another tenfold.  Two consecutive
+        // steps that fail to cut it by `newton_stall_ratio` hand the rest of
+        // the solve back to FASCD.  On a mixed handle the FASCD cycles after
+        // the switch run in binary64: the binary32 defect correction stops near
+        // the binary32 rounding level of the residual.
         bool newton_off = false;
         int stall = 0;
+        double gate = newton_switch;
         double prev = ab;
+        Level<R>& L0 = lv[start];
         while (rel > c.relative_tolerance && ab > c.absolute_tolerance && it < c.maximum_vcycles) {
             // forward solves may finish with Newton steps once the FAS phase is close
             int k = kind;
-            const bool newton_phase = (kind == 0 || kind == 2) && forward_method == 1 && rel <= newton_switch;
-            if (newton_phase && !newton_off) k = 4;
+            const bool forward_newton = (kind == 0 || kind == 2) && forward_method == 1;
+            const bool newton_phase = forward_newton && rel <= newton_switch;
+            if (newton_phase && !newton_off && rel <= gate) k = 4;
             else if (newton_phase && kind == 2) k = 0;
             if (k == 4 && !in_newton) {
-                newton_prologue(start, dt, s);
+                // the Newton residual (active set decided inline) of the
+                // current state: the norm the first step is judged against
+                newton_prologue(start, dt, true, s);
+                read_norms(nr, s);
+                prev = nr[3];
                 in_newton = true;
             }
             if (k != 4) in_newton = false;
+            if (k == 4) {
+                copy(L0.a[F_BK_U], L0.a[GLIDE_U], s);
+                copy(L0.a[F_BK_V], L0.a[GLIDE_V], s);
+                copy(L0.a[F_BK_H], L0.a[GLIDE_H], s);
+                copy(L0.a[F_BK_MASK], L0.a[GLIDE_MASK], s);
+            }
             cycle_and_check(k, start, dt, s);
             read_norms(nr, s);
             ab = nr[3];
+            if (k == 4 && !(ab <= prev)) {  // grew or not finite: undo the step
+                copy(L0.a[GLIDE_U], L0.a[F_BK_U], s);
+                copy(L0.a[GLIDE_V], L0.a[F_BK_V], s);
+                copy(L0.a[GLIDE_H], L0.a[F_BK_H], s);
+                copy(L0.a[GLIDE_MASK], L0.a[F_BK_MASK], s);
+                ab = prev;
+                gate = 0.1 * (prev / r0);
+                in_newton = false;
+                stall = 0;
+                ++newton_rejects;
+            }
             if (!std::isfinite(ab)) fail(GLIDE_ERR_NONFINITE, "residual norm became non-finite");
             rel = ab / r0;
-            if (k == 4) {
+            if (k == 4 && in_newton) {
                 stall = ab > newton_stall_ratio * prev ? stall + 1 : 0;
                 if (stall >= 2) newton_off = true;
             }
@@ -859,8 +899,8 @@ struct Solver : SolverBase {
     // recomputes phi, the residual, the next active set and the masked norms.
     int tangent_vcycles = 1;
 
-    void newton_prologue(int l, double dt, cudaStream_t s) {
-        residual(l, dt, true, false, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, false, s, true);
+    void newton_prologue(int l, double dt, bool norms, cudaStream_t s) {
+        residual(l, dt, true, false, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, norms, s, true);
     }
 
     template <class T>

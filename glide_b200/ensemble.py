@@ -65,7 +65,7 @@ def member_specs(n_members: int, seed: int = 0, sizes=(128, 192, 256, 384, 512, 
 
 # solver schedules the autotuner chooses among (applied through the options API)
 CANDIDATES = {
-    "fast": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="newton", switch=2,
+    "fast": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="newton", switch=0,
                  tangent=(4, 4, 0, 20)),
     "fascd": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="fascd", switch=None,
                   tangent=None),

@@ -168,14 +168,33 @@ def test_mixed_precision_reaches_reference_solution(c1_reference_solution):
         assert rel_err(_np(h.view(k, 0)), ref) <= 1e-8, k
 
 
-def test_fast_form_reaches_reference_solution(c1_reference_solution):
+@pytest.mark.parametrize("switch", [0, 2])
+def test_fast_form_reaches_reference_solution(c1_reference_solution, switch):
     """The benchmark's fast form: mixed precision, corrected transfers,
-    FASCD (4/4/0/200, local Newton capped at 3) to 1e-2, then Newton."""
-    h, st = _solve_c1(precision="mixed", quirks=False, schedule=(4, 4, 0, 200), method="newton",
-                      newton_steps=3, switch=2)
+    guarded Newton from the start (switch 0) or after FASCD (4/4/0/50, local
+    Newton capped at 3) has reached 1e-2 (switch 2)."""
+    h, st = _solve_c1(precision="mixed", quirks=False, schedule=(4, 4, 0, 50), method="newton",
+                      newton_steps=3, switch=switch)
     assert st["final_norm"] <= 1e-11 * st["initial_norm"]
     for k, ref in c1_reference_solution.items():
         assert rel_err(_np(h.view(k, 0)), ref) <= 1e-8, k
+
+
+def test_rejected_newton_step_is_undone():
+    """Newton from a cold start on a steep dome makes the residual grow at
+    first; the guard undoes those steps and the solve still converges."""
+    from cases import dome
+    from glide_b200.hierarchy import Hierarchy
+    f = dome(128, 1500.0, 86e3, seed=3)
+    h = Hierarchy(128, 128, 1500.0, 4, precision="mixed", reference_quirks=False)
+    for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+        h.set(k, 0, torch.as_tensor(f[k]), restrict_down=True)
+    h.set_fas(False, maximum_vcycles=80, relative_tolerance=1e-9, absolute_tolerance=0.0,
+              pre_steps=4, post_steps=4, finest_steps=0, coarsest_steps=50)
+    h.set_vanka(False, -1, newton_steps=3)
+    h.set_tuning(forward_method="newton", newton_switch_exp10=0)
+    st = h.forward(5.0, 0)
+    assert np.isfinite(st["final_norm"]) and st["final_norm"] <= 1e-9 * st["initial_norm"], st
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
