@@ -47,6 +47,16 @@ GRAD_ALL = 15
 
 MAX_HISTORY = 256
 
+# glide_transfer op codes
+TRANSFER_OPS = {
+    "restrict_vfacet": 0, "restrict_hfacet": 1, "restrict_cell_avg": 2, "restrict_cell_max": 3,
+    "restrict_cell_min": 4, "restrict_cell_var": 5,
+    "prolongate_vfacet_injection": 6, "prolongate_vfacet_bilinear": 7,
+    "prolongate_hfacet_injection": 8, "prolongate_hfacet_bilinear": 9,
+    "prolongate_cell_injection": 10, "prolongate_cell_bilinear": 11,
+    "prolongate_hfacet_as_vfacet_injection": 12, "prolongate_hfacet_as_vfacet_bilinear": 13,
+}
+
 
 class GlideError(RuntimeError):
     def __init__(self, code, msg):
@@ -127,6 +137,8 @@ SIGNATURES = {
     "glide_residual_norms_noalloc": ([_I, _I, _D, _D, ctypes.POINTER(Phys), _P, _I, _P, _I, _P, _P, _P,
                                       _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P], _I),
     "glide_noalloc_last_error": ([], ctypes.c_char_p),
+    "glide_vcycle": ([_H, _I, _I, _I, _D, _P], _I),
+    "glide_transfer": ([_I, _I, _I, _I, _P, _I, _P, _I, _P], _I),
 }
 
 class EnthalpyConfig(ctypes.Structure):

@@ -1376,4 +1376,55 @@ int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, gl
     });
 }
 
+int glide_vcycle(glide_handle h, int which, int level, int finest, double dt, void* stream) {
+    return guarded([&] {
+        if (which != 0 && which != 1) fail(GLIDE_ERR_ARG, "which must be 0 (FASCD) or 1 (adjoint)");
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            if (which == 0) {
+                s.check_quirks();
+                s.vcycle(level, finest != 0, dt, S(stream));
+            } else {
+                s.ensure_blocks();
+                s.adj_vcycle(level, finest != 0, dt, S(stream));
+            }
+        });
+    });
+}
+
+int glide_transfer(int op, int dtype, int ny_fine, int nx_fine, const void* src, int ld_src, void* dst, int ld_dst,
+                   void* stream) {
+    return guarded([&] {
+        if (!src || !dst) fail(GLIDE_ERR_ARG, "null array");
+        if (op < GLIDE_RESTRICT_VFACET || op > GLIDE_PROLONG_HFACET_AS_VFACET_BILINEAR)
+            fail(GLIDE_ERR_ARG, "unknown transfer op");
+        if (dtype != GLIDE_F64 && dtype != GLIDE_F32) fail(GLIDE_ERR_ARG, "dtype must be GLIDE_F64 or GLIDE_F32");
+        if (ny_fine < 2 || nx_fine < 2 || (ny_fine & 1) || (nx_fine & 1))
+            fail(GLIDE_ERR_SHAPE, "fine cell counts must be even and >= 2");
+        if (op >= GLIDE_PROLONG_HFACET_AS_VFACET_INJECTION && ny_fine != nx_fine)
+            fail(GLIDE_ERR_SHAPE, "the u-face prolongation of v-face memory needs a square grid");
+        const int nyc = ny_fine / 2, nxc = nx_fine / 2;
+        // (rows, cols) of the fine and coarse arrays of this field's kind
+        int fr = ny_fine, fc = nx_fine, cr = nyc, cc = nxc;
+        const bool ufaces = op == GLIDE_RESTRICT_VFACET || op == GLIDE_PROLONG_VFACET_INJECTION ||
+                            op == GLIDE_PROLONG_VFACET_BILINEAR;
+        const bool vfaces = op == GLIDE_RESTRICT_HFACET || op == GLIDE_PROLONG_HFACET_INJECTION ||
+                            op == GLIDE_PROLONG_HFACET_BILINEAR || op >= GLIDE_PROLONG_HFACET_AS_VFACET_INJECTION;
+        if (ufaces) ++fc, ++cc;
+        if (vfaces) ++fr, ++cr;
+        const bool restrict_op = op <= GLIDE_RESTRICT_CELL_VAR;
+        const int sr = restrict_op ? fr : cr, sc = restrict_op ? fc : cc;
+        const int dr = restrict_op ? cr : fr, dc = restrict_op ? cc : fc;
+        if (ld_src < sc || ld_dst < dc) fail(GLIDE_ERR_ARG, "leading dimension smaller than the row length");
+        auto run = [&](auto* s) {
+            using R = std::remove_const_t<std::remove_pointer_t<decltype(s)>>;
+            Arr<R> a{const_cast<R*>(s), sr, sc, ld_src}, b{static_cast<R*>(dst), dr, dc, ld_dst};
+            k_transfer<R><<<dim3((dc + 255) / 256, dr), 256, 0, S(stream)>>>(a, b, op, ny_fine, nx_fine);
+            check_launch("k_transfer");
+        };
+        if (dtype == GLIDE_F64) run(static_cast<const double*>(src));
+        else run(static_cast<const float*>(src));
+    });
+}
+
 }  // extern "C"

@@ -222,4 +222,79 @@ __global__ void k_fill(Arr<R> a, R val, int rows, int cols) {
     if (i < rows && j < cols) a.at(i, j) = val;
 }
 
+// One stand-alone transfer of one field between caller arrays (the
+// Multigrid.restrict_* / prolongate_* helpers, glide/multigrid.py:119-259,
+// with the kernels of glide/cuda/transfer.cu).  `op` is a GLIDE_RESTRICT_* /
+// GLIDE_PROLONG_* code; (nyf, nxf) are the fine cell counts, the coarse ones
+// half of them.  One thread per element of `dst`, whose shape (rows, cols) is
+// the launch's.  Codes 12/13 run the u-face formulas over the flat memory of
+// v-face arrays, which is what the reference's prolongate_hfacet launches
+// (square grids: both layouts then hold (n+1) n elements).
+template <class R>
+__global__ void k_transfer(Arr<R> src, Arr<R> dst, int op, int nyf, int nxf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (j >= dst.rows || i >= dst.cols) return;
+    const int nyc = nyf / 2, nxc = nxf / 2;
+    auto c = [&](int J, int I) { return src.at(J, I); };
+    R o;
+    switch (op) {
+        case 0:  // restrict_vfacet (transfer.cu:2-19)
+            o = R(0.5) * (src.at(2 * j, 2 * i) + src.at(2 * j + 1, 2 * i));
+            break;
+        case 1:  // restrict_hfacet (transfer.cu:22-39)
+            o = R(0.5) * (src.at(2 * j, 2 * i) + src.at(2 * j, 2 * i + 1));
+            break;
+        case 2: case 3: case 4: case 5: {  // restrict_cell_{avg,max,min,var} (transfer.cu:42-139)
+            const R a = src.at(2 * j, 2 * i), b = src.at(2 * j, 2 * i + 1);
+            const R cc = src.at(2 * j + 1, 2 * i), d = src.at(2 * j + 1, 2 * i + 1);
+            if (op == 2) o = R(0.25) * (a + b + cc + d);
+            else if (op == 3) o = fmax(fmax(a, b), fmax(cc, d));
+            else if (op == 4) o = fmin(fmin(a, b), fmin(cc, d));
+            else {
+                const R mu = R(0.25) * (a + b + cc + d);
+                const R d1 = a - mu, d2 = b - mu, d3 = cc - mu, d4 = d - mu;
+                o = R(0.25) * (d1 * d1 + d2 * d2 + d3 * d3 + d4 * d4);
+            }
+            break;
+        }
+        case 6: {  // prolongate_vfacet_injection (transfer.cu:142-174)
+            const int J = j / 2, I = i / 2;
+            o = (i % 2 == 0 || I >= nxc) ? c(J, I) : R(0.5) * (c(J, I) + c(J, I + 1));
+            break;
+        }
+        case 7:  // prolongate_vfacet_bilinear (transfer.cu:177-229)
+            o = bilinear_u<R>(c, j, i, nyc, nxc);
+            break;
+        case 8: {  // prolongate_hfacet_injection (transfer.cu:232-267)
+            const int J = j / 2, I = i / 2;
+            o = (j % 2 == 0 || J >= nyc) ? c(J, I) : R(0.5) * (c(J, I) + c(J + 1, I));
+            break;
+        }
+        case 9:  // prolongate_hfacet_bilinear (transfer.cu:270-323)
+            o = bilinear_v<R>(c, j, i, nyc, nxc);
+            break;
+        case 10:  // prolongate_cell_injection (transfer.cu:326-345)
+            o = c(j >> 1, i >> 1);
+            break;
+        case 11:  // prolongate_cell_bilinear (transfer.cu:348-395)
+            o = bilinear_c<R>(c, j, i, nyc, nxc);
+            break;
+        default: {  // 12, 13: u-face formulas on v-face memory
+            const long flat = long(j) * nxf + i;
+            const int jj = int(flat / (nxf + 1)), ii = int(flat % (nxf + 1));
+            auto q = [&](int J, int I) {
+                const long cf = long(J) * (nxc + 1) + I;
+                return src.at(int(cf / nxc), int(cf % nxc));
+            };
+            if (op == 12) {
+                const int J = jj / 2, I = ii / 2;
+                o = (ii % 2 == 0 || I >= nxc) ? q(J, I) : R(0.5) * (q(J, I) + q(J, I + 1));
+            } else {
+                o = bilinear_u<R>(q, jj, ii, nyc, nxc);
+            }
+        }
+    }
+    dst.at(j, i) = o;
+}
+
 }  // namespace glide

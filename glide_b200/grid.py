@@ -146,5 +146,13 @@ class Grid:
             self._adjoint_operators = AdjointOperators(self)
         return self._adjoint_operators
 
+    def spawn_child(self):
+        """A new stand-alone Grid of half the cells and twice the spacing,
+        linked as this grid's child, fields zero (glide/grid.py:374-380; the
+        reference leaves the origin at 0, as here)."""
+        child = Grid(self.ny // 2, self.nx // 2, self.dx * 2, parent=self, dtype=self._hier.dtype)
+        self.child = child
+        return child
+
     def __repr__(self):
         return f"Grid(level={self.level}, ny={self.ny}, nx={self.nx}, dx={self.dx})"

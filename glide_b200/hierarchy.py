@@ -19,6 +19,22 @@ def _stream_ptr():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def transfer(op: str, src: torch.Tensor, dst: torch.Tensor, ny_fine: int, nx_fine: int):
+    """One glide_transfer (restriction or prolongation of one field) between
+    two 2-D CUDA tensors of one float dtype with unit column stride."""
+    for t in (src, dst):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.ndim == 2):
+            raise TypeError("transfers take 2-D CUDA tensors")
+        if t.stride(1) != 1 and t.shape[1] > 1:
+            raise ValueError("transfers need rows with unit stride")
+    if src.dtype != dst.dtype or src.dtype not in (torch.float64, torch.float32):
+        raise TypeError("source and destination must both be float64 or both float32")
+    dtype = _lib.GLIDE_F64 if src.dtype == torch.float64 else _lib.GLIDE_F32
+    call("glide_transfer", _lib.TRANSFER_OPS[op], dtype, int(ny_fine), int(nx_fine),
+         ctypes.c_void_p(src.data_ptr()), max(src.stride(0), src.shape[1]), ctypes.c_void_p(dst.data_ptr()),
+         max(dst.stride(0), dst.shape[1]), _stream_ptr())
+
+
 class _DeviceBuffer:
     """__cuda_array_interface__ adaptor so torch can alias arena memory."""
 
@@ -231,6 +247,10 @@ class Hierarchy:
 
     def gradients(self, level: int, dt: float, mask: int = _lib.GRAD_ALL):
         call("glide_gradients", self._h, int(level), float(dt), int(mask), _stream_ptr())
+
+    def vcycle(self, adjoint: bool, level: int, finest: bool, dt: float):
+        """One V-cycle from `level` (no residual around it; see glide_vcycle)."""
+        call("glide_vcycle", self._h, int(bool(adjoint)), int(level), int(bool(finest)), float(dt), _stream_ptr())
 
     def backward(self, dt: float, start_level: int = 0, mask: int = _lib.GRAD_ALL) -> dict:
         st = _lib.Stats()

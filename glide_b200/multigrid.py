@@ -15,7 +15,7 @@ import torch
 
 from .field import BroadcastOption, LocalOption
 from .grid import Grid
-from .hierarchy import Hierarchy
+from .hierarchy import Hierarchy, transfer
 from .operators import NewtonConfig, VankaConfig, _Synced
 
 
@@ -67,6 +67,164 @@ class Multigrid:
 
     def __getitem__(self, key):
         return self.levels[key]
+
+    # ------------------------------------------------- level construction
+    def create_grid_hierarchy(self, n_levels, restrict_fields=True):
+        """glide/multigrid.py:54-60.  The device arena is sized for
+        `self.n_levels` levels when the Multigrid is built, so the call
+        re-derives the existing levels (restricting every field down from the
+        finest when restrict_fields) and n_levels must equal that count."""
+        if int(n_levels) != self.n_levels:
+            raise ValueError(f"this Multigrid holds {self.n_levels} levels, fixed when it was built; "
+                             f"build a new Multigrid for {n_levels}")
+        levels = [self.finest_grid]
+        for _ in range(1, self.n_levels):
+            levels.append(self.create_coarse_grid(levels[-1], restrict_fields=restrict_fields))
+        return self.levels
+
+    def create_coarse_grid(self, parent_grid, restrict_fields=True):
+        """glide/multigrid.py:62-79: the grid of half the cells and twice the
+        spacing under `parent_grid`, its origin shifted by half a fine cell.
+        A level of this hierarchy returns its existing child; any other grid
+        (or the coarsest level) gets a new stand-alone Grid.  With
+        restrict_fields, the state, geometry, rheology, sliding, calving and
+        forcing are restricted into it."""
+        child = parent_grid.child
+        if child is None:
+            child = Grid(parent_grid.ny // 2, parent_grid.nx // 2, parent_grid.dx * 2,
+                         x0=parent_grid.x0 + parent_grid.dx / 2, y0=parent_grid.y0 - parent_grid.dx / 2,
+                         crs=parent_grid.crs, parent=parent_grid, dtype=parent_grid._hier.dtype)
+            parent_grid.child = child
+        if restrict_fields:
+            self.restrict_state(parent_grid, child)
+            self.restrict_geometry(parent_grid, child)
+            self.restrict_rheology(parent_grid, child)
+            self.restrict_sliding(parent_grid, child)
+            self.restrict_calving(parent_grid, child)
+            self.restrict_forcing(parent_grid, child)
+        return child
+
+    # ------------------------------------------- grid-to-grid restriction
+    def restrict_state(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:81-87."""
+        f, c = fine_grid.state, coarse_grid.state
+        self.restrict_vfacet(f.u.data, c.u.data)
+        self.restrict_hfacet(f.v.data, c.v.data)
+        self.restrict_cell(f.H.data, c.H.data)
+        self.restrict_cell(f.H_prev.data, c.H_prev.data)
+        self.restrict_cell(f.phi.data, c.phi.data)
+        self.restrict_cell(f.mask.data, c.mask.data, method="max")
+
+    def restrict_geometry(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:89-92."""
+        self.restrict_cell(fine_grid.geometry.bed.data, coarse_grid.geometry.bed.data)
+        coarse_grid.geometry.thklim.set(fine_grid.geometry.thklim.value)
+        coarse_grid.geometry.flotation_reg_driving.set(fine_grid.geometry.flotation_reg_driving.value)
+
+    def restrict_rheology(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:94-97."""
+        self.restrict_cell(fine_grid.rheology.B.data, coarse_grid.rheology.B.data)
+        coarse_grid.rheology.n.set(fine_grid.rheology.n.value)
+        coarse_grid.rheology.eps_reg.set(fine_grid.rheology.eps_reg.value)
+
+    def restrict_sliding(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:99-104."""
+        self.restrict_cell(fine_grid.sliding.beta.data, coarse_grid.sliding.beta.data)
+        for k in ("m", "u_reg", "water_drag", "flotation_reg_sliding"):
+            getattr(coarse_grid.sliding, k).set(getattr(fine_grid.sliding, k).value)
+
+    def restrict_calving(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:106-108."""
+        coarse_grid.calving.calving_rate.set(fine_grid.calving.calving_rate.value)
+        coarse_grid.calving.flotation_reg_calving.set(fine_grid.calving.flotation_reg_calving.value)
+
+    def restrict_forcing(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:110-111."""
+        self.restrict_cell(fine_grid.forcing.smb.data, coarse_grid.forcing.smb.data)
+
+    def restrict_residual(self, fine_grid, coarse_grid):
+        """glide/multigrid.py:113-116."""
+        f, c = fine_grid.forward_operators, coarse_grid.forward_operators
+        self.restrict_vfacet(f.r_u, c.r_u)
+        self.restrict_hfacet(f.r_v, c.r_v)
+        self.restrict_cell(f.r_H, c.r_H)
+
+    # ------------------------------------------------ one-field transfers
+    # glide/multigrid.py:118-259 over the kernels of glide/cuda/transfer.cu.
+    # Arrays are 2-D CUDA tensors (float64 or float32); a missing output is
+    # allocated with the input's dtype.  Fine cell counts must be even.
+    def restrict_vfacet(self, fine_field, coarse_field=None):
+        """u faces (ny, nx+1) -> (ny/2, nx/2+1): mean of the two fine faces on
+        each coarse face."""
+        ny, nx = fine_field.shape[0], fine_field.shape[1] - 1
+        if coarse_field is None:
+            coarse_field = fine_field.new_empty((ny // 2, nx // 2 + 1))
+        _check_shape(coarse_field, (ny // 2, nx // 2 + 1))
+        transfer("restrict_vfacet", fine_field, coarse_field, ny, nx)
+        return coarse_field
+
+    def restrict_hfacet(self, fine_field, coarse_field=None):
+        """v faces (ny+1, nx) -> (ny/2+1, nx/2)."""
+        ny, nx = fine_field.shape[0] - 1, fine_field.shape[1]
+        if coarse_field is None:
+            coarse_field = fine_field.new_empty((ny // 2 + 1, nx // 2))
+        _check_shape(coarse_field, (ny // 2 + 1, nx // 2))
+        transfer("restrict_hfacet", fine_field, coarse_field, ny, nx)
+        return coarse_field
+
+    def restrict_cell(self, fine_field, coarse_field=None, method="avg"):
+        """Cells (ny, nx) -> (ny/2, nx/2): 2x2 mean, maximum, minimum or
+        (population) variance."""
+        if method not in ("avg", "max", "min", "var"):
+            raise TypeError("Valid restriction methods: [avg,max,min]")
+        ny, nx = fine_field.shape
+        if coarse_field is None:
+            coarse_field = fine_field.new_empty((ny // 2, nx // 2))
+        _check_shape(coarse_field, (ny // 2, nx // 2))
+        transfer("restrict_cell_" + method, fine_field, coarse_field, ny, nx)
+        return coarse_field
+
+    def prolongate_vfacet(self, coarse_field, fine_field=None, method="injection"):
+        """u faces (nyc, nxc+1) -> (2 nyc, 2 nxc+1)."""
+        if method not in ("injection", "bilinear"):
+            raise TypeError("Valid prolongation methods: [injection, bilinear]")
+        nyf, nxf = 2 * coarse_field.shape[0], 2 * (coarse_field.shape[1] - 1)
+        if fine_field is None:
+            fine_field = coarse_field.new_empty((nyf, nxf + 1))
+        _check_shape(fine_field, (nyf, nxf + 1))
+        transfer("prolongate_vfacet_" + method, coarse_field, fine_field, nyf, nxf)
+        return fine_field
+
+    def prolongate_hfacet(self, coarse_field, fine_field=None, method="injection"):
+        """v faces (nyc+1, nxc) -> (2 nyc+1, 2 nxc).  With reference quirks on
+        (the default) this runs what the reference runs: its u-face kernels
+        over the v arrays' memory (square grids only); with them off, the
+        v-face formulas."""
+        if method not in ("injection", "bilinear"):
+            raise TypeError("Valid prolongation methods: [injection, bilinear]")
+        nyf, nxf = 2 * (coarse_field.shape[0] - 1), 2 * coarse_field.shape[1]
+        if fine_field is None:
+            fine_field = coarse_field.new_empty((nyf + 1, nxf))
+        _check_shape(fine_field, (nyf + 1, nxf))
+        op = ("prolongate_hfacet_as_vfacet_" if self.hierarchy.reference_quirks else "prolongate_hfacet_") + method
+        transfer(op, coarse_field, fine_field, nyf, nxf)
+        return fine_field
+
+    def prolongate_cell(self, coarse_field, fine_field=None, method="injection"):
+        """Cells (nyc, nxc) -> (2 nyc, 2 nxc)."""
+        if method not in ("injection", "bilinear"):
+            raise TypeError("Valid prolongation methods: [injection, bilinear]")
+        nyf, nxf = 2 * coarse_field.shape[0], 2 * coarse_field.shape[1]
+        if fine_field is None:
+            fine_field = coarse_field.new_empty((nyf, nxf))
+        _check_shape(fine_field, (nyf, nxf))
+        transfer("prolongate_cell_" + method, coarse_field, fine_field, nyf, nxf)
+        return fine_field
+
+
+def _check_shape(t, shape):
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"expected an array of shape {tuple(shape)}, got {tuple(t.shape)}")
 
 
 class HierarchyFieldManager:
@@ -281,6 +439,14 @@ class FASCDSolver:
                 print(f"  V-cycle {k - 1}: |r|/|r0| = {h[k] / h[0]:.2e}")
         return st
 
+    def vcycle(self, l, finest=False):
+        """One FASCD V-cycle from level l (glide/multigrid.py:536-645) with the
+        dt of the last `solve` (or the dt attribute set by the caller); the
+        right-hand side of level l must be set (ForwardOperators.set_rhs)."""
+        if self.dt is None:
+            raise AttributeError("dt is unset: call solve() first or set solver.dt")
+        self.multigrid.hierarchy.vcycle(False, l, finest, self.dt)
+
 
 @dataclass
 class FASAdjointLevel:
@@ -312,3 +478,12 @@ class FASAdjointSolver:
             for k in range(1, len(h)):
                 print(f"  V-cycle {k - 1}: |r|/|r0| = {h[k] / h[0]:.2e}")
         return st
+
+    def vcycle(self, l, finest=False):
+        """One linear FAS V-cycle of the adjoint system from level l
+        (glide/multigrid.py:905-973) with the dt of the last `solve` (or the dt
+        attribute set by the caller); the adjoint right-hand side of level l
+        must be set."""
+        if self.dt is None:
+            raise AttributeError("dt is unset: call solve() first or set solver.dt")
+        self.multigrid.hierarchy.vcycle(True, l, finest, self.dt)

@@ -174,6 +174,12 @@ class AdjointOperators:
     def vanka_sweep(self, dt, n_iter, freeze_calving=False):
         self._h.adjoint_sweep(self._l, dt, n_iter)
 
+    def vanka_smooth(self, dt, freeze_calving=False):
+        """One adjoint smoother pass (glide/operators.py:474-515).  As in the
+        forward operators, the update lambda -= omega * delta is applied in the
+        same fused kernel (there are no separate delta buffers)."""
+        self.vanka_sweep(dt, 1, freeze_calving=freeze_calving)
+
     def compute_gradient_beta(self):
         self._h.gradients(self._l, 1.0, _lib.GRAD_BETA)
 

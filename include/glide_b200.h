@@ -29,6 +29,9 @@
  *   glide_gradients                AdjointOperators.compute_gradient_* (glide/operators.py:526-593)
  *   glide_backward                 IceDynamics.backward (glide/model.py:74-94) with
  *                                  FASAdjointSolver.solve (glide/multigrid.py:873-903)
+ *   glide_vcycle                   FASCDSolver.vcycle / FASAdjointSolver.vcycle
+ *                                  (glide/multigrid.py:536-645, :905-973)
+ *   glide_transfer                 Multigrid.restrict_* / prolongate_* (glide/multigrid.py:119-259)
  */
 #ifndef GLIDE_B200_H
 #define GLIDE_B200_H
@@ -187,6 +190,15 @@ int glide_adjoint_sweep(glide_handle h, int level, double dt, int n, void* strea
 int glide_gradients(glide_handle h, int level, double dt, int grad_mask, void* stream);
 int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, glide_stats* stats,
                    void* stream);
+/* One V-cycle from `level` and nothing around it: FASCDSolver.vcycle
+ * (glide/multigrid.py:536-645) for which = 0, FASAdjointSolver.vcycle
+ * (glide/multigrid.py:905-973) for which = 1.  finest != 0 takes the
+ * top-of-cycle snapshot (w = x, chi = thklim - H) as the reference's
+ * finest=True does.  The right-hand side of `level` must already be set
+ * (glide_set_rhs for the forward system, the adjoint right-hand side for the
+ * adjoint); no residual is evaluated.  Runs the handle's binary64 hierarchy on
+ * a mixed handle. */
+int glide_vcycle(glide_handle h, int which, int level, int finest, double dt, void* stream);
 
 /* Residual and its norms on caller-owned device arrays, allocating nothing.
  * No counterpart in the reference: it is glide_residual (the reference's
@@ -213,6 +225,39 @@ int glide_residual_norms_noalloc(int ny, int nx, double dx, double dt, const gli
                                  double* r_H, double* norms, void* stream);
 /* Message of the last failed glide_residual_norms_noalloc on this thread. */
 const char* glide_noalloc_last_error(void);
+
+/* One restriction or prolongation of one field between caller arrays, no
+ * handle needed: the reference's Multigrid.restrict_vfacet / restrict_hfacet /
+ * restrict_cell / prolongate_vfacet / prolongate_hfacet / prolongate_cell
+ * (glide/multigrid.py:119-259) over the kernels of glide/cuda/transfer.cu.
+ * ny_fine, nx_fine: the fine grid's cell counts (even); the coarse grid has
+ * half of each.  Array shapes, rows x cols, fine / coarse:
+ *   VFACET  (u faces)  ny_fine x (nx_fine+1)  /  ny_c x (nx_c+1)
+ *   HFACET  (v faces)  (ny_fine+1) x nx_fine  /  (ny_c+1) x nx_c
+ *   CELL               ny_fine x nx_fine      /  ny_c x nx_c
+ * A restriction reads the fine array (src) and writes the coarse one (dst);
+ * a prolongation the other way round.  ld_src / ld_dst are leading
+ * dimensions in elements; src and dst must not overlap.  dtype GLIDE_F64 or
+ * GLIDE_F32.  GLIDE_PROLONG_HFACET_AS_VFACET_* is what the reference's
+ * prolongate_hfacet runs: the u-face kernels over the flat memory of v-face
+ * arrays (square grids only, else GLIDE_ERR_SHAPE).  Asynchronous on
+ * `stream`; errors in glide_last_error(). */
+#define GLIDE_RESTRICT_VFACET 0
+#define GLIDE_RESTRICT_HFACET 1
+#define GLIDE_RESTRICT_CELL_AVG 2
+#define GLIDE_RESTRICT_CELL_MAX 3
+#define GLIDE_RESTRICT_CELL_MIN 4
+#define GLIDE_RESTRICT_CELL_VAR 5
+#define GLIDE_PROLONG_VFACET_INJECTION 6
+#define GLIDE_PROLONG_VFACET_BILINEAR 7
+#define GLIDE_PROLONG_HFACET_INJECTION 8
+#define GLIDE_PROLONG_HFACET_BILINEAR 9
+#define GLIDE_PROLONG_CELL_INJECTION 10
+#define GLIDE_PROLONG_CELL_BILINEAR 11
+#define GLIDE_PROLONG_HFACET_AS_VFACET_INJECTION 12
+#define GLIDE_PROLONG_HFACET_AS_VFACET_BILINEAR 13
+int glide_transfer(int op, int dtype, int ny_fine, int nx_fine, const void* src, int ld_src, void* dst, int ld_dst,
+                   void* stream);
 
 #ifdef __cplusplus
 }

@@ -181,6 +181,43 @@ def vanka_dump_case(glide):
     np.savez_compressed(HERE / "random_vanka_dump_f64.npz", **out)
 
 
+def transfer_cases(glide):
+    """Multigrid.restrict_* / prolongate_* (glide/multigrid.py:118-259) on
+    seeded arrays: every method on a square 16 x 16 grid (prolongate_hfacet is
+    the reference's u-face kernel run on v arrays), and all but
+    prolongate_hfacet on a 12 x 20 grid.  The reference's own v-face
+    prolongation kernels, which its Python never launches, are run directly
+    (transfer.cu:232-323)."""
+    with quiet():
+        mg = glide.multigrid.Multigrid(n_levels=2, ny=16, nx=16, dx=1000.0)
+    rng = np.random.default_rng(11)
+    out = {}
+    for tag, (ny, nx) in (("sq", (16, 16)), ("rect", (12, 20))):
+        nyc, nxc = ny // 2, nx // 2
+        fine = {"u": rng.standard_normal((ny, nx + 1)), "v": rng.standard_normal((ny + 1, nx)),
+                "c": rng.standard_normal((ny, nx))}
+        coarse = {"u": rng.standard_normal((nyc, nxc + 1)), "v": rng.standard_normal((nyc + 1, nxc)),
+                  "c": rng.standard_normal((nyc, nxc))}
+        for k, v in fine.items():
+            out[f"{tag}_fine_{k}"] = v
+        for k, v in coarse.items():
+            out[f"{tag}_coarse_{k}"] = v
+        out[f"{tag}_restrict_vfacet"] = np.array(mg.restrict_vfacet(fine["u"]))
+        out[f"{tag}_restrict_hfacet"] = np.array(mg.restrict_hfacet(fine["v"]))
+        for m in ("avg", "max", "min", "var"):
+            out[f"{tag}_restrict_cell_{m}"] = np.array(mg.restrict_cell(fine["c"], method=m))
+        for m in ("injection", "bilinear"):
+            out[f"{tag}_prolongate_vfacet_{m}"] = np.array(mg.prolongate_vfacet(coarse["u"], method=m))
+            out[f"{tag}_prolongate_cell_{m}"] = np.array(mg.prolongate_cell(coarse["c"], method=m))
+            if ny == nx:
+                out[f"{tag}_prolongate_hfacet_{m}"] = np.array(mg.prolongate_hfacet(coarse["v"], method=m))
+            f = np.zeros((ny + 1, nx))
+            n = (ny + 1) * nx
+            glide._kernels.launch(f"prolongate_hfacet_{m}", (n + 255) // 256, 256, (coarse["v"], f, ny, nx))
+            out[f"{tag}_vface_prolongate_hfacet_{m}"] = f
+    np.savez_compressed(HERE / "transfers_f64.npz", **out)
+
+
 def enthalpy_cases(glide):
     """EnthalpyOperators (glide/enthalpy.py) on a rough random state: residual,
     one column smooth, one layer smooth, omega, and column sweeps; then one
@@ -265,7 +302,7 @@ def enthalpy_cases(glide):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", default=None, help="enthalpy | dump: only those fixtures")
+    ap.add_argument("--only", default=None, help="enthalpy | dump | transfers: only those fixtures")
     a = ap.parse_args(argv)
     if a.only == "enthalpy":
         enthalpy_cases(load_reference(fp64=True, reference=a.reference))
@@ -273,11 +310,15 @@ def main(argv=None):
     if a.only == "dump":
         vanka_dump_case(load_reference(fp64=True, reference=a.reference))
         return
+    if a.only == "transfers":
+        transfer_cases(load_reference(fp64=True, reference=a.reference))
+        return
     glide = load_reference(fp64=True, reference=a.reference)
     c1_forward_and_adjoint(glide, "f64")
     random_cases(glide)
     enthalpy_cases(glide)
     vanka_dump_case(glide)
+    transfer_cases(glide)
     glide32 = load_reference(fp64=False, reference=a.reference)
     c1_forward_and_adjoint(glide32, "f32")
     for p in sorted(HERE.glob("*.npz")):

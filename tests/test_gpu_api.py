@@ -133,3 +133,54 @@ def test_unknown_option_raises():
     model = _model(g)
     with pytest.raises(AttributeError):
         model.forward_solver.fas_options.set(no_such_option=1)
+
+
+def test_solver_vcycle_reproduces_reference_solves():
+    """FASCDSolver.vcycle / FASAdjointSolver.vcycle called by hand, with the
+    set-up their solve() does around them (right-hand side and phi; adjoint
+    forcing), repeat the reference's 3-cycle forward and 2-cycle adjoint."""
+    g = load_golden("c1_adjoint_f64")
+    model = _model(g)
+    lv = model.mg.levels[0]
+    ops = lv.forward_operators
+    ops.set_rhs(10.0)
+    ops.compute_residual(10.0)
+    fs = model.forward_solver
+    with pytest.raises(AttributeError):
+        fs.vcycle(0, finest=True)
+    fs.dt = 10.0
+    for _ in range(3):
+        fs.vcycle(0, finest=True)
+    for k in ("u", "v", "H"):
+        assert rel_err(_np(getattr(lv.state, k).data), g[f"out_{k}"]) <= 1e-10, k
+    aops = lv.adjoint_operators
+    aops.f_u.copy_(-torch.as_tensor(g["in_dJdu"], device="cuda"))
+    aops.f_v.copy_(-torch.as_tensor(g["in_dJdv"], device="cuda"))
+    aops.f_H.zero_()
+    adj = model.adjoint_solver
+    adj.dt = 10.0
+    for _ in range(2):
+        adj.vcycle(0, finest=True)
+    for k in ("lambda_u", "lambda_v", "lambda_H"):
+        assert rel_err(_np(getattr(lv.adjoint, k).data), g[f"out_{k}"]) <= 1e-10, k
+
+
+def test_adjoint_vanka_smooth_is_one_sweep():
+    """AdjointOperators.vanka_smooth applies one adjoint smoother pass."""
+    g = load_golden("c1_adjoint_f64")
+    out = []
+    for smooth in (True, False):
+        model = _model(g)
+        model.forward(0.0, 10.0, update_geometry=False)
+        lv = model.mg.levels[0]
+        lv.adjoint_operators.f_u.copy_(-torch.as_tensor(g["in_dJdu"], device="cuda"))
+        lv.adjoint_operators.f_v.zero_()
+        lv.adjoint_operators.f_H.zero_()
+        if smooth:
+            lv.adjoint_operators.vanka_smooth(10.0)
+            lv.adjoint_operators.vanka_smooth(10.0)
+        else:
+            lv.adjoint_operators.vanka_sweep(10.0, 2)
+        out.append(_np(lv.adjoint.lambda_u.data))
+    assert np.abs(out[0]).max() > 0
+    assert rel_err(out[0], out[1]) == 0.0
