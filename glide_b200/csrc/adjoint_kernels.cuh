@@ -12,6 +12,7 @@
 #pragma once
 
 #include "forward_kernels.cuh"
+#include "tma.cuh"
 
 namespace glide {
 
@@ -251,6 +252,7 @@ struct VjpArgs {
     Arr<R> o_u, o_v, o_H;   // outputs
     Arr<R> s_u, s_v, s_H;   // optional subtrahends
     double* partial;
+    int* err;  // set when a bounded wait gives up
     PhysR<R> p;
     int ny, nx, use_forcing;
 };
@@ -487,26 +489,27 @@ struct BlockArgs {
     R* f;               // factors
     size_t plane;
     int pitch;
+    int* err;           // set when a bounded wait gives up
     PhysR<R> p;
     R omega, ssa_damping, mc_damping;
     int ny, nx;
 };
 
 template <class R, bool TR>
-__global__ void __launch_bounds__(kTile * kTile) k_block_factor(BlockArgs<R> a) {
-    using TileT = Tile<R, kTile, 1, 1>;
-    constexpr int NC = TileT::NC;
-    __shared__ TileT t;
+__global__ void __launch_bounds__(kTile * kTile)
+    k_block_factor(BlockArgs<R> a, const __grid_constant__ BoxMaps<7> maps) {
+    using TileT = StateBoxTile<R>;
+    constexpr int NC = TileT::NE;
+    __shared__ __align__(128) TileT t;
+    __shared__ unsigned long long bar;
     const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
     const int ny = a.ny, nx = a.nx;
-    stage_tile<R, kTile, 1, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
-    __syncthreads();
-    TileView<R, kTile, 1, 1> s{t, i0, j0, ny, nx};
+    if (!stage_state_boxes<R>(t, maps, a.u, a.v, a.H, a.phi, a.bed, a.beta, a.B, i0, j0, &bar, a.err)) return;
+    StateBoxView<R> s{t, i0, j0, ny, nx};
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
         int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        R Bc = a.B.at(clampi(gi, 0, ny - 1), clampi(gj, 0, nx - 1));
-        t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+        t.eta[r][c] = eta_at<R>(s, s.BC(gi, gj), a.p, gi, gj);
     }
     __syncthreads();
     const int i = i0 + threadIdx.x / kTile, j = j0 + threadIdx.x % kTile;

@@ -3,6 +3,7 @@
 
 #include "stencil.cuh"
 #include "tile.cuh"
+#include "tma.cuh"
 
 namespace glide {
 
@@ -23,30 +24,31 @@ struct ResidualArgs {
     Arr<R> o_u, o_v, o_H;        // outputs
     Arr<R> s_u, s_v, s_H;        // optional subtrahends (p == nullptr: none)
     double* partial;             // optional: 3 sums of squares per block
+    int* err;                    // set when a bounded wait gives up
     PhysR<R> p;
     int ny, nx;
     int use_forcing, use_mask;
     int active_set;              // Newton mode (see the mass row below)
 };
 
-// Each warp computes a 4 x 8 patch of the 16 x 16 tile; rows are padded to 24
-// entries so that the patch's stencil reads are bank-conflict free.
+// The tile's state is staged in box layout (TMA on large levels).  Each warp
+// computes a 4 x 8 patch of the 16 x 16 tile; with 24-entry rows the patch's
+// stencil reads are bank-conflict free.
 template <class R>
-__global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a) {
-    using TileT = Tile<R, kTile, 1, 1, 24>;
-    constexpr int NC = TileT::NC;
-    __shared__ TileT t;
+__global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a, const __grid_constant__ BoxMaps<7> maps) {
+    using TileT = StateBoxTile<R>;
+    constexpr int NC = TileT::NE;
+    __shared__ __align__(128) TileT t;
     __shared__ double red[3][8];
+    __shared__ unsigned long long bar;
     const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
     const int ny = a.ny, nx = a.nx;
-    stage_tile<R, kTile, 1, 1, 24>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
-    __syncthreads();
-    TileView<R, kTile, 1, 1, 24> s{t, i0, j0, ny, nx};
+    if (!stage_state_boxes<R>(t, maps, a.u, a.v, a.H, a.phi, a.bed, a.beta, a.B, i0, j0, &bar, a.err)) return;
+    StateBoxView<R> s{t, i0, j0, ny, nx};
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
         int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        R Bc = ldg(&a.B.p[size_t(clampi(gi, 0, ny - 1)) * a.B.pitch + clampi(gj, 0, nx - 1)]);
-        t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+        t.eta[r][c] = eta_at<R>(s, s.BC(gi, gj), a.p, gi, gj);
     }
     __syncthreads();
     const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;

@@ -172,7 +172,11 @@ extern "C" int glide_residual_norms_noalloc(int ny, int nx, double dx, double dt
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
-        k_residual<double><<<dim3(unsigned(tiles_x), unsigned(tiles_y)), 256, 0, s>>>(a);
+        // caller-owned arrays: the tiles are staged with clamped scalar loads
+        BoxMaps<7> maps;
+        maps.use = 0;
+        a.err = nullptr;
+        k_residual<double><<<dim3(unsigned(tiles_x), unsigned(tiles_y)), 256, 0, s>>>(a, maps);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {

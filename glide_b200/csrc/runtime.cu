@@ -8,8 +8,10 @@
 // one V-cycle plus its convergence-check residual is captured once and
 // replayed, so a solve costs one host synchronisation per V-cycle.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -147,6 +149,24 @@ static glide_vanka_config default_tangent_vanka() {
 
 static int round_up(int a, int m) { return (a + m - 1) / m * m; }
 
+// the arrays of a StateBoxTile, in its staging order
+static constexpr int kStateBoxes[7] = {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_BED, GLIDE_BETA, GLIDE_B};
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library links only libcudart)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
 struct SolverBase {
     virtual ~SolverBase() {}
     int dtype = GLIDE_F64;
@@ -185,6 +205,11 @@ struct Solver : SolverBase {
     double* partial = nullptr;
     double* norms_dev = nullptr;
     double* norms_host = nullptr;
+    int* err_dev = nullptr;  // set by a kernel whose bounded wait gave up
+    // TMA tensor maps of every (level, field), encoded on first use
+    std::vector<CUtensorMap> tmaps;
+    std::vector<unsigned char> tmap_done;
+    bool use_tma = true;
     // one captured V-cycle per cycle kind (0 FAS, 1 adjoint, 2 mixed FAS,
     // 3 mixed adjoint, 4 Newton), each valid for the (version, dt, start) it
     // was captured with, so that solves alternating kinds replay, not recapture
@@ -251,7 +276,8 @@ struct Solver : SolverBase {
                 v.a[f].p = reinterpret_cast<R*>(arena + reinterpret_cast<size_t>(v.a[f].p));
         partial = reinterpret_cast<double*>(arena + partial_off);
         norms_dev = reinterpret_cast<double*>(arena + norms_off);
-        GCU(cudaMallocHost(&norms_host, 4 * sizeof(double)));
+        err_dev = reinterpret_cast<int*>(arena + norms_off + 4 * sizeof(double));
+        GCU(cudaMallocHost(&norms_host, 5 * sizeof(double)));
         // gamma holds thklim between sweep groups
         for (auto& v : lv) fill(v.a[GLIDE_GAMMA], R(v.phys.thklim), nullptr);
         GCU(cudaDeviceSynchronize());
@@ -332,12 +358,13 @@ struct Solver : SolverBase {
         a.o_u = v.a[out_u]; a.o_v = v.a[out_v]; a.o_H = v.a[out_H];
         if (sub) { a.s_u = sub[0]; a.s_v = sub[1]; a.s_H = sub[2]; }
         a.partial = norms ? partial : nullptr;
+        a.err = err_dev;
         a.p = physr(l, dt, freeze_calving);
         a.ny = v.ny; a.nx = v.nx;
         a.use_forcing = use_forcing; a.use_mask = use_mask;
         a.active_set = active_set ? 1 : 0;
         dim3 g(v.blocks_x(), v.blocks_y());
-        k_residual<R><<<g, 256, 0, s>>>(a);
+        k_residual<R><<<g, 256, 0, s>>>(a, box_maps(l, kStateBoxes));
         counted("residual");
         if (norms) {
             k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
@@ -353,6 +380,7 @@ struct Solver : SolverBase {
         a.beta = v.a[GLIDE_BETA]; a.gamma = v.a[GLIDE_GAMMA];
         a.f_u = v.a[GLIDE_F_U]; a.f_v = v.a[GLIDE_F_V]; a.f_H = v.a[GLIDE_F_H];
         a.partial = nullptr;
+        a.err = err_dev;
         a.p = physr(l, dt, false);
         a.ny = v.ny; a.nx = v.nx;
         a.use_forcing = 1; a.use_mask = 0; a.active_set = 0;
@@ -360,10 +388,51 @@ struct Solver : SolverBase {
         counted("vanka_dump");
     }
 
+    // the norm vector and, in the same copy, the error word behind it
     void read_norms(double out[4], cudaStream_t s) {
-        GCU(cudaMemcpyAsync(norms_host, norms_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GCU(cudaMemcpyAsync(norms_host, norms_dev, 4 * sizeof(double) + sizeof(int), cudaMemcpyDeviceToHost, s));
         GCU(cudaStreamSynchronize(s));
         for (int q = 0; q < 4; ++q) out[q] = norms_host[q];
+        int e;
+        std::memcpy(&e, norms_host + 4, sizeof(int));
+        if (e) fail(GLIDE_ERR_CUDA, "a kernel's bounded wait for its tile copies gave up");
+    }
+
+    // TMA staging needs a level at least one box wide and high
+    bool tma_level(int l) const { return use_tma && lv[l].nx >= kBoxW && lv[l].ny >= kBoxH; }
+
+    const CUtensorMap& tmap(int l, int f) {
+        if (tmaps.empty()) {
+            tmaps.resize(size_t(n_levels) * F_COUNT);
+            tmap_done.assign(size_t(n_levels) * F_COUNT, 0);
+        }
+        const size_t k = size_t(l) * F_COUNT + f;
+        if (!tmap_done[k]) {
+            PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+            if (!enc) fail(GLIDE_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+            const Arr<R>& a = lv[l].a[f];
+            const cuuint64_t dims[2] = {cuuint64_t(a.cols), cuuint64_t(a.rows)};
+            const cuuint64_t strides[1] = {cuuint64_t(a.pitch) * sizeof(R)};
+            const cuuint32_t box[2] = {cuuint32_t(kBoxW), cuuint32_t(kBoxH)};
+            const cuuint32_t estr[2] = {1, 1};
+            const CUresult r = enc(&tmaps[k], sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                                               : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                   2, a.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) fail(GLIDE_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+            tmap_done[k] = 1;
+        }
+        return tmaps[k];
+    }
+
+    template <int N>
+    BoxMaps<N> box_maps(int l, const int (&fields)[N]) {
+        BoxMaps<N> m;
+        m.use = tma_level(l) ? 1 : 0;
+        if (m.use)
+            for (int q = 0; q < N; ++q) m.m[q] = tmap(l, fields[q]);
+        return m;
     }
 
     // n additive-Vanka sweeps on level l, ending in the home state buffers
@@ -562,6 +631,8 @@ struct Solver : SolverBase {
         f.quirks = quirks;
         f.sweep_blocks_per_sm = sweep_blocks_per_sm;
         f.use_graphs = 0;
+        f.use_tma = use_tma;
+        f.err_dev = err_dev;  // shadow kernels report into this handle's error word
         for (int l = 0; l < n_levels; ++l) {
             if (f.lv[l].phys.thklim != lv[l].phys.thklim)
                 f.fill(f.lv[l].a[GLIDE_GAMMA], float(lv[l].phys.thklim), nullptr);
@@ -775,6 +846,7 @@ struct Solver : SolverBase {
         a.o_u = v.a[out[0]]; a.o_v = v.a[out[1]]; a.o_H = v.a[out[2]];
         if (sub) { a.s_u = v.a[sub[0]]; a.s_v = v.a[sub[1]]; a.s_H = v.a[sub[2]]; }
         a.partial = norms ? partial : nullptr;
+        a.err = err_dev;
         a.p = physr(l, dt, false);
         a.ny = v.ny; a.nx = v.nx; a.use_forcing = use_forcing;
         dim3 g((a.nx + kTileA - 1) / kTileA, (a.ny + kTileA - 1) / kTileA);
@@ -782,7 +854,9 @@ struct Solver : SolverBase {
             k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a);
             counted("vjp");
         } else {
-            k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, ref_rows ? 1 : 0);
+            const int fl[JvpTile<R>::NB] = {GLIDE_U, GLIDE_V, L.x[0], L.x[1], GLIDE_H, GLIDE_PHI, GLIDE_BED,
+                                            GLIDE_BETA, GLIDE_B, L.x[2]};
+            k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, ref_rows ? 1 : 0, box_maps(l, fl));
             counted("jvp");
         }
         if (norms) {
@@ -826,6 +900,7 @@ struct Solver : SolverBase {
         a.f = blk[l];
         a.plane = size_t(v.ny) * v.pc;
         a.pitch = v.pc;
+        a.err = err_dev;
         a.p = physr(l, dt, false);
         a.omega = R(c.omega); a.ssa_damping = R(c.ssa_damping); a.mc_damping = R(c.mc_damping);
         a.ny = v.ny; a.nx = v.nx;
@@ -835,8 +910,9 @@ struct Solver : SolverBase {
     void block_factor(int l, double dt, const Lin& L, cudaStream_t s) {
         BlockArgs<R> a = block_args(l, dt, L);
         dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
-        if (L.tr) k_block_factor<R, true><<<g, kTile * kTile, 0, s>>>(a);
-        else k_block_factor<R, false><<<g, kTile * kTile, 0, s>>>(a);
+        const BoxMaps<7> m = box_maps(l, kStateBoxes);
+        if (L.tr) k_block_factor<R, true><<<g, kTile * kTile, 0, s>>>(a, m);
+        else k_block_factor<R, false><<<g, kTile * kTile, 0, s>>>(a, m);
         counted("block_factor");
     }
 
@@ -1229,6 +1305,9 @@ int glide_set_tuning(glide_handle h, int key, int value) {
             } else if (key == GLIDE_TUNE_TANGENT_VCYCLES) {
                 if (value < 1 || value > 16) fail(GLIDE_ERR_ARG, "tangent V-cycles must be in [1, 16]");
                 s.tangent_vcycles = value;
+            } else if (key == GLIDE_TUNE_TMA_STAGING) {
+                if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "TMA staging must be 0 or 1");
+                s.use_tma = value != 0;
             } else {
                 fail(GLIDE_ERR_ARG, "unknown tuning key");
             }

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "adjoint_kernels.cuh"
+#include "tma.cuh"
 
 namespace glide {
 
@@ -139,15 +140,16 @@ __device__ __forceinline__ R vmom_jvp(const S& s, const PhysR<R>& p, int i, int 
     return d;
 }
 
-// Staged tile of the JVP: the state and e with a one-cell halo, eta and
-// eta-dot.  Rows are padded to 24 entries: with the 4 x 8 cell patch each warp
-// computes (see jvp_cell), every stencil access of a warp then hits distinct
-// shared-memory banks, for 4- and 8-byte values alike.
+// Staged tile of the JVP: state, e and B in the TMA box layout (rows from
+// i0 - 2, columns from j0 - 4), eta and eta-dot of the tile plus a one-cell
+// halo.  With 24-entry rows and the 4 x 8 cell patch each warp computes (see
+// k_jvp), every stencil access of a warp hits distinct shared-memory banks,
+// for 4- and 8-byte values alike.
 template <class R>
 struct JvpTile {
-    static constexpr int T = kTileA, A = 1, NC = T + 2, P = 24;
-    R u[NC + 2][P], v[NC + 1][P], eu[NC + 2][P], ev[NC + 1][P];
-    R H[NC][P], phi[NC][P], bed[NC][P], beta[NC][P], eta[NC][P], etad[NC][P], eH[NC][P];
+    static constexpr int T = kTileA, A = 1, NC = T + 2, P = 24, NB = 10;
+    Box<R> u, v, eu, ev, H, phi, bed, beta, B, eH;
+    R eta[NC][P], etad[NC][P];
 };
 
 template <class R>
@@ -155,17 +157,20 @@ struct JvpView {
     const JvpTile<R>& t;
     int i0, j0, ny, nx;
     static constexpr int A = 1;
-    __device__ R U(int i, int j) const { return t.u[i - (i0 - A - 1)][j - (j0 - A)]; }
-    __device__ R V(int i, int j) const { return t.v[i - (i0 - A)][j - (j0 - A - 1)]; }
-    __device__ R LU(int i, int j) const { return t.eu[i - (i0 - A - 1)][j - (j0 - A)]; }
-    __device__ R LV(int i, int j) const { return t.ev[i - (i0 - A)][j - (j0 - A - 1)]; }
-    __device__ R Hc(int i, int j) const { return t.H[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R PHI(int i, int j) const { return t.phi[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R BED(int i, int j) const { return t.bed[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R BETA(int i, int j) const { return t.beta[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ int r(int i) const { return i - (i0 - kBoxY); }
+    __device__ int c(int j) const { return j - (j0 - kBoxX); }
+    __device__ R U(int i, int j) const { return t.u[r(i)][c(j)]; }
+    __device__ R V(int i, int j) const { return t.v[r(i)][c(j)]; }
+    __device__ R LU(int i, int j) const { return t.eu[r(i)][c(j)]; }
+    __device__ R LV(int i, int j) const { return t.ev[r(i)][c(j)]; }
+    __device__ R Hc(int i, int j) const { return t.H[r(i)][c(j)]; }
+    __device__ R PHI(int i, int j) const { return t.phi[r(i)][c(j)]; }
+    __device__ R BED(int i, int j) const { return t.bed[r(i)][c(j)]; }
+    __device__ R BETA(int i, int j) const { return t.beta[r(i)][c(j)]; }
+    __device__ R BC(int i, int j) const { return t.B[r(i)][c(j)]; }
     __device__ R ETA(int i, int j) const { return t.eta[i - (i0 - A)][j - (j0 - A)]; }
     __device__ R ETAD(int i, int j) const { return t.etad[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R EH(int i, int j) const { return t.eH[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R EH(int i, int j) const { return t.eH[r(i)][c(j)]; }
 };
 
 // Viscosity and its derivative along e at one cell, sharing the strain rates
@@ -196,54 +201,31 @@ __device__ __forceinline__ void eta_and_dot(const S& s, R Bc, const PhysR<R>& p,
     etad = eta * p.gexp * deII / eII;
 }
 
-template <class R>
-__device__ void stage_jvp(JvpTile<R>& t, int i0, int j0, const VjpArgs<R>& a) {
-    using TT = JvpTile<R>;
-    constexpr int NC = TT::NC, A = TT::A;
-    const int ny = a.ny, nx = a.nx, tid = threadIdx.x, nt = blockDim.x;
-    for (int k = tid; k < (NC + 2) * (NC + 1); k += nt) {
-        int r = k / (NC + 1), c = k % (NC + 1);
-        int gi = clampi(i0 - A - 1 + r, 0, ny - 1), gj = clampi(j0 - A + c, 0, nx);
-        t.u[r][c] = ldg(&a.u.p[size_t(gi) * a.u.pitch + gj]);
-        t.eu[r][c] = ldg(&a.lu.p[size_t(gi) * a.lu.pitch + gj]);
-    }
-    for (int k = tid; k < (NC + 1) * (NC + 2); k += nt) {
-        int r = k / (NC + 2), c = k % (NC + 2);
-        int gi = clampi(i0 - A + r, 0, ny), gj = clampi(j0 - A - 1 + c, 0, nx - 1);
-        t.v[r][c] = ldg(&a.v.p[size_t(gi) * a.v.pitch + gj]);
-        t.ev[r][c] = ldg(&a.lv.p[size_t(gi) * a.lv.pitch + gj]);
-    }
-    for (int k = tid; k < NC * NC; k += nt) {
-        int r = k / NC, c = k % NC;
-        int gi = clampi(i0 - A + r, 0, ny - 1), gj = clampi(j0 - A + c, 0, nx - 1);
-        size_t o = size_t(gi) * a.H.pitch + gj;  // all cell arrays share one pitch
-        t.H[r][c] = ldg(&a.H.p[o]);
-        t.bed[r][c] = ldg(&a.bed.p[o]);
-        t.beta[r][c] = ldg(&a.beta.p[o]);
-        t.phi[r][c] = ldg(&a.phi.p[o]);
-        t.eH[r][c] = ldg(&a.lH.p[o]);
-    }
-}
-
 // r_lin = J e - f (- sub) over one level, optional per-block sums of squares.
 // Uses VjpArgs with lu/lv/lH carrying e and f_* the right-hand side.  Each
 // warp computes a 4 x 8 patch of the 16 x 16 tile.
+// The arrays k_jvp stages, in the order of its BoxMaps: u, v, e_u, e_v, H,
+// phi, bed, beta, B, e_H.
 template <class R>
-__global__ void __launch_bounds__(kTileA * kTileA) k_jvp(VjpArgs<R> a, int ref_rows) {
+__global__ void __launch_bounds__(kTileA * kTileA)
+    k_jvp(VjpArgs<R> a, int ref_rows, const __grid_constant__ BoxMaps<JvpTile<R>::NB> maps) {
     using TT = JvpTile<R>;
     constexpr int NC = TT::NC;
-    __shared__ TT T;
+    __shared__ __align__(128) TT T;
     __shared__ double red[3][kTileA * kTileA / 32];
+    __shared__ unsigned long long bar;
     const int i0 = blockIdx.y * kTileA, j0 = blockIdx.x * kTileA;
     const int ny = a.ny, nx = a.nx;
-    stage_jvp(T, i0, j0, a);
-    __syncthreads();
+    {
+        Box<R>* const dst[TT::NB] = {&T.u, &T.v, &T.eu, &T.ev, &T.H, &T.phi, &T.bed, &T.beta, &T.B, &T.eH};
+        const Arr<R> src[TT::NB] = {a.u, a.v, a.lu, a.lv, a.H, a.phi, a.bed, a.beta, a.B, a.lH};
+        if (!stage_boxes<R, TT::NB>(dst, src, maps, i0, j0, &bar, a.err)) return;
+    }
     JvpView<R> s{T, i0, j0, ny, nx};
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
         int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        R Bc = a.B.at(clampi(gi, 0, ny - 1), clampi(gj, 0, nx - 1));
-        eta_and_dot<R>(s, Bc, a.p, gi, gj, T.eta[r][c], T.etad[r][c]);
+        eta_and_dot<R>(s, s.BC(gi, gj), a.p, gi, gj, T.eta[r][c], T.etad[r][c]);
     }
     __syncthreads();
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;

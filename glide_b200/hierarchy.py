@@ -180,7 +180,7 @@ class Hierarchy:
 
     def set_tuning(self, sweep_blocks_per_sm: int | None = None, mixed_inner_vcycles: int | None = None,
                    forward_method: str | None = None, newton_switch_exp10: int | None = None,
-                   tangent_vcycles: int | None = None):
+                   tangent_vcycles: int | None = None, tma_staging: bool | None = None):
         """Solver knobs with no counterpart in the reference (see glide_set_tuning).
         forward_method: "fascd" (the reference's V-cycles only) or "newton"
         (FASCD until 10^-newton_switch_exp10, then Newton steps whose correction
@@ -195,6 +195,8 @@ class Hierarchy:
             call("glide_set_tuning", self._h, 4, int(newton_switch_exp10))
         if tangent_vcycles is not None:
             call("glide_set_tuning", self._h, 5, int(tangent_vcycles))
+        if tma_staging is not None:
+            call("glide_set_tuning", self._h, 6, int(bool(tma_staging)))
 
     def launch_count(self) -> int:
         c = ctypes.c_longlong()

@@ -164,6 +164,10 @@ int glide_launch_count(glide_handle h, long long* count);
 #define GLIDE_TUNE_FORWARD_METHOD 3
 #define GLIDE_TUNE_NEWTON_SWITCH_EXP10 4
 #define GLIDE_TUNE_TANGENT_VCYCLES 5
+/* GLIDE_TUNE_TMA_STAGING: 1 (default) stages the halo tiles of the stencil
+ * kernels with TMA bulk tensor copies on levels at least 24 x 20 cells;
+ * 0 uses clamped per-thread loads everywhere (same results). */
+#define GLIDE_TUNE_TMA_STAGING 6
 int glide_set_tuning(glide_handle h, int key, int value);
 
 int glide_set_rhs(glide_handle h, int level, double dt, void* stream);
