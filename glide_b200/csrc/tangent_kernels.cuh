@@ -36,108 +36,92 @@ __device__ __forceinline__ R mass_jvp(const S& s, const PhysR<R>& p, int i, int 
     return d;
 }
 
-// d(x-momentum row on u face (i,j)) . e (residuals.cu:441-548), interior rows
+// Linearised stresses along e, built from the per-cell products the tile
+// holds: etaH = eta H and detaH = eta-dot H + eta e_H (the derivative of
+// eta H).  Each is the stress routine's derivative coefficients (stress.cu;
+// sxx / syy / sxy in stencil.cuh) contracted with e.
+//
+// sigma_xx H on cell (i, j) (stress.cu:44-66): d_ul = -2q, d_ur = 2q,
+// d_vt = q, d_vb = -q with q = 2 eta H dxi, d_eH = 2 e.
 template <class R, class S>
-__device__ __forceinline__ R umom_jvp(const S& s, const PhysR<R>& p, int i, int j) {
-    const int ny = s.ny, nx = s.nx;
-    const R dxi = p.dxi;
-    const R Hc = s.Hc(i, j), Hl = s.Hc(i, j - 1), ul = s.U(i, j);
-    R d = 0;
-    {
-        NormalT<R> a = sxx(ul, s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.ETA(i, j) * Hc, dxi, j, nx);
-        d += (a.d_ul * s.LU(i, j) + a.d_ur * s.LU(i, j + 1) + a.d_vt * s.LV(i, j) + a.d_vb * s.LV(i + 1, j) +
-              a.d_eH * (s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j))) * dxi;
-    }
-    {
-        NormalT<R> a = sxx(s.U(i, j - 1), ul, s.V(i, j - 1), s.V(i + 1, j - 1), s.ETA(i, j - 1) * Hl, dxi, j - 1, nx);
-        d -= (a.d_ul * s.LU(i, j - 1) + a.d_ur * s.LU(i, j) + a.d_vt * s.LV(i, j - 1) +
-              a.d_vb * s.LV(i + 1, j - 1) + a.d_eH * (s.ETAD(i, j - 1) * Hl + s.ETA(i, j - 1) * s.EH(i, j - 1))) * dxi;
-    }
-    {
-        R eH = vertex_eH(s.ETA(i - 1, j - 1), s.ETA(i - 1, j), s.ETA(i, j - 1), s.ETA(i, j), s.Hc(i - 1, j - 1),
-                         s.Hc(i - 1, j), Hl, Hc);
-        R deH = R(0.25) * (s.ETAD(i - 1, j - 1) * s.Hc(i - 1, j - 1) + s.ETA(i - 1, j - 1) * s.EH(i - 1, j - 1) +
-                           s.ETAD(i - 1, j) * s.Hc(i - 1, j) + s.ETA(i - 1, j) * s.EH(i - 1, j) +
-                           s.ETAD(i, j - 1) * Hl + s.ETA(i, j - 1) * s.EH(i, j - 1) +
-                           s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j));
-        ShearT<R> a = sxy(s.U(i - 1, j), ul, s.V(i, j - 1), s.V(i, j), eH, dxi, i, j, ny, nx);
-        d += (a.d_ut * s.LU(i - 1, j) + a.d_ub * s.LU(i, j) + a.d_vl * s.LV(i, j - 1) + a.d_vr * s.LV(i, j) +
-              a.d_eH * deH) * dxi;
-    }
-    {
-        R eH = vertex_eH(s.ETA(i, j - 1), s.ETA(i, j), s.ETA(i + 1, j - 1), s.ETA(i + 1, j), Hl, Hc,
-                         s.Hc(i + 1, j - 1), s.Hc(i + 1, j));
-        R deH = R(0.25) * (s.ETAD(i, j - 1) * Hl + s.ETA(i, j - 1) * s.EH(i, j - 1) + s.ETAD(i, j) * Hc +
-                           s.ETA(i, j) * s.EH(i, j) + s.ETAD(i + 1, j - 1) * s.Hc(i + 1, j - 1) +
-                           s.ETA(i + 1, j - 1) * s.EH(i + 1, j - 1) + s.ETAD(i + 1, j) * s.Hc(i + 1, j) +
-                           s.ETA(i + 1, j) * s.EH(i + 1, j));
-        ShearT<R> a = sxy(ul, s.U(i + 1, j), s.V(i + 1, j - 1), s.V(i + 1, j), eH, dxi, i + 1, j, ny, nx);
-        d -= (a.d_ut * s.LU(i, j) + a.d_ub * s.LU(i + 1, j) + a.d_vl * s.LV(i + 1, j - 1) +
-              a.d_vr * s.LV(i + 1, j) + a.d_eH * deH) * dxi;
-    }
-    {
-        BasalT<R> b = basal(ul, s.V(i, j - 1), s.V(i, j), s.V(i + 1, j - 1), s.V(i + 1, j), s.PHI(i, j - 1),
-                            s.PHI(i, j), s.BETA(i, j - 1), s.BETA(i, j), p);
-        d += b.d_w * s.LU(i, j) + b.d_a * s.LV(i, j - 1) + b.d_b * s.LV(i, j) + b.d_c * s.LV(i + 1, j - 1) +
-             b.d_d * s.LV(i + 1, j);
-    }
-    {
-        DriveT<R> dr = driving(Hl, Hc, s.BED(i, j - 1), s.BED(i, j), s.PHI(i, j - 1), s.PHI(i, j), dxi, j, nx);
-        d -= dr.d_H0 * s.EH(i, j - 1) + dr.d_H1 * s.EH(i, j);
-    }
-    return d;
+__device__ __forceinline__ R nxx_lin(const S& s, R dxi, int i, int j, int nx) {
+    if (j < 0 || j >= nx) return R(0);
+    const R e = R(2) * (s.U(i, j + 1) - s.U(i, j)) * dxi + (s.V(i, j) - s.V(i + 1, j)) * dxi;
+    const R q = R(2) * s.ETAH(i, j) * dxi;
+    return q * (R(2) * (s.LU(i, j + 1) - s.LU(i, j)) + (s.LV(i, j) - s.LV(i + 1, j))) + R(2) * e * s.DETAH(i, j);
 }
 
-// d(y-momentum row on v face (i,j)) . e (residuals.cu:551-658), interior rows
+// sigma_yy H on cell (i, j) (stress.cu:79-102): d_ul = -q, d_ur = q,
+// d_vt = 2q, d_vb = -2q, d_eH = 2 e.
 template <class R, class S>
-__device__ __forceinline__ R vmom_jvp(const S& s, const PhysR<R>& p, int i, int j) {
+__device__ __forceinline__ R nyy_lin(const S& s, R dxi, int i, int j, int ny) {
+    if (i < 0 || i >= ny) return R(0);
+    const R e = (s.U(i, j + 1) - s.U(i, j)) * dxi + R(2) * (s.V(i, j) - s.V(i + 1, j)) * dxi;
+    const R q = R(2) * s.ETAH(i, j) * dxi;
+    return q * ((s.LU(i, j + 1) - s.LU(i, j)) + R(2) * (s.LV(i, j) - s.LV(i + 1, j))) + R(2) * e * s.DETAH(i, j);
+}
+
+// sigma_xy H on vertex (i, j), zero on the boundary (stress.cu:160-183), with
+// the vertex's eta H the mean of its four cells: d_ut = q, d_ub = -q,
+// d_vl = -q, d_vr = q with q = eta H dxi, d_eH = 2 e.
+template <class R, class S>
+__device__ __forceinline__ R sxy_lin(const S& s, R dxi, int i, int j, int ny, int nx) {
+    if (i <= 0 || i >= ny || j <= 0 || j >= nx) return R(0);
+    const R e = R(0.5) * ((s.U(i - 1, j) - s.U(i, j)) * dxi + (s.V(i, j) - s.V(i, j - 1)) * dxi);
+    const R eH = R(0.25) * (s.ETAH(i - 1, j - 1) + s.ETAH(i - 1, j) + s.ETAH(i, j - 1) + s.ETAH(i, j));
+    const R deH = R(0.25) * (s.DETAH(i - 1, j - 1) + s.DETAH(i - 1, j) + s.DETAH(i, j - 1) + s.DETAH(i, j));
+    const R q = eH * dxi;
+    return q * ((s.LU(i - 1, j) - s.LU(i, j)) + (s.LV(i, j) - s.LV(i, j - 1))) + R(2) * e * deH;
+}
+
+// d(x-momentum row on u face (i,j)) . e and d(y-momentum row on v face
+// (i,j)) . e for interior rows (residuals.cu:441-658).  The shear on vertex
+// (i, j) enters both rows and is evaluated once; `want_u` / `want_v` skip a
+// row the caller pins.
+template <class R, class S>
+__device__ __forceinline__ void mom_jvp(const S& s, const PhysR<R>& p, int i, int j, bool want_u, bool want_v,
+                                        R& du, R& dv) {
     const int ny = s.ny, nx = s.nx;
     const R dxi = p.dxi;
-    const R Hc = s.Hc(i, j), Ht = s.Hc(i - 1, j), vt = s.V(i, j);
-    R d = 0;
-    {
-        NormalT<R> a = syy(s.U(i - 1, j), s.U(i - 1, j + 1), s.V(i - 1, j), vt, s.ETA(i - 1, j) * Ht, dxi, i - 1, ny);
-        d += (a.d_ul * s.LU(i - 1, j) + a.d_ur * s.LU(i - 1, j + 1) + a.d_vt * s.LV(i - 1, j) +
-              a.d_vb * s.LV(i, j) + a.d_eH * (s.ETAD(i - 1, j) * Ht + s.ETA(i - 1, j) * s.EH(i - 1, j))) * dxi;
+    const R sh = sxy_lin<R>(s, dxi, i, j, ny, nx);
+    if (want_u) {
+        const R Hc = s.Hc(i, j), Hl = s.Hc(i, j - 1), ul = s.U(i, j);
+        R d = 0;
+        d += nxx_lin<R>(s, dxi, i, j, nx) * dxi;
+        d -= nxx_lin<R>(s, dxi, i, j - 1, nx) * dxi;
+        d += sh * dxi;
+        d -= sxy_lin<R>(s, dxi, i + 1, j, ny, nx) * dxi;
+        {
+            BasalT<R> b = basal(ul, s.V(i, j - 1), s.V(i, j), s.V(i + 1, j - 1), s.V(i + 1, j), s.PHI(i, j - 1),
+                                s.PHI(i, j), s.BETA(i, j - 1), s.BETA(i, j), p);
+            d += b.d_w * s.LU(i, j) + b.d_a * s.LV(i, j - 1) + b.d_b * s.LV(i, j) + b.d_c * s.LV(i + 1, j - 1) +
+                 b.d_d * s.LV(i + 1, j);
+        }
+        {
+            DriveT<R> dr = driving(Hl, Hc, s.BED(i, j - 1), s.BED(i, j), s.PHI(i, j - 1), s.PHI(i, j), dxi, j, nx);
+            d -= dr.d_H0 * s.EH(i, j - 1) + dr.d_H1 * s.EH(i, j);
+        }
+        du = d;
     }
-    {
-        NormalT<R> a = syy(s.U(i, j), s.U(i, j + 1), vt, s.V(i + 1, j), s.ETA(i, j) * Hc, dxi, i, ny);
-        d -= (a.d_ul * s.LU(i, j) + a.d_ur * s.LU(i, j + 1) + a.d_vt * s.LV(i, j) + a.d_vb * s.LV(i + 1, j) +
-              a.d_eH * (s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j))) * dxi;
+    if (want_v) {
+        const R Hc = s.Hc(i, j), Ht = s.Hc(i - 1, j), vt = s.V(i, j);
+        R d = 0;
+        d += nyy_lin<R>(s, dxi, i - 1, j, ny) * dxi;
+        d -= nyy_lin<R>(s, dxi, i, j, ny) * dxi;
+        d -= sh * dxi;
+        d += sxy_lin<R>(s, dxi, i, j + 1, ny, nx) * dxi;
+        {
+            BasalT<R> b = basal(vt, s.U(i - 1, j), s.U(i - 1, j + 1), s.U(i, j), s.U(i, j + 1), s.PHI(i - 1, j),
+                                s.PHI(i, j), s.BETA(i - 1, j), s.BETA(i, j), p);
+            d += b.d_w * s.LV(i, j) + b.d_a * s.LU(i - 1, j) + b.d_b * s.LU(i - 1, j + 1) + b.d_c * s.LU(i, j) +
+                 b.d_d * s.LU(i, j + 1);
+        }
+        {
+            DriveT<R> dr = driving(Hc, Ht, s.BED(i, j), s.BED(i - 1, j), s.PHI(i, j), s.PHI(i - 1, j), dxi, i, ny);
+            d -= dr.d_H0 * s.EH(i, j) + dr.d_H1 * s.EH(i - 1, j);
+        }
+        dv = d;
     }
-    {
-        R eH = vertex_eH(s.ETA(i - 1, j - 1), s.ETA(i - 1, j), s.ETA(i, j - 1), s.ETA(i, j), s.Hc(i - 1, j - 1), Ht,
-                         s.Hc(i, j - 1), Hc);
-        R deH = R(0.25) * (s.ETAD(i - 1, j - 1) * s.Hc(i - 1, j - 1) + s.ETA(i - 1, j - 1) * s.EH(i - 1, j - 1) +
-                           s.ETAD(i - 1, j) * Ht + s.ETA(i - 1, j) * s.EH(i - 1, j) +
-                           s.ETAD(i, j - 1) * s.Hc(i, j - 1) + s.ETA(i, j - 1) * s.EH(i, j - 1) +
-                           s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j));
-        ShearT<R> a = sxy(s.U(i - 1, j), s.U(i, j), s.V(i, j - 1), vt, eH, dxi, i, j, ny, nx);
-        d -= (a.d_ut * s.LU(i - 1, j) + a.d_ub * s.LU(i, j) + a.d_vl * s.LV(i, j - 1) + a.d_vr * s.LV(i, j) +
-              a.d_eH * deH) * dxi;
-    }
-    {
-        R eH = vertex_eH(s.ETA(i - 1, j), s.ETA(i - 1, j + 1), s.ETA(i, j), s.ETA(i, j + 1), Ht, s.Hc(i - 1, j + 1),
-                         Hc, s.Hc(i, j + 1));
-        R deH = R(0.25) * (s.ETAD(i - 1, j) * Ht + s.ETA(i - 1, j) * s.EH(i - 1, j) +
-                           s.ETAD(i - 1, j + 1) * s.Hc(i - 1, j + 1) + s.ETA(i - 1, j + 1) * s.EH(i - 1, j + 1) +
-                           s.ETAD(i, j) * Hc + s.ETA(i, j) * s.EH(i, j) + s.ETAD(i, j + 1) * s.Hc(i, j + 1) +
-                           s.ETA(i, j + 1) * s.EH(i, j + 1));
-        ShearT<R> a = sxy(s.U(i - 1, j + 1), s.U(i, j + 1), vt, s.V(i, j + 1), eH, dxi, i, j + 1, ny, nx);
-        d += (a.d_ut * s.LU(i - 1, j + 1) + a.d_ub * s.LU(i, j + 1) + a.d_vl * s.LV(i, j) +
-              a.d_vr * s.LV(i, j + 1) + a.d_eH * deH) * dxi;
-    }
-    {
-        BasalT<R> b = basal(vt, s.U(i - 1, j), s.U(i - 1, j + 1), s.U(i, j), s.U(i, j + 1), s.PHI(i - 1, j),
-                            s.PHI(i, j), s.BETA(i - 1, j), s.BETA(i, j), p);
-        d += b.d_w * s.LV(i, j) + b.d_a * s.LU(i - 1, j) + b.d_b * s.LU(i - 1, j + 1) + b.d_c * s.LU(i, j) +
-             b.d_d * s.LU(i, j + 1);
-    }
-    {
-        DriveT<R> dr = driving(Hc, Ht, s.BED(i, j), s.BED(i - 1, j), s.PHI(i, j), s.PHI(i - 1, j), dxi, i, ny);
-        d -= dr.d_H0 * s.EH(i, j) + dr.d_H1 * s.EH(i - 1, j);
-    }
-    return d;
 }
 
 // Staged tile of the JVP: state, e and B in the TMA box layout (rows from
@@ -149,7 +133,7 @@ template <class R>
 struct JvpTile {
     static constexpr int T = kTileA, A = 1, NC = T + 2, P = 24, NB = 10;
     Box<R> u, v, eu, ev, H, phi, bed, beta, B, eH;
-    R eta[NC][P], etad[NC][P];
+    R etah[NC][P], detah[NC][P];  // eta H and its derivative along e
 };
 
 template <class R>
@@ -168,8 +152,8 @@ struct JvpView {
     __device__ R BED(int i, int j) const { return t.bed[r(i)][c(j)]; }
     __device__ R BETA(int i, int j) const { return t.beta[r(i)][c(j)]; }
     __device__ R BC(int i, int j) const { return t.B[r(i)][c(j)]; }
-    __device__ R ETA(int i, int j) const { return t.eta[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R ETAD(int i, int j) const { return t.etad[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R ETAH(int i, int j) const { return t.etah[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ R DETAH(int i, int j) const { return t.detah[i - (i0 - A)][j - (j0 - A)]; }
     __device__ R EH(int i, int j) const { return t.eH[r(i)][c(j)]; }
 };
 
@@ -225,7 +209,11 @@ __global__ void __launch_bounds__(kTileA * kTileA)
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
         int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        eta_and_dot<R>(s, s.BC(gi, gj), a.p, gi, gj, T.eta[r][c], T.etad[r][c]);
+        R eta, etad;
+        eta_and_dot<R>(s, s.BC(gi, gj), a.p, gi, gj, eta, etad);
+        const R Hc = s.Hc(gi, gj);
+        T.etah[r][c] = eta * Hc;
+        T.detah[r][c] = etad * Hc + eta * s.EH(gi, gj);
     }
     __syncthreads();
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -244,10 +232,13 @@ __global__ void __launch_bounds__(kTileA * kTileA)
         if (ref_rows) dH = (R(1) - mk) * dH;
         else if (mk > R(0.5)) dH = s.EH(I, J);
         emit(a.o_H, a.f_H, a.s_H, I, J, dH, ssh);
-        R du = (J == 0) ? (ref_rows ? R(0) : s.LU(I, 0)) : umom_jvp<R>(s, a.p, I, J);
+        R du = R(0), dv = R(0);
+        mom_jvp<R>(s, a.p, I, J, J > 0, I > 0, du, dv);
+        // pinned Dirichlet rows; the boundary entries are read only on the boundary
+        if (J == 0 && !ref_rows) du = s.LU(I, 0);
+        if (I == 0 && !ref_rows) dv = s.LV(0, J);
         emit(a.o_u, a.f_u, a.s_u, I, J, du, ssu);
         if (J == nx - 1) emit(a.o_u, a.f_u, a.s_u, I, nx, ref_rows ? R(0) : s.LU(I, nx), ssu);
-        R dv = (I == 0) ? (ref_rows ? R(0) : s.LV(0, J)) : vmom_jvp<R>(s, a.p, I, J);
         emit(a.o_v, a.f_v, a.s_v, I, J, dv, ssv);
         if (I == ny - 1) emit(a.o_v, a.f_v, a.s_v, ny, J, ref_rows ? R(0) : s.LV(ny, J), ssv);
     }
