@@ -311,7 +311,7 @@ def run_kernels(a):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # binary32 fine-level kernels on the 2048^2 workload, from one ncu capture of
 # `python bench.py --mode kernels` on a B200.
-NCU_TRAFFIC_2048_FP32 = {"k_residual": 225.087e6, "k_jvp": 223.795e6, "k_vanka_sweep": 249.767e6}
+NCU_TRAFFIC_2048_FP32 = {"k_residual": 225.250e6, "k_jvp": 223.709e6, "k_vanka_sweep": 249.812e6}
 
 
 def kernel_roofline(a, h, stream, fields=None, probe=False):
