@@ -45,10 +45,12 @@ sys.path.insert(0, str(ROOT / "tests"))
 METRIC = "SSA+mass coupled steps/s at 2048^2 to rel. residual 1e-8"
 
 FORMS = {
+    # the adjoint of the fast form: short 4/4/0/50 cycles, block-smoother omega
+    # 0.8, two binary32 V-cycles per binary64 defect correction
     "fast": dict(precision="mixed", native=True, method="newton", switch=0, schedule="4,4,0,50", newton_steps=3,
-                 tangent_schedule="4,4,0,20"),
+                 tangent_schedule="4,4,0,10", adj_schedule="4,4,0,50", adj_omega=0.8, inner=2),
     "reference": dict(precision="fp64", native=False, method="fascd", switch=None, schedule=None,
-                      newton_steps=None, tangent_schedule=None),
+                      newton_steps=None, tangent_schedule=None, adj_schedule=None, adj_omega=None),
 }
 
 
@@ -100,6 +102,8 @@ def parse(argv=None):
     ap.add_argument("--tangent-vcycles", type=int, default=None)
     ap.add_argument("--tangent-schedule", default=None, help="pre,post,finest,coarsest of the tangent multigrid")
     ap.add_argument("--tangent-omega", type=float, default=None)
+    ap.add_argument("--adj-schedule", default=None, help="pre,post,finest,coarsest of the adjoint multigrid")
+    ap.add_argument("--adj-omega", type=float, default=None, help="adjoint block-smoother omega (default 0.5)")
     a = ap.parse_args(argv)
     preset = FORMS[a.form]
     for k, v in preset.items():
@@ -132,6 +136,11 @@ def apply_solver_options(h, a):
         h.set_fas(2, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
     if a.tangent_omega is not None:
         h.set_vanka(2, -1, omega=a.tangent_omega)
+    if a.adj_schedule:
+        pre, post, fin, coarse = (int(x) for x in a.adj_schedule.split(","))
+        h.set_fas(True, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
+    if a.adj_omega is not None:
+        h.set_vanka(True, -1, omega=a.adj_omega)
 
 
 def run_sweeps(a):
@@ -444,6 +453,8 @@ def run_ours(a, rank, world):
         g_ms = reduce_max(event_time(lambda: gstats.append(grad()), kg, stream), dev, world)
         grads = {"value": world * 1000.0 / g_ms, "unit": "grads/s", "ms_per_grad": g_ms,
                  "vcycles_per_grad": float(np.mean([s["vcycles"] for s in gstats])),
+                 "adjoint_schedule": a.adj_schedule or "10,20,50,200", "adjoint_omega": a.adj_omega or 0.5,
+                 "binary32_vcycles_per_correction": a.inner,
                  "what": "adjoint FAS solve to rel. residual 1e-8 plus gradients w.r.t. beta, bed, H_prev, smb"}
 
     # dominant kernels alone on the step-start state

@@ -44,14 +44,17 @@ __device__ __forceinline__ R eta_dot_at(const S& s, R Bc, const PhysR<R>& p, int
     return R(0.5) * Bc * p.gexp * glen_pow_m1(eII, p) * deII;
 }
 
-// Staged tile for the transpose: forward state, lambda and eta / eta-dot.
+// Staged tile for the transpose: forward state, lambda and B in box layout
+// (TMA on large levels) with a two-cell halo -- u faces need rows
+// [i0-3, i0+19), so the box starts at row i0 - 3 and is 24 rows high in
+// binary32, 22 in binary64 (both multiples of 128 bytes) -- and eta, eta-dot
+// on cells [i0-2, i0+18).
+constexpr int kAdjBoxY = 3;
 template <class R>
 struct AdjTile {
-    Tile<R, kTileA, 2, 2> t;
-    static constexpr int NC = Tile<R, kTileA, 2, 2>::NC;
-    R lu[NC + 2][NC + 1];
-    R lv[NC + 1][NC + 2];
-    R etad[NC][NC];
+    static constexpr int BH = sizeof(R) == 4 ? 24 : 22, NB = 9, NC = kTileA + 4, P = sizeof(R) == 4 ? 24 : NC;
+    BoxT<R, BH> u, v, H, phi, bed, beta, B, lu, lv;  // staging order of the box maps
+    R eta[NC][P], etad[NC][P];
 };
 
 template <class R>
@@ -61,15 +64,18 @@ struct AdjView {
     const Arr<R>* mask;
     int i0, j0, ny, nx;
     static constexpr int A = 2;
-    __device__ R U(int i, int j) const { return a.t.u[i - (i0 - A - 1)][j - (j0 - A)]; }
-    __device__ R V(int i, int j) const { return a.t.v[i - (i0 - A)][j - (j0 - A - 1)]; }
-    __device__ R LU(int i, int j) const { return a.lu[i - (i0 - A - 1)][j - (j0 - A)]; }
-    __device__ R LV(int i, int j) const { return a.lv[i - (i0 - A)][j - (j0 - A - 1)]; }
-    __device__ R Hc(int i, int j) const { return a.t.H[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R PHI(int i, int j) const { return a.t.phi[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R BED(int i, int j) const { return a.t.bed[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R BETA(int i, int j) const { return a.t.beta[i - (i0 - A)][j - (j0 - A)]; }
-    __device__ R ETA(int i, int j) const { return a.t.eta[i - (i0 - A)][j - (j0 - A)]; }
+    __device__ int r(int i) const { return i - (i0 - kAdjBoxY); }
+    __device__ int c(int j) const { return j - (j0 - kBoxX); }
+    __device__ R U(int i, int j) const { return a.u[r(i)][c(j)]; }
+    __device__ R V(int i, int j) const { return a.v[r(i)][c(j)]; }
+    __device__ R LU(int i, int j) const { return a.lu[r(i)][c(j)]; }
+    __device__ R LV(int i, int j) const { return a.lv[r(i)][c(j)]; }
+    __device__ R Hc(int i, int j) const { return a.H[r(i)][c(j)]; }
+    __device__ R PHI(int i, int j) const { return a.phi[r(i)][c(j)]; }
+    __device__ R BED(int i, int j) const { return a.bed[r(i)][c(j)]; }
+    __device__ R BETA(int i, int j) const { return a.beta[r(i)][c(j)]; }
+    __device__ R BC(int i, int j) const { return a.B[r(i)][c(j)]; }
+    __device__ R ETA(int i, int j) const { return a.eta[i - (i0 - A)][j - (j0 - A)]; }
     __device__ R ETAD(int i, int j) const { return a.etad[i - (i0 - A)][j - (j0 - A)]; }
     // masked cell multiplier of a source cell inside the domain
     __device__ R LHm(int i, int j) const { return lH->at(i, j) * (R(1) - mask->at(i, j)); }
@@ -257,41 +263,33 @@ struct VjpArgs {
     int ny, nx, use_forcing;
 };
 
-// Stage state, lambda, eta and eta-dot of the tile (kTileA x kTileA targets).
+// Box maps in AdjTile staging order: u, v, H, phi, bed, beta, B, lambda_u,
+// lambda_v.  Each warp computes a 4 x 8 patch of the 16 x 16 tile.
 template <class R>
-__device__ void stage_adjoint(AdjTile<R>& T, int i0, int j0, const VjpArgs<R>& a) {
-    constexpr int NC = AdjTile<R>::NC;
-    const int ny = a.ny, nx = a.nx;
-    stage_tile<R, kTileA, 2, 2>(T.t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, &a.phi);
-    for (int k = threadIdx.x; k < (NC + 2) * (NC + 1); k += blockDim.x) {
-        int r = k / (NC + 1), c = k % (NC + 1);
-        T.lu[r][c] = a.lu.at(clampi(i0 - 3 + r, 0, ny - 1), clampi(j0 - 2 + c, 0, nx));
-    }
-    for (int k = threadIdx.x; k < (NC + 1) * (NC + 2); k += blockDim.x) {
-        int r = k / (NC + 2), c = k % (NC + 2);
-        T.lv[r][c] = a.lv.at(clampi(i0 - 2 + r, 0, ny), clampi(j0 - 3 + c, 0, nx - 1));
-    }
-}
-
-template <class R>
-__global__ void __launch_bounds__(kTileA * kTileA) k_vjp(VjpArgs<R> a) {
-    constexpr int NC = AdjTile<R>::NC;
-    __shared__ AdjTile<R> T;
+__global__ void __launch_bounds__(kTileA * kTileA) k_vjp(VjpArgs<R> a, const __grid_constant__ BoxMaps<9> maps) {
+    using TT = AdjTile<R>;
+    constexpr int NC = TT::NC;
+    __shared__ __align__(128) TT T;
     __shared__ double red[3][kTileA * kTileA / 32];
+    __shared__ unsigned long long bar;
     const int i0 = blockIdx.y * kTileA, j0 = blockIdx.x * kTileA;
     const int ny = a.ny, nx = a.nx;
-    stage_adjoint(T, i0, j0, a);
-    __syncthreads();
+    {
+        BoxT<R, TT::BH>* const dst[TT::NB] = {&T.u, &T.v, &T.H, &T.phi, &T.bed, &T.beta, &T.B, &T.lu, &T.lv};
+        const Arr<R> src[TT::NB] = {a.u, a.v, a.H, a.phi, a.bed, a.beta, a.B, a.lu, a.lv};
+        if (!stage_boxes<R, TT::NB, TT::BH, kAdjBoxY>(dst, src, maps, i0, j0, &bar, a.err)) return;
+    }
     AdjView<R> s{T, &a.lH, &a.mask, i0, j0, ny, nx};
     for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
         int r = k / NC, c = k % NC;
         int gi = i0 - 2 + r, gj = j0 - 2 + c;
-        R Bc = a.B.at(clampi(gi, 0, ny - 1), clampi(gj, 0, nx - 1));
-        T.t.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
+        const R Bc = s.BC(gi, gj);
+        T.eta[r][c] = eta_at<R>(s, Bc, a.p, gi, gj);
         T.etad[r][c] = eta_dot_at<R>(s, Bc, a.p, gi, gj);
     }
     __syncthreads();
-    const int I = i0 + threadIdx.x / kTileA, J = j0 + threadIdx.x % kTileA;
+    const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    const int I = i0 + 4 * (wp >> 1) + (ln >> 3), J = j0 + 8 * (wp & 1) + (ln & 7);
     double ssu = 0, ssv = 0, ssh = 0;
     const bool f = a.use_forcing != 0;
     const PhysR<R>& p = a.p;

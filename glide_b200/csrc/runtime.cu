@@ -207,8 +207,10 @@ struct Solver : SolverBase {
     double* norms_host = nullptr;
     int* err_dev = nullptr;  // set by a kernel whose bounded wait gave up
     // TMA tensor maps of every (level, field), encoded on first use
-    std::vector<CUtensorMap> tmaps;
-    std::vector<unsigned char> tmap_done;
+    // slot per box height (kTmaHeights)
+    static constexpr int kTmaHeights[3] = {kBoxH, 22, 24};
+    std::vector<CUtensorMap> tmaps[3];
+    std::vector<unsigned char> tmap_done[3];
     bool use_tma = true;
     // one captured V-cycle per cycle kind (0 FAS, 1 adjoint, 2 mixed FAS,
     // 3 mixed adjoint, 4 Newton), each valid for the (version, dt, start) it
@@ -399,39 +401,42 @@ struct Solver : SolverBase {
     }
 
     // TMA staging needs a level at least one box wide and high
-    bool tma_level(int l) const { return use_tma && lv[l].nx >= kBoxW && lv[l].ny >= kBoxH; }
+    bool tma_level(int l, int bh = kBoxH) const { return use_tma && lv[l].nx >= kBoxW && lv[l].ny >= bh; }
 
-    const CUtensorMap& tmap(int l, int f) {
-        if (tmaps.empty()) {
-            tmaps.resize(size_t(n_levels) * F_COUNT);
-            tmap_done.assign(size_t(n_levels) * F_COUNT, 0);
+    const CUtensorMap& tmap(int l, int f, int bh = kBoxH) {
+        int w = 0;
+        while (w < 3 && kTmaHeights[w] != bh) ++w;
+        if (w == 3) fail(GLIDE_ERR_STATE, "no tensor-map slot for this box height");
+        if (tmaps[w].empty()) {
+            tmaps[w].resize(size_t(n_levels) * F_COUNT);
+            tmap_done[w].assign(size_t(n_levels) * F_COUNT, 0);
         }
         const size_t k = size_t(l) * F_COUNT + f;
-        if (!tmap_done[k]) {
+        if (!tmap_done[w][k]) {
             PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
             if (!enc) fail(GLIDE_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
             const Arr<R>& a = lv[l].a[f];
             const cuuint64_t dims[2] = {cuuint64_t(a.cols), cuuint64_t(a.rows)};
             const cuuint64_t strides[1] = {cuuint64_t(a.pitch) * sizeof(R)};
-            const cuuint32_t box[2] = {cuuint32_t(kBoxW), cuuint32_t(kBoxH)};
+            const cuuint32_t box[2] = {cuuint32_t(kBoxW), cuuint32_t(bh)};
             const cuuint32_t estr[2] = {1, 1};
-            const CUresult r = enc(&tmaps[k], sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
-                                                               : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+            const CUresult r = enc(&tmaps[w][k], sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                                    2, a.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             if (r != CUDA_SUCCESS) fail(GLIDE_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-            tmap_done[k] = 1;
+            tmap_done[w][k] = 1;
         }
-        return tmaps[k];
+        return tmaps[w][k];
     }
 
     template <int N>
-    BoxMaps<N> box_maps(int l, const int (&fields)[N]) {
+    BoxMaps<N> box_maps(int l, const int (&fields)[N], int bh = kBoxH) {
         BoxMaps<N> m;
-        m.use = tma_level(l) ? 1 : 0;
+        m.use = tma_level(l, bh) ? 1 : 0;
         if (m.use)
-            for (int q = 0; q < N; ++q) m.m[q] = tmap(l, fields[q]);
+            for (int q = 0; q < N; ++q) m.m[q] = tmap(l, fields[q], bh);
         return m;
     }
 
@@ -851,7 +856,9 @@ struct Solver : SolverBase {
         a.ny = v.ny; a.nx = v.nx; a.use_forcing = use_forcing;
         dim3 g((a.nx + kTileA - 1) / kTileA, (a.ny + kTileA - 1) / kTileA);
         if (L.tr) {
-            k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a);
+            const int fl[AdjTile<R>::NB] = {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_BED, GLIDE_BETA,
+                                            GLIDE_B, L.x[0], L.x[1]};
+            k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a, box_maps(l, fl, AdjTile<R>::BH));
             counted("vjp");
         } else {
             const int fl[JvpTile<R>::NB] = {GLIDE_U, GLIDE_V, L.x[0], L.x[1], GLIDE_H, GLIDE_PHI, GLIDE_BED,

@@ -21,8 +21,12 @@ namespace glide {
 
 constexpr int kBoxW = 24, kBoxH = 20, kBoxX = 4, kBoxY = 2;
 
+// A box of BH rows and kBoxW columns; BY is its first row's offset above the
+// tile (kernels with a two-cell halo stage a taller box).
+template <class R, int BH = kBoxH>
+using BoxT = R[BH][kBoxW];
 template <class R>
-using Box = R[kBoxH][kBoxW];
+using Box = BoxT<R, kBoxH>;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -80,30 +84,31 @@ struct BoxMaps {
 };
 
 // Scalar staging of one array into the box layout, indices clamped.
-template <class R>
-__device__ __forceinline__ void stage_box_scalar(Box<R>& t, const Arr<R>& a, int i0, int j0) {
-    for (int k = threadIdx.x; k < kBoxH * kBoxW; k += blockDim.x) {
+template <class R, int BH = kBoxH, int BY = kBoxY>
+__device__ __forceinline__ void stage_box_scalar(BoxT<R, BH>& t, const Arr<R>& a, int i0, int j0) {
+    for (int k = threadIdx.x; k < BH * kBoxW; k += blockDim.x) {
         const int r = k / kBoxW, c = k % kBoxW;
-        const int gi = clampi(i0 - kBoxY + r, 0, a.rows - 1), gj = clampi(j0 - kBoxX + c, 0, a.cols - 1);
+        const int gi = clampi(i0 - BY + r, 0, a.rows - 1), gj = clampi(j0 - kBoxX + c, 0, a.cols - 1);
         t[r][c] = ldg(&a.p[size_t(gi) * a.pitch + gj]);
     }
 }
 
 // True when the box of the tile at (i0, j0) reaches outside an array of
 // rows x cols elements.
+template <int BH = kBoxH, int BY = kBoxY>
 __device__ __forceinline__ bool box_on_edge(int i0, int j0, int rows, int cols) {
-    return i0 - kBoxY < 0 || j0 - kBoxX < 0 || i0 - kBoxY + kBoxH > rows || j0 - kBoxX + kBoxW > cols;
+    return i0 - BY < 0 || j0 - kBoxX < 0 || i0 - BY + BH > rows || j0 - kBoxX + kBoxW > cols;
 }
 
 // Replace the zero-filled elements outside a rows x cols array by the value
 // at the clamped index (which lies inside the box and was copied).
-template <class R>
-__device__ __forceinline__ void box_fixup(Box<R>& t, int rows, int cols, int i0, int j0) {
-    for (int k = threadIdx.x; k < kBoxH * kBoxW; k += blockDim.x) {
+template <class R, int BH = kBoxH, int BY = kBoxY>
+__device__ __forceinline__ void box_fixup(BoxT<R, BH>& t, int rows, int cols, int i0, int j0) {
+    for (int k = threadIdx.x; k < BH * kBoxW; k += blockDim.x) {
         const int r = k / kBoxW, c = k % kBoxW;
-        const int gi = i0 - kBoxY + r, gj = j0 - kBoxX + c;
+        const int gi = i0 - BY + r, gj = j0 - kBoxX + c;
         if (gi >= 0 && gi < rows && gj >= 0 && gj < cols) continue;
-        const int si = clampi(gi, 0, rows - 1) - (i0 - kBoxY), sj = clampi(gj, 0, cols - 1) - (j0 - kBoxX);
+        const int si = clampi(gi, 0, rows - 1) - (i0 - BY), sj = clampi(gj, 0, cols - 1) - (j0 - kBoxX);
         t[r][c] = t[si][sj];
     }
 }
@@ -112,13 +117,13 @@ __device__ __forceinline__ void box_fixup(Box<R>& t, int rows, int cols, int i0,
 // thread waits on the barrier, edge tiles are fixed up.  Returns false on
 // every thread of the block if the wait gave up (the error word is then set
 // and the block must return without touching the boxes).
-template <class R, int N>
-__device__ __forceinline__ bool stage_boxes(Box<R>* const (&dst)[N], const Arr<R> (&src)[N],
+template <class R, int N, int BH = kBoxH, int BY = kBoxY>
+__device__ __forceinline__ bool stage_boxes(BoxT<R, BH>* const (&dst)[N], const Arr<R> (&src)[N],
                                             const BoxMaps<N>& maps, int i0, int j0, unsigned long long* bar,
                                             int* err) {
     if (!maps.use) {
 #pragma unroll
-        for (int q = 0; q < N; ++q) stage_box_scalar(*dst[q], src[q], i0, j0);
+        for (int q = 0; q < N; ++q) stage_box_scalar<R, BH, BY>(*dst[q], src[q], i0, j0);
         __syncthreads();
         return true;
     }
@@ -128,9 +133,9 @@ __device__ __forceinline__ bool stage_boxes(Box<R>* const (&dst)[N], const Arr<R
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        mbar_expect_tx(bar, unsigned(N * sizeof(Box<R>)));
+        mbar_expect_tx(bar, unsigned(N * sizeof(BoxT<R, BH>)));
 #pragma unroll
-        for (int q = 0; q < N; ++q) tma_load_2d(dst[q], &maps.m[q], j0 - kBoxX, i0 - kBoxY, bar);
+        for (int q = 0; q < N; ++q) tma_load_2d(dst[q], &maps.m[q], j0 - kBoxX, i0 - BY, bar);
     }
     const bool ok = __syncthreads_and(mbar_wait(bar, 0));
     if (!ok) {
@@ -140,11 +145,12 @@ __device__ __forceinline__ bool stage_boxes(Box<R>* const (&dst)[N], const Arr<R
     }
     bool edge = false;
 #pragma unroll
-    for (int q = 0; q < N; ++q) edge |= box_on_edge(i0, j0, src[q].rows, src[q].cols);
+    for (int q = 0; q < N; ++q) edge |= box_on_edge<BH, BY>(i0, j0, src[q].rows, src[q].cols);
     if (edge) {
 #pragma unroll
         for (int q = 0; q < N; ++q)
-            if (box_on_edge(i0, j0, src[q].rows, src[q].cols)) box_fixup(*dst[q], src[q].rows, src[q].cols, i0, j0);
+            if (box_on_edge<BH, BY>(i0, j0, src[q].rows, src[q].cols))
+                box_fixup<R, BH, BY>(*dst[q], src[q].rows, src[q].cols, i0, j0);
         __syncthreads();
     }
     return true;
