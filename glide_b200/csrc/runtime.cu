@@ -500,6 +500,48 @@ struct Solver : SolverBase {
         counted("vanka_sweep");
     }
 
+    // Restrictions of several fields of level l in one launch; each job is
+    // (field, field receiving a copy of the coarse values or -1, cell kind
+    // or -1 for the field's own kind).
+    struct RJob { int f, copy_to, cell_kind; };
+    void restrict_batch(int l, const RJob* jobs, int n, cudaStream_t s) {
+        Level<R>& F = lv[l];
+        Level<R>& C = lv[l + 1];
+        RestrictJobs<R> b;
+        if (n > kMaxRestrictJobs) fail(GLIDE_ERR_STATE, "too many restrictions in one batch");
+        for (int q = 0; q < n; ++q) {
+            const Arr<R>& fa = F.a[jobs[q].f];
+            b.f[q] = fa;
+            b.c[q] = C.a[jobs[q].f];
+            b.copy[q] = jobs[q].copy_to >= 0 ? C.a[jobs[q].copy_to] : Arr<R>();
+            if (fa.cols == F.nx + 1) b.kind[q] = kFaceU;
+            else if (fa.rows == F.ny + 1) b.kind[q] = kFaceV;
+            else b.kind[q] = jobs[q].cell_kind >= 0 ? jobs[q].cell_kind
+                                                    : (jobs[q].f == GLIDE_MASK ? kCellMax : kCellAvg);
+        }
+        b.nyc = C.ny; b.nxc = C.nx;
+        dim3 g = pw_grid(C.ny + 1, C.nx + 1);
+        g.z = n;
+        k_restrict_batch<R><<<g, 256, 0, s>>>(b);
+        counted("restrict_batch");
+    }
+
+    // the u, v and H corrections of level l (fields x, snapshots w, kinds k)
+    void correct3(int l, const int (&x)[3], const int (&w)[3], const int (&kinds)[3], int mode, cudaStream_t s) {
+        Level<R>& F = lv[l];
+        Level<R>& C = lv[l + 1];
+        CorrectJobs<R> b;
+        for (int q = 0; q < 3; ++q) {
+            CorrectArgs<R>& a = b.j[q];
+            a.x = F.a[x[q]]; a.w = F.a[w[q]]; a.xc = C.a[x[q]]; a.wc = C.a[w[q]];
+            a.kind = kinds[q]; a.mode = mode; a.vquirk = quirks; a.nyf = F.ny; a.nxf = F.nx;
+        }
+        dim3 g = pw_grid(F.ny + 1, F.nx + 1);
+        g.z = 3;
+        k_correct_batch<R><<<g, 256, 0, s>>>(b);
+        counted("correct_batch");
+    }
+
     void correct(int l, int field, int wfield, int kind, int mode, cudaStream_t s) {
         Level<R>& F = lv[l];
         Level<R>& C = lv[l + 1];
@@ -530,23 +572,20 @@ struct Solver : SolverBase {
         Level<R>& n = lv[l + 1];
         restrict_arr(v.a[F_CHI], n.a[F_CHI], kCellMax, l, s);
         sweeps(l, dt, c.pre_steps, kGammaWPhi, fcal, fphi, nullptr, s);
-        restrict_field(GLIDE_U, l, s, n.a[F_W_U]);
-        restrict_field(GLIDE_V, l, s, n.a[F_W_V]);
-        restrict_field(GLIDE_H, l, s, n.a[F_W_H]);
-        restrict_field(GLIDE_H_PREV, l, s);
-        restrict_field(GLIDE_PHI, l, s);
-        restrict_field(GLIDE_MASK, l, s);
+        // the residual (phi frozen) reads level l only, so the state and the
+        // residual are restricted together after it, in one launch
         residual(l, dt, true, false, fcal, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, false, s);
-        restrict_field(GLIDE_R_U, l, s);
-        restrict_field(GLIDE_R_V, l, s);
-        restrict_field(GLIDE_R_H, l, s);
+        {
+            const RJob jobs[9] = {{GLIDE_U, F_W_U, -1}, {GLIDE_V, F_W_V, -1}, {GLIDE_H, F_W_H, -1},
+                                  {GLIDE_H_PREV, -1, -1}, {GLIDE_PHI, -1, -1}, {GLIDE_MASK, -1, -1},
+                                  {GLIDE_R_U, -1, -1}, {GLIDE_R_V, -1, -1}, {GLIDE_R_H, -1, -1}};
+            restrict_batch(l, jobs, 9, s);
+        }
         const Arr<R> sub[3] = {n.a[GLIDE_R_U], n.a[GLIDE_R_V], n.a[GLIDE_R_H]};
         residual(l + 1, dt, false, false, c.freeze_coarse_calving != 0, c.freeze_coarse_phi != 0, GLIDE_F_U,
                  GLIDE_F_V, GLIDE_F_H, sub, false, s);
         vcycle(l + 1, false, dt, s);
-        correct(l, GLIDE_U, F_W_U, kFaceU, 0, s);
-        correct(l, GLIDE_V, F_W_V, kFaceV, 0, s);
-        correct(l, GLIDE_H, F_W_H, kCellAvg, 0, s);
+        correct3(l, {GLIDE_U, GLIDE_V, GLIDE_H}, {F_W_U, F_W_V, F_W_H}, {kFaceU, kFaceV, kCellAvg}, 0, s);
         sweeps(l, dt, c.post_steps, kGammaWChi, fcal, fphi, nullptr, s);
         if (finest) sweeps(l, dt, c.finest_steps, kGammaArray, false, false, nullptr, s);
     }
@@ -950,21 +989,20 @@ struct Solver : SolverBase {
         }
         Level<R>& n = lv[l + 1];
         lin_sweeps(l, dt, c.pre_steps, L, s, false);
-        restrict_field(GLIDE_U, l, s);
-        restrict_field(GLIDE_V, l, s);
-        restrict_field(GLIDE_H, l, s);
-        restrict_field(GLIDE_H_PREV, l, s);
-        restrict_field(GLIDE_PHI, l, s);
-        restrict_field(GLIDE_MASK, l, s);
-        for (int q = 0; q < 3; ++q) restrict_field(L.x[q], l, s, n.a[L.w[q]]);
+        // the residual reads level l only: state, unknowns and residual are
+        // restricted together after it, in one launch
         lin_residual(l, dt, L, false, s);
-        for (int q = 0; q < 3; ++q) restrict_field(L.r[q], l, s);
+        {
+            const RJob jobs[12] = {{GLIDE_U, -1, -1}, {GLIDE_V, -1, -1}, {GLIDE_H, -1, -1},
+                                   {GLIDE_H_PREV, -1, -1}, {GLIDE_PHI, -1, -1}, {GLIDE_MASK, -1, -1},
+                                   {L.x[0], L.w[0], -1}, {L.x[1], L.w[1], -1}, {L.x[2], L.w[2], -1},
+                                   {L.r[0], -1, -1}, {L.r[1], -1, -1}, {L.r[2], -1, -1}};
+            restrict_batch(l, jobs, 12, s);
+        }
         // coarse right-hand side f_c = Op_c(x_c) - R r, in one pass
         lin_op(l + 1, dt, L, L.f, L.r, false, false, false, s);
         lin_vcycle(l + 1, false, dt, L, s);
-        correct(l, L.x[0], L.w[0], kFaceU, 1, s);
-        correct(l, L.x[1], L.w[1], kFaceV, 1, s);
-        correct(l, L.x[2], L.w[2], kCellMax, 1, s);
+        correct3(l, {L.x[0], L.x[1], L.x[2]}, {L.w[0], L.w[1], L.w[2]}, {kFaceU, kFaceV, kCellMax}, 1, s);
         lin_sweeps(l, dt, c.post_steps, L, s, false);
         if (finest) lin_sweeps(l, dt, c.finest_steps, L, s, false);
     }

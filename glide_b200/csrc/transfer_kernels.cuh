@@ -9,11 +9,12 @@ namespace glide {
 
 enum FieldKind { kFaceU = 0, kFaceV = 1, kCellAvg = 2, kCellMax = 3, kCellMin = 4 };
 
-// Restriction of one field (transfer.cu:2-139).  Coarse sizes (nyc, nxc).
-// Optional second output `copy` receives the same values (w_c = x_c).
+// Restriction of one field (transfer.cu:2-139) at coarse (J, I).  Coarse
+// sizes (nyc, nxc).  Optional second output `copy` receives the same values
+// (w_c = x_c).
 template <class R>
-__global__ void k_restrict(Arr<R> f, Arr<R> c, Arr<R> copy, int kind, int nyc, int nxc) {
-    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y;
+__device__ __forceinline__ void restrict_at(const Arr<R>& f, const Arr<R>& c, const Arr<R>& copy, int kind,
+                                            int nyc, int nxc, int J, int I) {
     R o;
     if (kind == kFaceU) {
         if (J >= nyc || I > nxc) return;
@@ -31,6 +32,26 @@ __global__ void k_restrict(Arr<R> f, Arr<R> c, Arr<R> copy, int kind, int nyc, i
     }
     c.at(J, I) = o;
     if (copy.p) copy.at(J, I) = o;
+}
+
+template <class R>
+__global__ void k_restrict(Arr<R> f, Arr<R> c, Arr<R> copy, int kind, int nyc, int nxc) {
+    restrict_at(f, c, copy, kind, nyc, nxc, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Several restrictions of one level in one launch: job blockIdx.z.
+constexpr int kMaxRestrictJobs = 12;
+template <class R>
+struct RestrictJobs {
+    Arr<R> f[kMaxRestrictJobs], c[kMaxRestrictJobs], copy[kMaxRestrictJobs];
+    int kind[kMaxRestrictJobs];
+    int nyc, nxc;
+};
+
+template <class R>
+__global__ void k_restrict_batch(RestrictJobs<R> b) {
+    const int q = blockIdx.z;
+    restrict_at(b.f[q], b.c[q], b.copy[q], b.kind[q], b.nyc, b.nxc, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Bilinear u-face value at fine (j, i) from coarse data addressed through
@@ -88,8 +109,7 @@ struct CorrectArgs {
 };
 
 template <class R>
-__global__ void k_correct(CorrectArgs<R> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+__device__ __forceinline__ void correct_at(const CorrectArgs<R>& a, int j, int i) {
     const int nyc = a.nyf / 2, nxc = a.nxf / 2;
     auto zc = [&](int J, int I) { return a.xc.at(J, I) - a.wc.at(J, I); };
     R pz;
@@ -123,6 +143,22 @@ __global__ void k_correct(CorrectArgs<R> a) {
     } else {
         x = x + pz;
     }
+}
+
+template <class R>
+__global__ void k_correct(CorrectArgs<R> a) {
+    correct_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The u, v and H corrections of one level in one launch: job blockIdx.z.
+template <class R>
+struct CorrectJobs {
+    CorrectArgs<R> j[3];
+};
+
+template <class R>
+__global__ void k_correct_batch(CorrectJobs<R> b) {
+    correct_at(b.j[blockIdx.z], blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Finest-level snapshot at the top of a V-cycle (multigrid.py:552-556):
