@@ -542,15 +542,6 @@ struct Solver : SolverBase {
         counted("correct_batch");
     }
 
-    void correct(int l, int field, int wfield, int kind, int mode, cudaStream_t s) {
-        Level<R>& F = lv[l];
-        Level<R>& C = lv[l + 1];
-        CorrectArgs<R> a;
-        a.x = F.a[field]; a.w = F.a[wfield]; a.xc = C.a[field]; a.wc = C.a[wfield];
-        a.kind = kind; a.mode = mode; a.vquirk = quirks; a.nyf = F.ny; a.nxf = F.nx;
-        k_correct<R><<<pw_grid(F.ny + 1, F.nx + 1), 256, 0, s>>>(a);
-        counted("correct");
-    }
 
     // ------------------------------------------------------ FASCD V-cycle
     // glide/multigrid.py:536-645

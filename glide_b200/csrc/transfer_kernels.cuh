@@ -145,11 +145,6 @@ __device__ __forceinline__ void correct_at(const CorrectArgs<R>& a, int j, int i
     }
 }
 
-template <class R>
-__global__ void k_correct(CorrectArgs<R> a) {
-    correct_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
-}
-
 // The u, v and H corrections of one level in one launch: job blockIdx.z.
 template <class R>
 struct CorrectJobs {
