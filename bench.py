@@ -80,6 +80,8 @@ def parse(argv=None):
     ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
     ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
+    ap.add_argument("--ens-adjoint", default="fast", choices=["fast", "reference"],
+                    help="ensemble adjoint: 4/4/0/50 cycles with omega 0.8, or the reference's 10/20/50/200")
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
     ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
@@ -640,6 +642,9 @@ def run_ensemble(a):
                                          absolute_tolerance=0.0, report_norms=False)
         m.adjoint_solver.fas_options.set(maximum_vcycles=max_cycles, relative_tolerance=a.rtol,
                                          absolute_tolerance=0.0, report_norms=False)
+        if a.ens_adjoint == "fast":
+            m.adjoint_solver.fas_options.set(pre_steps=4, post_steps=4, finest_steps=0, coarsest_steps=50)
+            m.adjoint_solver.vanka_options.set(omega=0.8)
         members.append(m)
     ens = Ensemble(members, workers=a.ens_workers)
     t0 = time.perf_counter()
@@ -668,7 +673,7 @@ def run_ensemble(a):
             "schedules": {str(k): v for k, v in chosen.items()}, "autotune_s": tune_s,
             "mean_forward_cycles": float(np.mean(fv)), "mean_adjoint_cycles": float(np.mean(bv)),
             "worst_forward_relative_residual": worst, "forward_solves_converged": converged,
-            "max_cycles": max_cycles, "workers": ens.workers,
+            "max_cycles": max_cycles, "workers": ens.workers, "adjoint": a.ens_adjoint,
             "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
 
 
