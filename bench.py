@@ -659,6 +659,7 @@ def run_ensemble(a):
     step(0.0)
     stream = torch.cuda.current_stream()
     stats = []
+    ens.retries = 0
     ms = event_time(lambda: stats.append(step(0.0)), a.ens_steps, stream)
     ens.close()
     cells = sum(sp.n * sp.n for sp in specs)
@@ -674,6 +675,7 @@ def run_ensemble(a):
             "mean_forward_cycles": float(np.mean(fv)), "mean_adjoint_cycles": float(np.mean(bv)),
             "worst_forward_relative_residual": worst, "forward_solves_converged": converged,
             "max_cycles": max_cycles, "workers": ens.workers, "adjoint": a.ens_adjoint,
+            "forward_retries": ens.retries,
             "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
 
 

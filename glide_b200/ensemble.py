@@ -75,6 +75,12 @@ CANDIDATES = {
 FALLBACK = "classic"
 
 
+def _converged(model: IceDynamics, st: dict) -> bool:
+    """The forward solve met its relative or absolute tolerance."""
+    c = model.forward_solver._fas_config
+    return st["final_norm"] <= max(c.relative_tolerance * st["initial_norm"], c.absolute_tolerance)
+
+
 def apply_schedule(model: IceDynamics, cfg: dict):
     h = model.mg.hierarchy
     h.set_reference_quirks(cfg["quirks"])
@@ -102,6 +108,7 @@ class Ensemble:
         self._pool = ThreadPoolExecutor(max_workers=self.workers)
         self._streams = [None] * self.workers
         self.schedules: dict[int, str] = {}
+        self.retries = 0  # forward solves repeated under another schedule
 
     def close(self):
         self._pool.shutdown(wait=True)
@@ -131,8 +138,48 @@ class Ensemble:
             caller.wait_event(e)
         return res
 
-    def forward(self, t: float, dt: float, update_geometry: bool = True):
-        return self._run(lambda k, m: m.forward(t, dt, update_geometry=update_geometry))
+    def forward(self, t: float, dt: float, update_geometry: bool = True, retry: bool = True):
+        """One forward step of every member.  With `retry`, a member whose
+        solve stops short of its tolerance (cycle cap reached) is solved again
+        from its current iterate under the other candidate schedules in turn,
+        each aiming at the first solve's target (relative tolerance times its
+        initial residual, or the absolute tolerance); the first that gets
+        there becomes that member's schedule.  The returned statistics span
+        all attempts.  The geometry update and post-forward hooks run once,
+        after the last solve."""
+        def one(k, m):
+            st = m.forward_solver.solve(dt, start_level=m.top_level, report_norms=False)
+            if retry and not _converged(m, st):
+                c = m.forward_solver._fas_config
+                rtol, atol = c.relative_tolerance, c.absolute_tolerance
+                target = max(rtol * st["initial_norm"], atol)
+                first, cycles = st, st["vcycles"]
+                m.forward_solver.fas_options.set(relative_tolerance=0.0, absolute_tolerance=target)
+                tried = {self.schedules.get(k)}
+                try:
+                    for name in list(CANDIDATES) + [FALLBACK]:
+                        if name in tried:
+                            continue
+                        tried.add(name)
+                        apply_schedule(m, CANDIDATES[name])
+                        st = m.forward_solver.solve(dt, start_level=m.top_level, report_norms=False)
+                        cycles += st["vcycles"]
+                        self.retries += 1
+                        if st["final_norm"] <= target:
+                            self.schedules[k] = name
+                            break
+                finally:
+                    m.forward_solver.fas_options.set(relative_tolerance=rtol, absolute_tolerance=atol)
+                    if self.schedules.get(k) in CANDIDATES:
+                        apply_schedule(m, CANDIDATES[self.schedules[k]])
+                st = dict(st, initial_norm=first["initial_norm"], vcycles=cycles)
+            if update_geometry:
+                lev = m.mg.levels[m.top_level]
+                lev.state.H_prev.data.copy_(lev.state.H.data)
+            for hook in m._post_forward_hooks:
+                hook(t + dt)
+            return st
+        return self._run(one)
 
     def backward(self, t: float, dt: float, dJ):
         """dJ(k, model) -> (dJdu, dJdv, dJdH) per member; returns the adjoint stats."""

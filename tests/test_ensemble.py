@@ -56,7 +56,7 @@ def test_concurrent_members_match_solo_runs():
         if concurrent:
             ens = Ensemble(members, workers=3)
             for step in range(2):
-                ens.forward(step * 10.0, 10.0)
+                ens.forward(step * 10.0, 10.0, retry=False)
             ens.backward(20.0, 10.0, dJ)
             torch.cuda.synchronize()
             ens.close()
@@ -74,3 +74,26 @@ def test_concurrent_members_match_solo_runs():
     for ma, mb in zip(a, b):
         for k in ma:
             np.testing.assert_array_equal(ma[k], mb[k], err_msg=k)
+
+
+@pytest.mark.gpu
+def test_forward_retries_other_schedules_when_a_solve_stops_short():
+    """A member whose solve stops at its cycle cap short of the tolerance is
+    solved again under each other candidate schedule until one converges;
+    with a one-cycle cap none does, so every other candidate is tried once
+    and the member keeps its schedule."""
+    from glide_b200.ensemble import CANDIDATES, FALLBACK, Ensemble, apply_schedule
+    m = _member(64, seed=3)
+    m.forward_solver.fas_options.set(maximum_vcycles=1, relative_tolerance=1e-12, absolute_tolerance=0.0)
+    ens = Ensemble([m], workers=1)
+    apply_schedule(m, CANDIDATES["fascd"])
+    ens.schedules[0] = "fascd"
+    st = ens.forward(0.0, 10.0)[0]
+    torch.cuda.synchronize()
+    ens.close()
+    others = {n for n in list(CANDIDATES) + [FALLBACK] if n != "fascd"}
+    assert ens.retries == len(others)
+    assert ens.schedules[0] == "fascd"
+    assert np.isfinite(st["final_norm"])
+    H = m.mg.hierarchy.get("H", 0)
+    assert bool(torch.equal(m.mg.hierarchy.get("H_prev", 0), H))
