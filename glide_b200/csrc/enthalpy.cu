@@ -119,8 +119,8 @@ struct Handle {
     int nblocks = 0;
     glide_enthalpy_config cfg;
     glide_enthalpy_inputs in;
-    int point_blocks = 5;   // resident blocks per SM of the residual / layer kernels (4, 5, 6)
-    int column_blocks = 6;  // of the column kernel (2 to 6)
+    int point_blocks = 4;   // resident blocks per SM of the residual / layer kernels (3 to 6)
+    int column_blocks = 4;  // of the column kernel (2 to 6)
 
     Handle(int ny_, int nx_, int nz_, double dx_) : ny(ny_), nx(nx_), nz(nz_), dx(dx_) {
         plane = size_t(ny) * nx;
@@ -206,7 +206,8 @@ struct Handle {
     dim3 col_grid() const { return dim3(unsigned(nblocks)); }
 
     void residual(const EnthArgs& a, int use_forcing, cudaStream_t s) {
-        if (point_blocks == 4) k_enth_residual<4><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
+        if (point_blocks == 3) k_enth_residual<3><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
+        else if (point_blocks == 4) k_enth_residual<4><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
         else if (point_blocks == 6) k_enth_residual<6><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
         else k_enth_residual<5><<<col_grid(), kColThreads, 0, s>>>(a, f[GLIDE_ENTH_R_E], use_forcing, partial);
         check_launch("enthalpy residual");
@@ -220,7 +221,8 @@ struct Handle {
         check_launch("enthalpy column smooth");
     }
     void layer(const EnthArgs& a, double* out, int mode, cudaStream_t s) {
-        if (point_blocks == 4) k_enth_layer<4><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        if (point_blocks == 3) k_enth_layer<3><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
+        else if (point_blocks == 4) k_enth_layer<4><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
         else if (point_blocks == 6) k_enth_layer<6><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
         else k_enth_layer<5><<<col_grid(), kColThreads, 0, s>>>(a, out, mode);
         check_launch("enthalpy layer smooth");
@@ -311,7 +313,7 @@ int glide_enthalpy_set_tuning(glide_enthalpy_handle h, int key, int value) {
     return guarded([&] {
         Handle* e = H(h);
         if (key == GLIDE_ENTH_TUNE_POINT_BLOCKS) {
-            if (value < 4 || value > 6) fail(GLIDE_ERR_ARG, "point blocks per SM must be 4, 5 or 6");
+            if (value < 3 || value > 6) fail(GLIDE_ERR_ARG, "point blocks per SM must lie in [3, 6]");
             e->point_blocks = value;
         } else if (key == GLIDE_ENTH_TUNE_COLUMN_BLOCKS) {
             if (value < 2 || value > 6) fail(GLIDE_ERR_ARG, "column blocks per SM must lie in [2, 6]");

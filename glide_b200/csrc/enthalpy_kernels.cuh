@@ -161,18 +161,30 @@ __device__ __forceinline__ FaceQ face_q(const EnthArgs& a, const ColumnCtx& x, i
     return q;
 }
 
-// Conservative horizontal advection at (i, j, k) with centre value Ec; the
-// neighbours come from the state array (enthalpy.cu:667-759).  sq =
-// sqrt(1 + lf_c), dx_inv = 1 / dx.
 struct HAdv { double res, diag; };
-__device__ __forceinline__ HAdv horiz(const EnthArgs& a, const ColumnCtx& x, int k, double Ec, const FaceQ& q,
-                                      double sq, double dx_inv) {
-    const size_t plane = size_t(a.ny) * a.nx;
-    const double* Ek = a.E + size_t(k) * plane;
-    Flux fl = x.j > 0 ? face_flux(q.l, Ek[x.c - 1], Ec, sq) : face_flux(0.0, Ec, Ec, sq);
-    Flux fr = x.j < a.nx - 1 ? face_flux(q.r, Ec, Ek[x.c + 1], sq) : face_flux(0.0, Ec, Ec, sq);
-    Flux ft = x.i > 0 ? face_flux(q.t, Ec, Ek[x.c - a.nx], sq) : face_flux(0.0, Ec, Ec, sq);
-    Flux fb = x.i < a.ny - 1 ? face_flux(q.b, Ek[x.c + a.nx], Ec, sq) : face_flux(0.0, Ec, Ec, sq);
+
+// The four horizontal neighbours of node (k, i, j) in the state array; a
+// neighbour across the domain edge reads as 0 and is not used.
+struct Nbr { double l, r, t, b; };
+__device__ __forceinline__ Nbr neighbours(const EnthArgs& a, const ColumnCtx& x, int k) {
+    const double* Ek = a.E + size_t(k) * (size_t(a.ny) * a.nx);
+    Nbr n{0.0, 0.0, 0.0, 0.0};
+    if (x.j > 0) n.l = Ek[x.c - 1];
+    if (x.j < a.nx - 1) n.r = Ek[x.c + 1];
+    if (x.i > 0) n.t = Ek[x.c - a.nx];
+    if (x.i < a.ny - 1) n.b = Ek[x.c + a.nx];
+    return n;
+}
+
+// Conservative horizontal advection at (i, j, k) with centre value Ec and
+// the neighbours n read from the state array (enthalpy.cu:667-759).  sq =
+// sqrt(1 + lf_c), dx_inv = 1 / dx.
+__device__ __forceinline__ HAdv horiz_vals(const EnthArgs& a, const ColumnCtx& x, double Ec, const Nbr& n,
+                                           const FaceQ& q, double sq, double dx_inv) {
+    Flux fl = x.j > 0 ? face_flux(q.l, n.l, Ec, sq) : face_flux(0.0, Ec, Ec, sq);
+    Flux fr = x.j < a.nx - 1 ? face_flux(q.r, Ec, n.r, sq) : face_flux(0.0, Ec, Ec, sq);
+    Flux ft = x.i > 0 ? face_flux(q.t, Ec, n.t, sq) : face_flux(0.0, Ec, Ec, sq);
+    Flux fb = x.i < a.ny - 1 ? face_flux(q.b, n.b, Ec, sq) : face_flux(0.0, Ec, Ec, sq);
     return {kRhoI * ((fr.res - fl.res) + (ft.res - fb.res)) * dx_inv,
             kRhoI * ((fr.dl - fl.dr) + (ft.dl - fb.dr)) * dx_inv};
 }
@@ -188,9 +200,6 @@ struct HCtx {
         sq = sqrt(1.0 + a.lf_c);
         dx_inv = 1.0 / a.dx;
         q = flat ? face_q(a, x, 0) : FaceQ{0.0, 0.0, 0.0, 0.0};
-    }
-    __device__ HAdv at(const EnthArgs& a, const ColumnCtx& x, int k, double Ec) const {
-        return horiz(a, x, k, Ec, flat ? q : face_q(a, x, k), sq, dx_inv);
     }
 };
 
@@ -247,6 +256,27 @@ __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, 
 
 __device__ __forceinline__ bool stopped(const int* done) { return done && *(volatile const int*)done; }
 
+// Inputs of row k of a column that do not depend on the column iterate:
+// E_prev, f_E (when used), omega of node k + 1 and the frozen horizontal
+// neighbours.  The kernels below load row k + 1's while row k is computed,
+// so the walk up the column does not wait on memory at every row.
+struct RowIn { double ep, fe, om_p; Nbr nb; };
+__device__ __forceinline__ RowIn row_inputs(const EnthArgs& a, const ColumnCtx& x, int k, bool hadv,
+                                            bool forcing) {
+    const size_t plane = size_t(a.ny) * a.nx;
+    const size_t n = size_t(k) * plane + x.c;
+    RowIn r{a.E_prev[n], forcing ? a.f_E[n] : 0.0, a.omega[n + plane], Nbr{0.0, 0.0, 0.0, 0.0}};
+    if (hadv) r.nb = neighbours(a, x, k);
+    return r;
+}
+__device__ __forceinline__ RowIn no_row() { return RowIn{0.0, 0.0, 0.0, Nbr{0.0, 0.0, 0.0, 0.0}}; }
+
+// Horizontal advection of row k from its loaded neighbours.
+__device__ __forceinline__ HAdv row_horiz(const EnthArgs& a, const ColumnCtx& x, const HCtx& hc, int k, double Ec,
+                                          const Nbr& nb) {
+    return horiz_vals(a, x, Ec, nb, hc.flat ? hc.q : face_q(a, x, k), hc.sq, hc.dx_inv);
+}
+
 // ------------------------------------------------------------- residual
 // enthalpy.cu:784-893.  out (layer-major) = F(E) - f_E, or F(E) without
 // forcing; partial[block] = max |out| over the block's nodes.
@@ -274,25 +304,29 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_residual(EnthArgs a,
             double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
             double K_lo = 0.0;
             double om_m = 0.0, om_k = om[0];
+            const bool hadv = (a.flags & kTermHorizAdv) != 0;
+            RowIn in = row_inputs(a, x, 0, hadv, use_forcing);
             for (int k = 0; k < nz - 1; ++k) {
-                const double om_p = om[size_t(k + 1) * plane];
+                const RowIn in_n = k + 1 < nz - 1 ? row_inputs(a, x, k + 1, hadv, use_forcing) : no_row();
+                const double E_n = (k + 2 < nz) ? E[size_t(k + 2) * plane] : 0.0;
+                const double om_p = in.om_p;
                 const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
-                double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[k * plane + x.c]) * inv_dt;
-                if (a.flags & kTermHorizAdv) r += hc.at(a, x, k, Ek).res;
+                double r = kRhoI * (x.h * Ek - x.h_prev * in.ep) * inv_dt;
+                if (hadv) r += row_horiz(a, x, hc, k, Ek, in.nb).res;
                 Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
                 r += vt.adv;
                 r += vt.dif;
                 r += vt.drn;
-                if (use_forcing) r = r - a.f_E[k * plane + x.c];
+                if (use_forcing) r = r - in.fe;
                 out[k * plane + x.c] = r;
                 mx = fmax(mx, fabs(r));
                 // slide the window
-                Ekm1 = Ek; Ek = Ekp1;
-                Ekp1 = (k + 2 < nz) ? E[size_t(k + 2) * plane] : 0.0;
+                Ekm1 = Ek; Ek = Ekp1; Ekp1 = E_n;
                 Epk = Epp;
                 Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
                 K_lo = K_up;
                 om_m = om_k; om_k = om_p;
+                in = in_n;
             }
             out[size_t(nz - 1) * plane + x.c] = 0.0;
         }
@@ -343,19 +377,24 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_column(EnthArgs a, d
     const double inv_dt = 1.0 / a.dt;
     const double* om = a.omega + x.c;
     const double bt = kRhoI * x.h * inv_dt;  // time-term diagonal
+    const bool hadv = (a.flags & kTermHorizAdv) != 0;
     for (int it = 0; it < a.n_newton; ++it) {
         double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
         double K_lo = 0.0, om_m = 0.0, om_k = om[0];
         double c_prev = 0.0, d_prev = 0.0;
+        // the iterate window of row k and the inputs of row k + 1 are
+        // loaded before row k is assembled
+        double Ekm1 = 0.0, Ek = El[0], Ekp1 = El[1];
+        RowIn in = row_inputs(a, x, 0, hadv, true);
         for (int k = 0; k < nz - 1; ++k) {
-            const double Ek = El[k], Ekp1 = El[k + 1], Ekm1 = k > 0 ? El[k - 1] : 0.0;
-            const double om_p = om[size_t(k + 1) * plane];
+            const RowIn in_n = k + 1 < nz - 1 ? row_inputs(a, x, k + 1, hadv, true) : no_row();
+            const double E_n = k + 2 < nz ? El[k + 2] : 0.0;
+            const double om_p = in.om_p;
             const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
-            const size_t n = size_t(k) * plane + x.c;
-            double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[n]) * inv_dt - a.f_E[n];
+            double r = kRhoI * (x.h * Ek - x.h_prev * in.ep) * inv_dt - in.fe;
             double hd = 0.0;
-            if (a.flags & kTermHorizAdv) {
-                HAdv ha = hc.at(a, x, k, Ek);
+            if (hadv) {
+                HAdv ha = row_horiz(a, x, hc, k, Ek, in.nb);
                 r += ha.res;
                 hd = ha.diag;
             }
@@ -375,10 +414,13 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_column(EnthArgs a, d
             Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
             K_lo = K_up;
             om_m = om_k; om_k = om_p;
+            Ekm1 = Ek; Ek = Ekp1; Ekp1 = E_n;
+            in = in_n;
         }
         // surface Dirichlet row: E = E_surface (a = c = 0, b = 1)
         double xk = -(El[nz - 1] - Es);
         El[nz - 1] += a.relaxation * xk;
+#pragma unroll 4
         for (int k = nz - 2; k >= 0; --k) {
             xk = dp[k] - cp[k] * xk;
             El[k] += a.relaxation * xk;
@@ -415,14 +457,18 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_layer(EnthArgs a, do
     double Ekm1 = 0.0, Ek = E[0], Ekp1 = E[plane];
     double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
     double K_lo = 0.0, om_m = 0.0, om_k = om[0];
+    const bool hadv = (a.flags & kTermHorizAdv) != 0;
+    RowIn in = row_inputs(a, x, 0, hadv, true);
     for (int k = 0; k < nz - 1; ++k) {
-        const double om_p = om[size_t(k + 1) * plane];
+        const RowIn in_n = k + 1 < nz - 1 ? row_inputs(a, x, k + 1, hadv, true) : no_row();
+        const double E_n = (k + 2 < nz) ? E[size_t(k + 2) * plane] : 0.0;
+        const double om_p = in.om_p;
         const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
         const size_t n = size_t(k) * plane + x.c;
-        double r = kRhoI * (x.h * Ek - x.h_prev * a.E_prev[n]) * inv_dt - a.f_E[n];
+        double r = kRhoI * (x.h * Ek - x.h_prev * in.ep) * inv_dt - in.fe;
         double diag = kRhoI * x.h * inv_dt;
-        if (a.flags & kTermHorizAdv) {
-            HAdv ha = hc.at(a, x, k, Ek);
+        if (hadv) {
+            HAdv ha = row_horiz(a, x, hc, k, Ek, in.nb);
             r += ha.res;
             diag += ha.diag;
         }
@@ -433,12 +479,12 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_layer(EnthArgs a, do
         diag += vt.b_dif + vt.b_adv + vt.b_drn;
         const double d = (fabs(diag) > 1e-30) ? (-r / diag) : 0.0;
         out[n] = mode ? Ek + a.omega_relax * d : d;
-        Ekm1 = Ek; Ek = Ekp1;
-        Ekp1 = (k + 2 < nz) ? E[size_t(k + 2) * plane] : 0.0;
+        Ekm1 = Ek; Ek = Ekp1; Ekp1 = E_n;
         Epk = Epp;
         Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
         K_lo = K_up;
         om_m = om_k; om_k = om_p;
+        in = in_n;
     }
     const size_t top = size_t(nz - 1) * plane + x.c;
     out[top] = mode ? E[size_t(nz - 1) * plane] : 0.0;
