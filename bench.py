@@ -722,7 +722,7 @@ def thermal_leg(a, h, f, stream, dev, world):
     st = getattr(ops, "last_stats", None)
     return {"ms_per_step": t_ms, "steps_per_s": world * 1000.0 / t_ms, "nz": a.nz, "columns": ncol,
             "sweeps_last_step": int(st.iterations) if st is not None else None,
-            "what": "ThermalModel.step at 2048^2 x nz (binary64), coupled to the solved SSA state",
+            "what": f"ThermalModel.step at {a.size}^2 x {a.nz} (binary64)",
             "kernels": kern}
 
 

@@ -119,7 +119,7 @@ struct Handle {
     int nblocks = 0;
     glide_enthalpy_config cfg;
     glide_enthalpy_inputs in;
-    int point_blocks = 4;   // resident blocks per SM of the residual / layer kernels (3 to 6)
+    int point_blocks = 3;   // resident blocks per SM of the residual / layer kernels (3 to 6)
     int column_blocks = 4;  // of the column kernel (2 to 6)
 
     Handle(int ny_, int nx_, int nz_, double dx_) : ny(ny_), nx(nx_), nz(nz_), dx(dx_) {

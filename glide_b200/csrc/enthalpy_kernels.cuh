@@ -63,15 +63,20 @@ __device__ __forceinline__ double e_pmp(double sigma, double H) {
     return kCI * (T_pmp - kTRef) / kEScale;
 }
 
+// diffusivity of the switch value s (enthalpy.cu:60-66)
+__device__ __forceinline__ double k_of_switch(double s) { return kKCold * (1.0 - s + kKTF * s); }
+
 // Values of the smoothed switches where their argument is clamped at -20 or
-// +20 (ice colder or warmer than ~2 K / ~2 kJ kg^-1 from the melting point).
-// They are evaluated once per thread from the same expressions, so the
-// clamped branches below return exactly what the general path would.
+// +20 (ice colder or warmer than ~2 K / ~2 kJ kg^-1 from the melting point),
+// and the diffusivity there.  They are evaluated once per thread from the
+// same expressions, so the clamped branches below return exactly what the
+// general path would.
 struct Clamped {
     double s_lo, s_hi, sp_lo;
+    double k_lo, k_hi;
     __device__ Clamped()
         : s_lo(1.0 / (1.0 + exp(20.0))), s_hi(1.0 / (1.0 + exp(-20.0))),
-          sp_lo(log(1.0 + exp(-20.0)) / kSharp) {}
+          sp_lo(log(1.0 + exp(-20.0)) / kSharp), k_lo(k_of_switch(s_lo)), k_hi(k_of_switch(s_hi)) {}
 };
 
 // logistic switch 1 / (1 + exp(-z)) with z clamped to [-20, 20]
@@ -84,21 +89,32 @@ __device__ __forceinline__ double switch_of(double z, const Clamped& c) {
 // enthalpy.cu:60-66
 __device__ __forceinline__ double k_diff(double E, double Ep, const Clamped& c) {
     double z = (E - Ep) * kEScale * kSharp;
-    double s = switch_of(z, c);
-    return kKCold * (1.0 - s + kKTF * s);
+    if (z <= -20.0) return c.k_lo;
+    if (z >= 20.0) return c.k_hi;
+    return k_of_switch(1.0 / (1.0 + exp(-z)));
 }
 
-// drainage residual and derivative (enthalpy.cu:71-91, :598-640)
+// drainage residual and derivative from the softplus sp and switch s
+// (enthalpy.cu:71-91, :598-640)
 struct Drain { double res, d; };
-__device__ __forceinline__ Drain drainage(double Ek, double Ep, double drain, double h, const Clamped& c) {
+__device__ __forceinline__ Drain drain_terms(double sp, double s, double drain, double h) {
+    return {h * kRhoW * kL * (drain * (sp / kL)) / kEScale, h * kRhoW * kL * drain * (s / kL)};
+}
+
+// `cold` is drain_terms at both clamped-low values for this column, which
+// is what the general path returns when both arguments are at or below -20.
+__device__ __forceinline__ Drain drainage(double Ek, double Ep, double drain, double h, const Clamped& c,
+                                          const Drain& cold) {
     double x = (Ek - Ep) * kEScale;
     double ax = kSharp * x;
+    double z = kSharp * (Ek - Ep) * kEScale;
+    if (ax <= -20.0 && z <= -20.0) return cold;
     double sp;
     if (ax <= -20.0) sp = c.sp_lo;
     else if (ax > 10.0) sp = x;
     else sp = log(1.0 + exp(ax)) / kSharp;
-    double s = switch_of(kSharp * (Ek - Ep) * kEScale, c);
-    return {h * kRhoW * kL * (drain * (sp / kL)) / kEScale, h * kRhoW * kL * drain * (s / kL)};
+    double s = switch_of(z, c);
+    return drain_terms(sp, s, drain, h);
 }
 
 // Lax-Friedrichs enthalpy flux through a face with mass flux q; sq = sqrt(1 + lf_c)
@@ -210,9 +226,20 @@ struct HCtx {
 // arguments).
 struct Vert { double adv, dif, drn; double a, b_dif, b_adv, b_drn, c; };
 
+// Per-column constants of the vertical terms: 1 / dsig, 1 / dsig^2 and the
+// drainage of ice below both switches' clamp (the same expressions the
+// per-row code evaluated).
+struct ColTerms {
+    double di, d2;
+    Drain cold;
+    __device__ ColTerms(const EnthArgs& a, const Clamped& c, double h, double dsig)
+        : di(1.0 / dsig), d2(1.0 / (dsig * dsig)), cold(drain_terms(c.sp_lo, c.s_lo, a.drain, h)) {}
+};
+
 __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, double Ek, double Ekp1,
                                          double Epk, double K_lo, double K_up, double om_m, double om_k,
-                                         double om_p, double h, double h_inv, double dsig, const Clamped& cl) {
+                                         double om_p, double h, double h_inv, double dsig, const Clamped& cl,
+                                         const ColTerms& ct) {
     Vert r{0, 0, 0, 0, 0, 0, 0, 0};
     if (k == 0) {
         const double dsh = 0.5 * dsig, dsh_inv = 1.0 / dsh;
@@ -229,7 +256,7 @@ __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, 
         r.b_dif = coeff;
         r.c += -coeff;
     } else {
-        const double di = 1.0 / dsig;
+        const double di = ct.di;
         if (a.flags & kTermSigmaDot) {
             double wu = 0.5 * (om_k + om_p), wl = 0.5 * (om_m + om_k);
             double up = fmax(wu, 0.0), un = fmin(wu, 0.0), lp = fmax(wl, 0.0), ln = fmin(wl, 0.0);
@@ -239,7 +266,7 @@ __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, 
             r.c = kRhoI * un * di;
             r.b_adv = kRhoI * (up - ln) * di;
         }
-        const double d2 = 1.0 / (dsig * dsig);
+        const double d2 = ct.d2;
         r.dif = -h_inv * d2 * (K_up * (Ekp1 - Ek) - K_lo * (Ek - Ekm1));
         double dl = h_inv * d2 * K_lo, du = h_inv * d2 * K_up;
         r.a += -dl;
@@ -247,7 +274,7 @@ __device__ __forceinline__ Vert vertical(const EnthArgs& a, int k, double Ekm1, 
         r.b_dif = dl + du;
     }
     if (a.flags & kTermDrainage) {
-        Drain d = drainage(Ek, Epk, a.drain, h, cl);
+        Drain d = drainage(Ek, Epk, a.drain, h, cl, ct.cold);
         r.drn = d.res;
         r.b_drn = d.d;
     }
@@ -298,6 +325,7 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_residual(EnthArgs a,
             const Clamped cl;
             const HCtx hc(a, x);
             const double dsig = 1.0 / double(nz - 1), inv_dt = 1.0 / a.dt;
+            const ColTerms ct(a, cl, x.h, dsig);
             const double* E = a.E + x.c;
             const double* om = a.omega + x.c;
             double Ekm1 = 0.0, Ek = E[0], Ekp1 = E[plane];
@@ -313,7 +341,7 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_residual(EnthArgs a,
                 const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
                 double r = kRhoI * (x.h * Ek - x.h_prev * in.ep) * inv_dt;
                 if (hadv) r += row_horiz(a, x, hc, k, Ek, in.nb).res;
-                Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
+                Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl, ct);
                 r += vt.adv;
                 r += vt.dif;
                 r += vt.drn;
@@ -374,6 +402,7 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_column(EnthArgs a, d
     for (int k = 0; k < nz; ++k) El[k] = E[size_t(k) * plane];
     const Clamped cl;
     const HCtx hc(a, x);
+    const ColTerms ct(a, cl, x.h, dsig);
     const double inv_dt = 1.0 / a.dt;
     const double* om = a.omega + x.c;
     const double bt = kRhoI * x.h * inv_dt;  // time-term diagonal
@@ -398,7 +427,7 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_column(EnthArgs a, d
                 r += ha.res;
                 hd = ha.diag;
             }
-            Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
+            Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl, ct);
             r += vt.adv;
             r += vt.dif;
             r += vt.drn;
@@ -453,6 +482,7 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_layer(EnthArgs a, do
     const Clamped cl;
     const HCtx hc(a, x);
     const double dsig = 1.0 / double(nz - 1), inv_dt = 1.0 / a.dt;
+    const ColTerms ct(a, cl, x.h, dsig);
     const double* om = a.omega + x.c;
     double Ekm1 = 0.0, Ek = E[0], Ekp1 = E[plane];
     double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
@@ -472,7 +502,7 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_layer(EnthArgs a, do
             r += ha.res;
             diag += ha.diag;
         }
-        Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl);
+        Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl, ct);
         r += vt.adv;
         r += vt.dif;
         r += vt.drn;

@@ -113,7 +113,7 @@ int glide_enthalpy_set_config(glide_enthalpy_handle h, const glide_enthalpy_conf
 int glide_enthalpy_get_config(glide_enthalpy_handle h, glide_enthalpy_config* c);
 int glide_enthalpy_set_inputs(glide_enthalpy_handle h, const glide_enthalpy_inputs* in);
 /* Launch shapes, no counterpart in the reference: resident blocks per SM the
- * residual / layer kernels (3 to 6; default 4) and the column kernel (2 to
+ * residual / layer kernels (3 to 6; default 3) and the column kernel (2 to
  * 6; default 4) are compiled for, and whether the column kernel prefers the
  * largest L1 (value 1) for its per-column Thomas arrays. */
 #define GLIDE_ENTH_TUNE_POINT_BLOCKS 1
