@@ -85,7 +85,7 @@ def parse(argv=None):
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
     ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
-    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels", "thermal", "ensemble"],
+    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels", "thermal", "ensemble", "vti"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -679,6 +679,98 @@ def run_ensemble(a):
             "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
 
 
+def run_vti(a):
+    """Profiling case: VTI snapshots through glide_b200.io of the dome at
+    --size (binary64 H, B, beta, bed and the u / v faces averaged to a cell
+    vector U: the SSA state a run writes each output step) and of a layer-
+    major binary64 enthalpy volume of --nz levels; beside them the
+    reference's writer path (host copies of the binary64 arrays, then the
+    NumPy cast / flip / reorder / file write, restated in oracle/vti_oracle.py)
+    on the host cores."""
+    import shutil
+    import tempfile
+    import torch
+    from cases import dome
+    from glide_b200 import io as gio
+    from glide_b200.grid import Grid
+    from glide_b200.hierarchy import Hierarchy
+    from oracle import vti_oracle as vo
+    n, nz = a.size, a.nz
+    f = dome(n, a.dx, a.radius, seed=0)
+    h = Hierarchy(n, n, a.dx, 1, precision="fp64")
+    load_dome(h, f)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    h.set("u", 0, 50.0 * torch.randn((n, n + 1), dtype=torch.float64, device="cuda", generator=gen))
+    h.set("v", 0, 50.0 * torch.randn((n + 1, n), dtype=torch.float64, device="cuda", generator=gen))
+    g = Grid(hierarchy=h, level=0)
+    fields = {"H": g.state.H, "U": [g.state.u, g.state.v], "B": g.rheology.B, "beta": g.sliding.beta,
+              "bed": g.geometry.bed}
+    E = torch.randn((nz, n, n), dtype=torch.float64, device="cuda", generator=gen)
+    volume = {"E": E.permute(1, 2, 0)}
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = measured_peaks()
+    tmp = Path(tempfile.mkdtemp(prefix="glide_vti_"))
+    out = {"mode": "vti", "size": n, "nz": nz}
+    try:
+        for tag, data, dz, read_b in (("snapshot_2d", fields, None, 6 * 8), ("volume_3d", volume, 1.0 / (nz - 1), 8)):
+            snap = gio._Snapshot(data, a.dx, a.dx, dz, (0.0, 0.0), 0.0, True)
+            pts = n * n * (nz if dz is not None else 1)
+            dev = torch.empty(snap.nbytes, dtype=torch.uint8, device="cuda")
+            host = torch.empty(snap.nbytes, dtype=torch.uint8, pin_memory=True)
+            snap.pack(dev, stream)
+            pack_ms = event_time(lambda: snap.pack(dev, stream), 10, stream)
+            alg = pts * read_b + snap.nbytes
+            d2h_ms = event_time(lambda: host.copy_(dev, non_blocking=True), 3, stream)
+            path = tmp / f"{tag}.vti"
+            gio.write_vti(path, data, a.dx, dz=dz, time_value=0.0)
+            reps = 3 if dz is None else 1
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                gio.write_vti(path, data, a.dx, dz=dz, time_value=0.0)
+            wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+            path.unlink()
+            r = {"file_bytes": snap.nbytes + len(snap.header) + len(gio._APPENDED_OPEN) + len(gio._APPENDED_CLOSE),
+                 "pack_ms": pack_ms,
+                 "pack_algorithmic_bytes": alg, "pack_gbs": alg / pack_ms / 1e6,
+                 "pack_frac_of_hbm": alg / pack_ms / 1e6 / peak, "hbm_peak_kind": peak_kind,
+                 "d2h_ms": d2h_ms, "d2h_gbs": snap.nbytes / d2h_ms / 1e6,
+                 "write_vti_ms": wall_ms, "write_vti_gbs": snap.nbytes / wall_ms / 1e6}
+            out[tag] = r
+        # the background writer: what the caller waits for per snapshot
+        w = gio.VTIWriter(out_dir=tmp / "series", base="s", dx=a.dx, dynamic_fields=fields, background=True)
+        w.append(None, time=0.0)
+        w.flush()
+        t0 = time.perf_counter()
+        for q in range(6):
+            w.append(None, time=float(q + 1))
+        t_append = (time.perf_counter() - t0) * 1e3 / 6
+        w.flush()
+        t_all = (time.perf_counter() - t0) * 1e3 / 6
+        out["snapshot_2d"]["background_append_ms"] = t_append
+        out["snapshot_2d"]["background_ms_per_snapshot_incl_flush"] = t_all
+        # the reference's path on the host cores: binary64 arrays to the host,
+        # then NumPy cast, flip, interleave and the file write
+        d2h_fields = [g.state.H.data, g.state.u.data, g.state.v.data, g.rheology.B.data, g.sliding.beta.data,
+                      g.geometry.bed.data]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hf = [t.cpu().numpy() for t in d2h_fields]
+        t_copy = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        b = vo.vti_bytes({"H": hf[0], "U": [vo.to_cell(hf[1], "vertical_facet"),
+                                             vo.to_cell(hf[2], "horizontal_facet")],
+                          "B": hf[3], "beta": hf[4], "bed": hf[5]}, a.dx, time_value=0.0)
+        (tmp / "ref.vti").write_bytes(b)
+        t_np = time.perf_counter() - t0
+        out["cpu_baseline"] = {"kind": "port", "cores": 1, "snapshot_2d_ms": (t_copy + t_np) * 1e3,
+                               "d2h_ms": t_copy * 1e3, "numpy_and_write_ms": t_np * 1e3,
+                               "sample": f"one {n}^2 snapshot of the same six fields through the reference's "
+                                         "writer algorithm (oracle/vti_oracle.py, NumPy, one thread)"}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps(out), flush=True)
+
+
 def thermal_leg(a, h, f, stream, dev, world):
     """The enthalpy column solve coupled to the solved state: ThermalModel
     steps (omega, frictional heating, forcing, up to 10 column/layer sweeps
@@ -842,6 +934,9 @@ def main():
         return 0
     if a.mode == "thermal":
         run_thermal(a)
+        return 0
+    if a.mode == "vti":
+        run_vti(a)
         return 0
     if a.mode == "ensemble":
         print(json.dumps({"mode": "ensemble", **run_ensemble(a)}), flush=True)

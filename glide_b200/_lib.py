@@ -179,6 +179,26 @@ SIGNATURES.update({
     "glide_enthalpy_arrhenius": ([_H, _D, _D, _P, _I, _P], _I),
 })
 
+
+
+class VtiComponent(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("dtype", ctypes.c_int), ("kind", ctypes.c_int),
+                ("stride_i", ctypes.c_longlong), ("stride_j", ctypes.c_longlong), ("stride_k", ctypes.c_longlong)]
+
+
+class VtiArray(ctypes.Structure):
+    _fields_ = [("n_components", ctypes.c_int), ("comp", VtiComponent * 3)]
+
+
+VTI_MAX_ARRAYS = 16
+VTI_PLAIN, VTI_XFACE, VTI_YFACE = 0, 1, 2
+
+SIGNATURES.update({
+    "glide_vti_pack": ([_I, _I, _I, _I, ctypes.POINTER(VtiArray), _I, _P, ctypes.c_size_t,
+                        ctypes.POINTER(ctypes.c_size_t), _P], _I),
+    "glide_io_last_error": ([], ctypes.c_char_p),
+})
+
 _LIB = None
 
 

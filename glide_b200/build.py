@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libglide_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-UNITS = ["runtime.cu", "noalloc.cu", "enthalpy.cu"]
+UNITS = ["runtime.cu", "noalloc.cu", "enthalpy.cu", "io.cu"]
 # Fast single-precision math (approximate division, square root, reciprocal
 # cube root; flush-to-zero) for the binary32 smoother and tangent kernels, as
 # the reference compiles its own kernels.  Binary64 code is unaffected.
@@ -33,7 +33,7 @@ def nvcc() -> str:
 
 
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "glide_b200.h"]
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h"))
 
 
 def stale() -> bool:

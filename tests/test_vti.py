@@ -1,0 +1,73 @@
+"""VTI / PVD output (glide/io.py:23-390): the oracle restatement against the
+files the reference's own writer produced (tests/golden/vti/, made by
+tests/golden/make_vti_golden.py), and the host-side header builder of
+glide_b200.io against the same files.  No GPU is used here."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+G = Path(__file__).resolve().parent / "golden" / "vti"
+
+
+@pytest.fixture(scope="module")
+def f():
+    with np.load(G / "inputs.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def _cells(f):
+    from oracle import vti_oracle as vo
+    return vo.to_cell(f["u"], "vertical_facet"), vo.to_cell(f["v"], "horizontal_facet")
+
+
+def cases(f):
+    """(golden file, oracle arguments) of every single-file case."""
+    u, v = _cells(f)
+    return [
+        ("scalars_vector2.vti", ({"H": f["H"], "U": [u, v], "B": f["B"]}, 1000.0),
+         dict(origin=(100.0, -50.0), time_value=2.5)),
+        ("vector3_noflip.vti", ({"W": [f["a"], f["b"], f["c"]], "bed": f["bed"]}, 250.0),
+         dict(dy=500.0, flip_y=False)),
+        ("volume.vti", ({"E": f["E"], "T": f["T"]}, 2000.0), dict(dz=0.5, origin=(1.0, 2.0, 3.0), time_value=10)),
+        ("series/dome_static.vti", ({"bed": f["bed"]}, 1000.0), {}),
+        ("series/dome_0000.vti", ({"H": f["H"], "U": [u, v], "Hsq": f["H"] * 2.0}, 1000.0), dict(time_value=0.0)),
+        ("series/dome_0001.vti", ({"H": f["H1"], "U": [u, v], "Hsq": f["H1"] * 2.0}, 1000.0),
+         dict(time_value=5.0)),
+    ]
+
+
+def test_oracle_matches_reference_files(f):
+    from oracle import vti_oracle as vo
+    for name, args, kw in cases(f):
+        assert vo.vti_bytes(*args, **kw) == (G / name).read_bytes(), name
+    assert vo.pvd_text([(0.0, "dome_0000.vti"), (5.0, "dome_0001.vti")]) == (G / "series/dome.pvd").read_text()
+
+
+def test_oracle_dimension_errors(f):
+    from oracle import vti_oracle as vo
+    with pytest.raises(ValueError):
+        vo.vti_bytes({"E": f["E"]}, 1.0)
+    with pytest.raises(NotImplementedError):
+        vo.vti_bytes({"E": f["E"], "U": [f["a"], f["c"]]}, 1.0, dz=1.0)
+    with pytest.raises(ValueError):
+        vo.vti_bytes({"H": f["H"], "E": f["E"]}, 1.0, dz=1.0)
+
+
+def test_product_header_matches_reference_files(f):
+    """glide_b200.io builds the XML part on the host: compare it with every
+    golden file up to the appended-data marker."""
+    from glide_b200.io import _vti_header
+    marker = b'  <AppendedData encoding="raw">'
+    for name, (data, dx), kw in cases(f):
+        scalars = {k: None for k, val in data.items() if not isinstance(val, list)}
+        vectors = {k: val for k, val in data.items() if isinstance(val, list)}
+        first = next(iter(data.values()))
+        shape = (first[0] if isinstance(first, list) else first).shape
+        dims = (shape[0], shape[1], shape[2] if len(shape) == 3 else 1)
+        hdr = _vti_header(scalars, vectors, dims, len(shape) == 3, dx, kw.get("dy", dx), kw.get("dz"),
+                          kw.get("origin", (0.0, 0.0)), kw.get("time_value"))
+        gold = (G / name).read_bytes()
+        assert hdr == gold[: gold.index(marker)], name
