@@ -286,13 +286,18 @@ __device__ __forceinline__ bool stopped(const int* done) { return done && *(vola
 // Inputs of row k of a column that do not depend on the column iterate:
 // E_prev, f_E (when used), omega of node k + 1 and the frozen horizontal
 // neighbours.  The kernels below load row k + 1's while row k is computed,
-// so the walk up the column does not wait on memory at every row.
+// so the walk up the column does not wait on memory at every row.  E_prev,
+// f_E and omega are each read by one thread only, so they are loaded with
+// the streaming hint (evict first): in L2 they then give way to the column
+// kernel's per-thread Newton/Thomas arrays and to the neighbour rows of E,
+// which other blocks read again.
 struct RowIn { double ep, fe, om_p; Nbr nb; };
 __device__ __forceinline__ RowIn row_inputs(const EnthArgs& a, const ColumnCtx& x, int k, bool hadv,
                                             bool forcing) {
     const size_t plane = size_t(a.ny) * a.nx;
     const size_t n = size_t(k) * plane + x.c;
-    RowIn r{a.E_prev[n], forcing ? a.f_E[n] : 0.0, a.omega[n + plane], Nbr{0.0, 0.0, 0.0, 0.0}};
+    RowIn r{__ldcs(a.E_prev + n), forcing ? __ldcs(a.f_E + n) : 0.0, __ldcs(a.omega + n + plane),
+            Nbr{0.0, 0.0, 0.0, 0.0}};
     if (hadv) r.nb = neighbours(a, x, k);
     return r;
 }

@@ -65,23 +65,38 @@ struct Pack {
 constexpr int kPackThreads = 256;
 constexpr long long kMaxRowBlocks = 4096;
 
-// The component's value at output point (i, j, k), rounded to binary32.
+// A component's value at offset e of its array (the point's own element),
+// rounded to binary32.
 template <class T>
-__device__ __forceinline__ float point_value(const Comp& c, long long k, int i, int j) {
-    const T* a = static_cast<const T*>(c.p) + k * c.sk + i * c.si + j * c.sj;
+__device__ __forceinline__ float point_value(const T* a, int kind, long long si, long long sj) {
     T x;
-    if (c.kind == GLIDE_VTI_XFACE) x = T(0.5) * (a[c.sj] + a[0]);
-    else if (c.kind == GLIDE_VTI_YFACE) x = T(0.5) * (a[c.si] + a[0]);
+    if (kind == GLIDE_VTI_XFACE) x = T(0.5) * (a[sj] + a[0]);
+    else if (kind == GLIDE_VTI_YFACE) x = T(0.5) * (a[si] + a[0]);
     else x = a[0];
     return float(x);
 }
 
+__device__ __forceinline__ float comp_value(const Comp& c, const void* row, int j) {
+    return c.f64 ? point_value(static_cast<const double*>(row) + j * c.sj, c.kind, c.si, c.sj)
+                 : point_value(static_cast<const float*>(row) + j * c.sj, c.kind, c.si, c.sj);
+}
+
+__device__ __forceinline__ const void* comp_row(const Comp& c, long long k, int i) {
+    const long long e = k * c.sk + i * c.si;
+    return c.f64 ? static_cast<const void*>(static_cast<const double*>(c.p) + e)
+                 : static_cast<const void*>(static_cast<const float*>(c.p) + e);
+}
+
 // blockIdx.y: array; blockIdx.x strides the output rows (z outer, y inner);
-// threads stride x.
-__global__ void __launch_bounds__(kPackThreads) k_vti_pack(const __grid_constant__ Pack P, int ny, int nx,
+// threads stride x.  The array's descriptors are copied to registers once
+// per block and each row's start is formed once per row, so the inner loop
+// is an address step, a load (two for face fields), a conversion and a
+// store; 32 registers keep 8 blocks (64 warps) resident per SM.
+__global__ void __launch_bounds__(kPackThreads, 8) k_vti_pack(const __grid_constant__ Pack P, int ny, int nx,
                                                            int nz, int flip, unsigned char* dst) {
     const int a = blockIdx.y;
     const int nc = P.nc[a];
+    const Comp c0 = P.c[a][0], c1 = P.c[a][1], c2 = P.c[a][2];
     unsigned char* base = dst + P.off[a];
     if (blockIdx.x == 0 && threadIdx.x == 0) *reinterpret_cast<unsigned int*>(base) = P.count[a];
     float* out = reinterpret_cast<float*>(base + 4);
@@ -91,11 +106,18 @@ __global__ void __launch_bounds__(kPackThreads) k_vti_pack(const __grid_constant
         const int row = int(r - k * ny);
         const int i = flip ? ny - 1 - row : row;
         float* o = out + r * nx * nc;
-        for (int j = threadIdx.x; j < nx; j += blockDim.x)
-            for (int q = 0; q < nc; ++q) {
-                const Comp& c = P.c[a][q];
-                o[j * nc + q] = c.f64 ? point_value<double>(c, k, i, j) : point_value<float>(c, k, i, j);
-            }
+        const void* r0 = comp_row(c0, k, i);
+        if (nc == 1) {
+            for (int j = threadIdx.x; j < nx; j += blockDim.x) o[j] = comp_value(c0, r0, j);
+            continue;
+        }
+        const void* r1 = comp_row(c1, k, i);
+        const void* r2 = nc > 2 ? comp_row(c2, k, i) : nullptr;
+        for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+            o[j * nc] = comp_value(c0, r0, j);
+            o[j * nc + 1] = comp_value(c1, r1, j);
+            if (nc > 2) o[j * nc + 2] = comp_value(c2, r2, j);
+        }
     }
 }
 
