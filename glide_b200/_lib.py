@@ -18,6 +18,8 @@ GLIDE_ERR_SHAPE = 2
 GLIDE_ERR_CUDA = 3
 GLIDE_ERR_NONFINITE = 4
 GLIDE_ERR_STATE = 5
+GLIDE_ERR_NOT_CONVERGED = 6
+GLIDE_ERR_TIMEOUT = 7
 GLIDE_F64 = 0
 GLIDE_F32 = 1
 GLIDE_MIXED = 2
@@ -62,6 +64,16 @@ class GlideError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"glide_b200 error {code}: {msg}")
         self.code = code
+
+
+class NotConverged(GlideError):
+    """A solve stopped at its cycle cap short of its tolerances (raised only
+    when the handle reports it; every output is written).  `stats` holds the
+    solve's statistics."""
+
+    def __init__(self, msg, stats):
+        super().__init__(GLIDE_ERR_NOT_CONVERGED, msg)
+        self.stats = stats
 
 
 class Phys(ctypes.Structure):

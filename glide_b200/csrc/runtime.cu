@@ -227,6 +227,10 @@ struct Solver : SolverBase {
     cudaStream_t own_stream = nullptr;
     long long launches = 0;        // kernels issued by this handle (graph replays included)
     long long newton_rejects = 0;  // Newton steps undone by the growth guard
+    int report_not_converged = 0;  // GLIDE_TUNE_REPORT_NOT_CONVERGED
+    bool last_not_converged = false;  // the last solve_loop ended short of its tolerances
+    double last_relative = 0.0;
+    int last_cycles = 0;
 
     void counted(const char* what) {
         check_launch(what);
@@ -397,7 +401,7 @@ struct Solver : SolverBase {
         for (int q = 0; q < 4; ++q) out[q] = norms_host[q];
         int e;
         std::memcpy(&e, norms_host + 4, sizeof(int));
-        if (e) fail(GLIDE_ERR_CUDA, "a kernel's bounded wait for its tile copies gave up");
+        if (e) fail(GLIDE_ERR_TIMEOUT, "a kernel's bounded wait for its tile copies gave up");
     }
 
     // TMA staging needs a level at least one box wide and high
@@ -843,6 +847,17 @@ struct Solver : SolverBase {
             st->final_norm = ab;
             for (int q = 0; q < 3; ++q) st->norms[q] = nr[q];
         }
+        last_not_converged = !(rel <= c.relative_tolerance || ab <= c.absolute_tolerance);
+        last_relative = rel;
+        last_cycles = it;
+    }
+
+    // after a whole forward / backward call: the optional status of a solve
+    // that stopped at the cycle cap
+    void report_convergence() const {
+        if (report_not_converged && last_not_converged)
+            fail(GLIDE_ERR_NOT_CONVERGED, "solve stopped after " + std::to_string(last_cycles) +
+                                              " cycles at relative residual " + std::to_string(last_relative));
     }
 
     void check_level(int l) const {
@@ -1344,6 +1359,10 @@ int glide_set_tuning(glide_handle h, int key, int value) {
             } else if (key == GLIDE_TUNE_TMA_STAGING) {
                 if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "TMA staging must be 0 or 1");
                 s.use_tma = value != 0;
+            } else if (key == GLIDE_TUNE_REPORT_NOT_CONVERGED) {
+                if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "report-not-converged must be 0 or 1");
+                s.report_not_converged = value;
+                return;  // no effect on captured graphs
             } else {
                 fail(GLIDE_ERR_ARG, "unknown tuning key");
             }
@@ -1419,7 +1438,12 @@ int glide_vanka_dump(glide_handle h, int level, double dt, void* J, void* r, voi
 }
 
 int glide_forward(glide_handle h, double dt, int start_level, glide_stats* stats, void* stream) {
-    return guarded([&] { dispatch(h, [&](auto& s) { s.forward(dt, start_level, stats, S(stream)); }); });
+    return guarded([&] {
+        dispatch(h, [&](auto& s) {
+            s.forward(dt, start_level, stats, S(stream));
+            s.report_convergence();
+        });
+    });
 }
 
 int glide_adjoint_residual(glide_handle h, int level, double dt, double* norms3, void* stream) {
@@ -1487,7 +1511,10 @@ int glide_launch_count(glide_handle h, long long* count) {
 
 int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, glide_stats* stats, void* stream) {
     return guarded([&] {
-        dispatch(h, [&](auto& s) { s.backward(dt, start_level, grad_mask, stats, S(stream)); });
+        dispatch(h, [&](auto& s) {
+            s.backward(dt, start_level, grad_mask, stats, S(stream));
+            s.report_convergence();
+        });
     });
 }
 

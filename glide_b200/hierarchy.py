@@ -15,6 +15,15 @@ from . import _lib
 from ._lib import FIELD_ID, call
 
 
+def _solve_status(code: int, st) -> None:
+    """Raise for a failed forward / backward call; NotConverged carries the
+    solve's statistics."""
+    if code == _lib.GLIDE_ERR_NOT_CONVERGED:
+        msg = _lib.load().glide_last_error()
+        raise _lib.NotConverged(msg.decode() if msg else "", st.to_dict())
+    _lib.check(code)
+
+
 def _stream_ptr():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -180,11 +189,15 @@ class Hierarchy:
 
     def set_tuning(self, sweep_blocks_per_sm: int | None = None, mixed_inner_vcycles: int | None = None,
                    forward_method: str | None = None, newton_switch_exp10: int | None = None,
-                   tangent_vcycles: int | None = None, tma_staging: bool | None = None):
+                   tangent_vcycles: int | None = None, tma_staging: bool | None = None,
+                   report_not_converged: bool | None = None):
         """Solver knobs with no counterpart in the reference (see glide_set_tuning).
         forward_method: "fascd" (the reference's V-cycles only) or "newton"
         (FASCD until 10^-newton_switch_exp10, then Newton steps whose correction
-        comes from the tangent linear multigrid)."""
+        comes from the tangent linear multigrid).  report_not_converged: forward
+        and backward raise NotConverged (with the solve's stats, after writing
+        every output) when a solve stops at its cycle cap short of its
+        tolerances; off by default, as the reference reports nothing."""
         if sweep_blocks_per_sm is not None:
             call("glide_set_tuning", self._h, 1, int(sweep_blocks_per_sm))
         if mixed_inner_vcycles is not None:
@@ -197,6 +210,8 @@ class Hierarchy:
             call("glide_set_tuning", self._h, 5, int(tangent_vcycles))
         if tma_staging is not None:
             call("glide_set_tuning", self._h, 6, int(bool(tma_staging)))
+        if report_not_converged is not None:
+            call("glide_set_tuning", self._h, 7, int(bool(report_not_converged)))
 
     def launch_count(self) -> int:
         c = ctypes.c_longlong()
@@ -230,7 +245,8 @@ class Hierarchy:
 
     def forward(self, dt: float, start_level: int = 0) -> dict:
         st = _lib.Stats()
-        call("glide_forward", self._h, float(dt), int(start_level), ctypes.byref(st), _stream_ptr())
+        _solve_status(_lib.load().glide_forward(self._h, float(dt), int(start_level), ctypes.byref(st),
+                                                _stream_ptr()), st)
         return st.to_dict()
 
     def adjoint_residual(self, level: int, dt: float, norms: bool = False):
@@ -256,6 +272,6 @@ class Hierarchy:
 
     def backward(self, dt: float, start_level: int = 0, mask: int = _lib.GRAD_ALL) -> dict:
         st = _lib.Stats()
-        call("glide_backward", self._h, float(dt), int(start_level), int(mask), ctypes.byref(st),
-             _stream_ptr())
+        _solve_status(_lib.load().glide_backward(self._h, float(dt), int(start_level), int(mask),
+                                                 ctypes.byref(st), _stream_ptr()), st)
         return st.to_dict()

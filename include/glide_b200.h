@@ -46,6 +46,11 @@ extern "C" {
 #define GLIDE_ERR_CUDA 3       /* a CUDA call failed */
 #define GLIDE_ERR_NONFINITE 4  /* residual norm became NaN or Inf */
 #define GLIDE_ERR_STATE 5      /* call not valid in the handle's current state */
+/* glide_forward / glide_backward stopped at maximum_vcycles short of both
+ * tolerances; returned only when GLIDE_TUNE_REPORT_NOT_CONVERGED is on (the
+ * reference reports nothing), after every output and *stats is written. */
+#define GLIDE_ERR_NOT_CONVERGED 6
+#define GLIDE_ERR_TIMEOUT 7    /* a kernel's bounded wait (for its staged tile copies) gave up */
 
 #define GLIDE_F64 0
 #define GLIDE_F32 1
@@ -168,6 +173,10 @@ int glide_launch_count(glide_handle h, long long* count);
  * kernels with TMA bulk tensor copies on levels at least 24 x 20 cells;
  * 0 uses clamped per-thread loads everywhere (same results). */
 #define GLIDE_TUNE_TMA_STAGING 6
+/* GLIDE_TUNE_REPORT_NOT_CONVERGED: 1 makes glide_forward / glide_backward
+ * return GLIDE_ERR_NOT_CONVERGED when the solve ends short of its
+ * tolerances; 0 (default) returns GLIDE_OK as the reference would. */
+#define GLIDE_TUNE_REPORT_NOT_CONVERGED 7
 int glide_set_tuning(glide_handle h, int key, int value);
 
 int glide_set_rhs(glide_handle h, int level, double dt, void* stream);

@@ -184,3 +184,32 @@ def test_adjoint_vanka_smooth_is_one_sweep():
         out.append(_np(lv.adjoint.lambda_u.data))
     assert np.abs(out[0]).max() > 0
     assert rel_err(out[0], out[1]) == 0.0
+
+
+def test_not_converged_status_is_opt_in():
+    """GLIDE_ERR_NOT_CONVERGED: off by default (the reference reports
+    nothing); when on, a solve that stops at its cycle cap short of its
+    tolerances raises NotConverged with its statistics, after writing every
+    output; a solve that meets its tolerance does not raise."""
+    from glide_b200._lib import GLIDE_ERR_NOT_CONVERGED, NotConverged
+    g = load_golden("c1_forward_f64")
+    model = _model(g)  # 3 cycles, zero tolerances: stops at the cap
+    model.forward(0.0, 10.0, update_geometry=False)
+    model = _model(g)
+    model.mg.hierarchy.set_tuning(report_not_converged=True)
+    with pytest.raises(NotConverged) as e:
+        model.forward(0.0, 10.0, update_geometry=False)
+    assert e.value.code == GLIDE_ERR_NOT_CONVERGED and e.value.stats["vcycles"] == 3
+    st = model.mg.levels[0].state
+    for k in ("u", "v", "H"):
+        assert rel_err(_np(getattr(st, k).data), g[f"out_{k}"]) <= 1e-10, k
+    ga = load_golden("c1_adjoint_f64")
+    model.adjoint_solver.fas_options.set(maximum_vcycles=2, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                         report_norms=False)
+    with pytest.raises(NotConverged):
+        model.backward(0.0, 10.0, dJdu=torch.as_tensor(ga["in_dJdu"]), dJdv=torch.as_tensor(ga["in_dJdv"]))
+    assert rel_err(_np(model.mg.levels[0].sliding.beta.grad), ga["out_grad_beta"]) <= 1e-10
+    model = _model(g)
+    model.mg.hierarchy.set_tuning(report_not_converged=True)
+    model.forward_solver.fas_options.set(maximum_vcycles=100, relative_tolerance=1e-3)
+    model.forward(0.0, 10.0, update_geometry=False)
