@@ -75,6 +75,7 @@ def parse(argv=None):
     ap.add_argument("--no-compare-plain", action="store_true", help="skip timing the binary64 reference form")
     ap.add_argument("--no-grads", action="store_true", help="skip timing the adjoint (gradient) solve")
     ap.add_argument("--no-thermal", action="store_true", help="skip timing the enthalpy (thermal) step")
+    ap.add_argument("--no-vti", action="store_true", help="skip timing the VTI output of the solved state")
     ap.add_argument("--nz", type=int, default=41, help="sigma levels of the enthalpy columns")
     ap.add_argument("--members", type=int, default=64, help="ensemble mode: members")
     ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
@@ -553,6 +554,15 @@ def run_ours(a, rank, world):
                  "what": "reference algorithm (FASCD 10/20/50/200, 30 local Newton iterations, quirks) in binary64"}
 
     thermal = None if a.no_thermal else thermal_leg(a, h, f, stream, dev, world)
+    output = None
+    if not a.no_vti:
+        import shutil
+        import tempfile
+        tmp = Path(tempfile.mkdtemp(prefix="glide_vti_"))
+        try:
+            output = vti_leg(a, h, stream, tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
 
     # the largest share of the step's device time (launch list of one step)
     dom = "k_jvp"
@@ -582,7 +592,7 @@ def run_ours(a, rank, world):
                    "schedule": {k: fas[k] for k in ("pre_steps", "post_steps", "finest_steps", "coarsest_steps")},
                    "parallelism": f"replicas x{world} (one domain per GPU)",
                    "l2": "inputs larger than L2 (2048^2 state and parameters: ~0.5 GB per fine-level pass)",
-                   "plain_fp64": plain, "grads": grads, "thermal": thermal},
+                   "plain_fp64": plain, "grads": grads, "thermal": thermal, "output": output},
         "gpu_launches": int(launches),
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -679,20 +689,68 @@ def run_ensemble(a):
             "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
 
 
+def vti_leg(a, h, stream, tmp):
+    """VTI output of the level-0 state through glide_b200.io (binary64 H, B,
+    beta, bed and U, the u / v faces averaged to cells on the GPU): the pack
+    kernel alone (CUDA events), the copy of its block to pinned host memory,
+    one synchronous write_vti into `tmp`, and the background VTIWriter's cost
+    of a snapshot: what the caller waits for when the writer is idle (the
+    pack and the hand-off), and the cost per snapshot of six back to back."""
+    import torch
+    from glide_b200 import io as gio
+    from glide_b200.grid import Grid
+    g = Grid(hierarchy=h, level=0)
+    fields = {"H": g.state.H, "U": [g.state.u, g.state.v], "B": g.rheology.B, "beta": g.sliding.beta,
+              "bed": g.geometry.bed}
+    n = a.size
+    snap = gio._Snapshot(fields, a.dx, a.dx, None, (0.0, 0.0), 0.0, True)
+    dev = torch.empty(snap.nbytes, dtype=torch.uint8, device="cuda")
+    host = torch.empty(snap.nbytes, dtype=torch.uint8, pin_memory=True)
+    snap.pack(dev, stream)
+    pack_ms = event_time(lambda: snap.pack(dev, stream), 10, stream)
+    alg = n * n * 6 * 8 + snap.nbytes  # six binary64 inputs read once, the block written once
+    peak, peak_kind = measured_peaks()
+    d2h_ms = event_time(lambda: host.copy_(dev, non_blocking=True), 3, stream)
+    path = tmp / "snapshot.vti"
+    gio.write_vti(path, fields, a.dx, time_value=0.0)
+    t0 = time.perf_counter()
+    gio.write_vti(path, fields, a.dx, time_value=0.0)
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    path.unlink()
+    w = gio.VTIWriter(out_dir=tmp / "series", base="s", dx=a.dx, dynamic_fields=fields, background=True)
+    w.append(None, time=0.0)
+    t_idle = 0.0
+    for q in range(3):  # snapshots a solver step apart: the writer is idle when the next one comes
+        w.flush()
+        t0 = time.perf_counter()
+        w.append(None, time=float(q + 1))
+        t_idle += (time.perf_counter() - t0) * 1e3 / 3
+    w.flush()
+    t0 = time.perf_counter()
+    for q in range(6):  # back to back: bound by the copy and the file system
+        w.append(None, time=float(q + 4))
+    w.flush()
+    t_all = (time.perf_counter() - t0) * 1e3 / 6
+    return {"what": f"VTI snapshot of the {n}^2 state (H, U from the u/v faces, B, beta, bed; binary32 file)",
+            "file_bytes": snap.nbytes + len(snap.header) + len(gio._APPENDED_OPEN) + len(gio._APPENDED_CLOSE),
+            "pack_ms": pack_ms, "pack_algorithmic_bytes": alg, "pack_gbs": alg / pack_ms / 1e6,
+            "pack_frac_of_hbm": alg / pack_ms / 1e6 / peak, "hbm_peak_kind": peak_kind,
+            "d2h_ms": d2h_ms, "d2h_gbs": snap.nbytes / d2h_ms / 1e6,
+            "write_vti_ms": wall_ms, "background_append_ms": t_idle,
+            "background_ms_per_snapshot_back_to_back": t_all}
+
+
 def run_vti(a):
     """Profiling case: VTI snapshots through glide_b200.io of the dome at
-    --size (binary64 H, B, beta, bed and the u / v faces averaged to a cell
-    vector U: the SSA state a run writes each output step) and of a layer-
-    major binary64 enthalpy volume of --nz levels; beside them the
-    reference's writer path (host copies of the binary64 arrays, then the
-    NumPy cast / flip / reorder / file write, restated in oracle/vti_oracle.py)
-    on the host cores."""
+    --size (vti_leg) and of a layer-major binary64 enthalpy volume of --nz
+    levels; beside them the reference's writer path (host copies of the
+    binary64 arrays, then the NumPy cast / flip / reorder / file write,
+    restated in oracle/vti_oracle.py) on the host cores."""
     import shutil
     import tempfile
     import torch
     from cases import dome
     from glide_b200 import io as gio
-    from glide_b200.grid import Grid
     from glide_b200.hierarchy import Hierarchy
     from oracle import vti_oracle as vo
     n, nz = a.size, a.nz
@@ -702,59 +760,41 @@ def run_vti(a):
     gen = torch.Generator(device="cuda").manual_seed(0)
     h.set("u", 0, 50.0 * torch.randn((n, n + 1), dtype=torch.float64, device="cuda", generator=gen))
     h.set("v", 0, 50.0 * torch.randn((n + 1, n), dtype=torch.float64, device="cuda", generator=gen))
-    g = Grid(hierarchy=h, level=0)
-    fields = {"H": g.state.H, "U": [g.state.u, g.state.v], "B": g.rheology.B, "beta": g.sliding.beta,
-              "bed": g.geometry.bed}
-    E = torch.randn((nz, n, n), dtype=torch.float64, device="cuda", generator=gen)
-    volume = {"E": E.permute(1, 2, 0)}
     stream = torch.cuda.current_stream()
     peak, peak_kind = measured_peaks()
     tmp = Path(tempfile.mkdtemp(prefix="glide_vti_"))
     out = {"mode": "vti", "size": n, "nz": nz}
     try:
-        for tag, data, dz, read_b in (("snapshot_2d", fields, None, 6 * 8), ("volume_3d", volume, 1.0 / (nz - 1), 8)):
-            snap = gio._Snapshot(data, a.dx, a.dx, dz, (0.0, 0.0), 0.0, True)
-            pts = n * n * (nz if dz is not None else 1)
-            dev = torch.empty(snap.nbytes, dtype=torch.uint8, device="cuda")
-            host = torch.empty(snap.nbytes, dtype=torch.uint8, pin_memory=True)
-            snap.pack(dev, stream)
-            pack_ms = event_time(lambda: snap.pack(dev, stream), 10, stream)
-            alg = pts * read_b + snap.nbytes
-            d2h_ms = event_time(lambda: host.copy_(dev, non_blocking=True), 3, stream)
-            path = tmp / f"{tag}.vti"
-            gio.write_vti(path, data, a.dx, dz=dz, time_value=0.0)
-            reps = 3 if dz is None else 1
-            t0 = time.perf_counter()
-            for _ in range(reps):
-                gio.write_vti(path, data, a.dx, dz=dz, time_value=0.0)
-            wall_ms = (time.perf_counter() - t0) * 1e3 / reps
-            path.unlink()
-            r = {"file_bytes": snap.nbytes + len(snap.header) + len(gio._APPENDED_OPEN) + len(gio._APPENDED_CLOSE),
-                 "pack_ms": pack_ms,
-                 "pack_algorithmic_bytes": alg, "pack_gbs": alg / pack_ms / 1e6,
-                 "pack_frac_of_hbm": alg / pack_ms / 1e6 / peak, "hbm_peak_kind": peak_kind,
-                 "d2h_ms": d2h_ms, "d2h_gbs": snap.nbytes / d2h_ms / 1e6,
-                 "write_vti_ms": wall_ms, "write_vti_gbs": snap.nbytes / wall_ms / 1e6}
-            out[tag] = r
-        # the background writer: what the caller waits for per snapshot
-        w = gio.VTIWriter(out_dir=tmp / "series", base="s", dx=a.dx, dynamic_fields=fields, background=True)
-        w.append(None, time=0.0)
-        w.flush()
+        out["snapshot_2d"] = vti_leg(a, h, stream, tmp)
+        E = torch.randn((nz, n, n), dtype=torch.float64, device="cuda", generator=gen)
+        volume = {"E": E.permute(1, 2, 0)}
+        dz = 1.0 / (nz - 1)
+        snap = gio._Snapshot(volume, a.dx, a.dx, dz, (0.0, 0.0), 0.0, True)
+        dev = torch.empty(snap.nbytes, dtype=torch.uint8, device="cuda")
+        host = torch.empty(snap.nbytes, dtype=torch.uint8, pin_memory=True)
+        snap.pack(dev, stream)
+        pack_ms = event_time(lambda: snap.pack(dev, stream), 10, stream)
+        alg = n * n * nz * 8 + snap.nbytes
+        d2h_ms = event_time(lambda: host.copy_(dev, non_blocking=True), 3, stream)
+        path = tmp / "volume.vti"
         t0 = time.perf_counter()
-        for q in range(6):
-            w.append(None, time=float(q + 1))
-        t_append = (time.perf_counter() - t0) * 1e3 / 6
-        w.flush()
-        t_all = (time.perf_counter() - t0) * 1e3 / 6
-        out["snapshot_2d"]["background_append_ms"] = t_append
-        out["snapshot_2d"]["background_ms_per_snapshot_incl_flush"] = t_all
+        gio.write_vti(path, volume, a.dx, dz=dz, time_value=0.0)
+        wall_ms = (time.perf_counter() - t0) * 1e3
+        path.unlink()
+        out["volume_3d"] = {"file_bytes": snap.nbytes + len(snap.header) + len(gio._APPENDED_OPEN) +
+                            len(gio._APPENDED_CLOSE), "pack_ms": pack_ms, "pack_algorithmic_bytes": alg,
+                            "pack_gbs": alg / pack_ms / 1e6, "pack_frac_of_hbm": alg / pack_ms / 1e6 / peak,
+                            "hbm_peak_kind": peak_kind, "d2h_ms": d2h_ms, "d2h_gbs": snap.nbytes / d2h_ms / 1e6,
+                            "write_vti_ms": wall_ms}
         # the reference's path on the host cores: binary64 arrays to the host,
         # then NumPy cast, flip, interleave and the file write
-        d2h_fields = [g.state.H.data, g.state.u.data, g.state.v.data, g.rheology.B.data, g.sliding.beta.data,
-                      g.geometry.bed.data]
+        from glide_b200.grid import Grid
+        g = Grid(hierarchy=h, level=0)
+        src = [g.state.H.data, g.state.u.data, g.state.v.data, g.rheology.B.data, g.sliding.beta.data,
+               g.geometry.bed.data]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hf = [t.cpu().numpy() for t in d2h_fields]
+        hf = [t.cpu().numpy() for t in src]
         t_copy = time.perf_counter() - t0
         t0 = time.perf_counter()
         b = vo.vti_bytes({"H": hf[0], "U": [vo.to_cell(hf[1], "vertical_facet"),
