@@ -718,6 +718,7 @@ def vti_leg(a, h, stream, tmp):
     wall_ms = (time.perf_counter() - t0) * 1e3
     path.unlink()
     w = gio.VTIWriter(out_dir=tmp / "series", base="s", dx=a.dx, dynamic_fields=fields, background=True)
+    w.append(None, time=-1.0)  # allocates the staging of both slots
     w.append(None, time=0.0)
     t_idle = 0.0
     for q in range(3):  # snapshots a solver step apart: the writer is idle when the next one comes
