@@ -226,6 +226,7 @@ struct Solver : SolverBase {
     CachedGraph graphs[kKinds];
     cudaStream_t own_stream = nullptr;
     long long launches = 0;        // kernels issued by this handle (graph replays included)
+    long long* launch_sink = nullptr;  // a binary32 shadow also counts into its handle's solver
     long long newton_rejects = 0;  // Newton steps undone by the growth guard
     int report_not_converged = 0;  // GLIDE_TUNE_REPORT_NOT_CONVERGED
     bool last_not_converged = false;  // the last solve_loop ended short of its tolerances
@@ -235,6 +236,7 @@ struct Solver : SolverBase {
     void counted(const char* what) {
         check_launch(what);
         ++launches;
+        if (launch_sink) ++*launch_sink;
     }
 
     Solver(int ny, int nx, double dx, int L) {
@@ -672,6 +674,7 @@ struct Solver : SolverBase {
         f.use_graphs = 0;
         f.use_tma = use_tma;
         f.err_dev = err_dev;  // shadow kernels report into this handle's error word
+        f.launch_sink = &launches;  // and count into its launches (captured cycles included)
         for (int l = 0; l < n_levels; ++l) {
             if (f.lv[l].phys.thklim != lv[l].phys.thklim)
                 f.fill(f.lv[l].a[GLIDE_GAMMA], float(lv[l].phys.thklim), nullptr);

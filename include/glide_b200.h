@@ -152,7 +152,8 @@ int glide_set_reference_quirks(glide_handle h, int on);
 /* use_graphs = 1 replays each V-cycle as a captured CUDA graph. */
 int glide_set_use_graphs(glide_handle h, int use_graphs);
 /* Number of kernels this handle has launched so far (graph replays count
- * every kernel node).  No counterpart in the reference: instrumentation. */
+ * every kernel node; a GLIDE_MIXED handle's binary32 kernels included).
+ * No counterpart in the reference: instrumentation. */
 int glide_launch_count(glide_handle h, long long* count);
 /* Kernel tuning knobs (no counterpart in the reference).
  * GLIDE_TUNE_SWEEP_BLOCKS_PER_SM: 1 or 2 resident Vanka-sweep blocks per SM.
