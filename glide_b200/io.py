@@ -82,7 +82,7 @@ class _Comp:
 def _tensor(a) -> torch.Tensor:
     if isinstance(a, torch.Tensor):
         return a if a.is_cuda else a.cuda()
-    return torch.as_tensor(np.asarray(a), device="cuda")
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")  # views with negative strides included
 
 
 def _entity(value) -> str | None:

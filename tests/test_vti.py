@@ -71,3 +71,26 @@ def test_product_header_matches_reference_files(f):
                           kw.get("origin", (0.0, 0.0)), kw.get("time_value"))
         gold = (G / name).read_bytes()
         assert hdr == gold[: gold.index(marker)], name
+
+
+def test_writer_manifest_and_bookkeeping(tmp_path):
+    """VTIWriter's host side (glide/io.py:187-353) without a snapshot: the PVD
+    manifest of recorded steps is the reference's file, initialize(overwrite=
+    True) clears earlier output and the records, and the argument errors of
+    append / initialize are the reference's."""
+    from glide_b200.io import VTIWriter
+    w = VTIWriter(out_dir=tmp_path, base="dome", dx=1000.0)
+    assert w.dy == 1000.0 and w.write_static(None) is None
+    w.records += [(0.0, "dome_0000.vti"), (5.0, "dome_0001.vti")]
+    w.write_pvd()
+    assert (tmp_path / "dome.pvd").read_bytes() == (G / "series" / "dome.pvd").read_bytes()
+    (tmp_path / "dome_0000.vti").write_bytes(b"x")
+    (tmp_path / "other_0000.vti").write_bytes(b"x")
+    w.initialize(None, overwrite=True)
+    assert not (tmp_path / "dome_0000.vti").exists() and not (tmp_path / "dome.pvd").exists()
+    assert (tmp_path / "other_0000.vti").exists() and w.records == []
+    with pytest.raises(ValueError, match="No dynamic fields"):
+        w.append(None, time=0.0)
+    w2 = VTIWriter(out_dir=tmp_path, dynamic_fields={"H": np.zeros((2, 2))})
+    with pytest.raises(ValueError, match="`time` must be provided"):
+        w2.initialize(None, write_dynamic_initial=True)
