@@ -555,8 +555,8 @@ __global__ void __launch_bounds__(kColThreads) k_enth_omega(EnthArgs a, double* 
     const double dh = dh_dt ? dh_dt[size_t(i) * ld_dh + j] : (h - a.H_prev[c]) / dh_div;
     double w = bmb ? -bmb[size_t(i) * ld_bmb + j] : -0.0;
     omega[c] = w / omega_div;
-    double div_prev = 0.0;
-    for (int k = 0; k < nz; ++k) {
+    // horizontal divergence of the thickness flux at level k
+    auto div_at = [&](int k) {
         const double* uk = a.u + k * a.u_layer + size_t(i) * a.ld_u;
         const double* vk = a.v + k * a.v_layer;
         const double ul = uk[j], ur = uk[j + 1];
@@ -566,7 +566,15 @@ __global__ void __launch_bounds__(kColThreads) k_enth_omega(EnthArgs a, double* 
         if (j > 0) fl = 0.5 * (Hxm + h) * ul - 0.5 * sqrt(ul * ul + kRegYr) * (h - Hxm);
         if (i < a.ny - 1) fb = 0.5 * (h + Hyp) * vb - 0.5 * sqrt(vb * vb + kRegYr) * (h - Hyp);
         if (i > 0) ft = 0.5 * (Hym + h) * vt - 0.5 * sqrt(vt * vt + kRegYr) * (Hym - h);
-        const double div = (fr - fl + ft - fb) * dx_inv;
+        return (fr - fl + ft - fb) * dx_inv;
+    };
+    // a depth-independent velocity (layer stride 0) gives every level the
+    // same divergence: evaluate it once
+    const bool flat = a.u_layer == 0 && a.v_layer == 0;
+    const double div_flat = flat ? div_at(0) : 0.0;
+    double div_prev = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const double div = flat ? div_flat : div_at(k);
         if (k > 0) {
             w = w - dsig * (dh + 0.5 * (div_prev + div));
             omega[size_t(k) * plane + c] = w / omega_div;
@@ -590,12 +598,17 @@ __global__ void __launch_bounds__(kColThreads) k_enth_set_rhs(EnthArgs a, double
     const size_t c = size_t(i) * a.nx + j;
     const double h = a.H[size_t(i) * a.ld_h + j];
     const double dsig_half = 0.5 * (1.0 / double(nz - 1));
+    // distinct arrays: the unrolled loop issues several levels' loads ahead
+    // of their stores
+    const double* __restrict__ ps = phi_strain + c;
+    double* __restrict__ fe = f_E + c;
+#pragma unroll 4
     for (int k = 0; k < nz - 1; ++k) {
-        double f = h * phi_strain[size_t(k) * plane + c] / e_scale;
+        double f = h * ps[size_t(k) * plane] / e_scale;
         if (k == 0) f += (Q_geo[c] + Q_fh[c]) / (dsig_half * e_scale);
-        f_E[size_t(k) * plane + c] = f;
+        fe[size_t(k) * plane] = f;
     }
-    f_E[size_t(nz - 1) * plane + c] = 0.0;
+    fe[size_t(nz - 1) * plane] = 0.0;
 }
 
 // Q_fh = beta |u_b|^(m+1) from the bed-layer velocity (glide/model.py:224-235)
@@ -614,7 +627,7 @@ __global__ void k_enth_friction(EnthArgs a, double* Q_fh, const double* beta, in
 // Depth-averaged rate factor B = mean_k(A)^(-1/n) / scale (Paterson-Budd with
 // water-content enhancement, glide/enthalpy.py:600-643).  Host-side constants
 // of glide/enthalpy.py (binary64), sigma as numpy.linspace gives it.
-__global__ void __launch_bounds__(kColThreads) k_enth_arrhenius(EnthArgs a, double* B, int ld_B, double n_glen,
+__global__ void __launch_bounds__(kColThreads, 8) k_enth_arrhenius(EnthArgs a, double* B, int ld_B, double n_glen,
                                                                    double scale) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= a.ny * a.nx) return;
