@@ -263,7 +263,9 @@ def write_vti(filename, data, dx, dy=None, dz=None, origin=(0.0, 0.0), time_valu
     centres) or lists of 2-D components (vectors).  3-D output needs dz and
     takes no vectors.  origin is (x, y) or (x, y, z).  flip_y writes row
     ny - 1 first (image rows to VTK's upward y).  Returns when the file is
-    written."""
+    written.  Each host thread keeps one device and one pinned host staging
+    buffer, grown to the largest snapshot it has written, for reuse by later
+    calls; release_staging() frees them."""
     if dy is None:
         dy = dx
     Path(filename).parent.mkdir(parents=True, exist_ok=True)
@@ -277,6 +279,11 @@ def write_vti(filename, data, dx, dy=None, dz=None, origin=(0.0, 0.0), time_valu
     host[: snap.nbytes].copy_(dev[: snap.nbytes], non_blocking=True)
     stream.synchronize()
     _write_file(Path(filename), snap.header, memoryview(host.numpy())[: snap.nbytes])
+
+
+def release_staging() -> None:
+    """Free this thread's write_vti staging buffers (device and pinned host)."""
+    _sync_staging.buf = None
 
 
 class _Background:

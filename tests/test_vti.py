@@ -94,3 +94,11 @@ def test_writer_manifest_and_bookkeeping(tmp_path):
     w2 = VTIWriter(out_dir=tmp_path, dynamic_fields={"H": np.zeros((2, 2))})
     with pytest.raises(ValueError, match="`time` must be provided"):
         w2.initialize(None, write_dynamic_initial=True)
+
+
+def test_release_staging_without_buffers():
+    """release_staging frees this thread's write_vti buffers; with none
+    allocated it is a no-op (no GPU touched)."""
+    from glide_b200 import io as gio
+    gio.release_staging()
+    assert getattr(gio._sync_staging, "buf", None) is None
