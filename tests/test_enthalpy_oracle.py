@@ -5,6 +5,8 @@ reference's enthalpy tests (tests/test_enthalpy_cold_column.py,
 tests/test_enthalpy_stefan.py)."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -87,3 +89,67 @@ def test_cold_column_smoother_reduces_residual():
         r.append(np.max(np.abs(eo.residual(s, cfg))))
         s["E"] += eo.column_smooth(s, cfg)
     assert r[0] / r[-1] > 100
+
+
+REF = os.environ.get("GLIDE_REFERENCE", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "glide", "cuda")),
+                    reason="reference checkout not present")
+@pytest.mark.parametrize("nz,flags", [(3, 7), (4, 1), (17, 6), (24, 0), (41, 7)])
+def test_oracle_matches_live_reference_across_nz_and_terms(nz, flags):
+    """Fresh states of several column heights and term selections (bit 1
+    horizontal advection, 2 sigma advection, 4 drainage), the reference's
+    EnthalpyOperators run live (its kernels on host cores): residual, column
+    and layer smoothers at 1e-12, and a 3-sweep alternating solve at 1e-10."""
+    import contextlib
+    import io
+
+    from cases import enthalpy_state
+    from oracle import build_oracle
+    from oracle.refpy import load_reference
+    build_oracle.build_reference(REF)
+    load_reference(fp64=True, reference=REF)
+    from glide.enthalpy import EnthalpyOperators, EnthalpyTermFlags
+    from glide.grid import Grid
+    ny, nx = 5, 7
+    st = enthalpy_state(ny, nx, nz, seed=31 + nz)
+    cfg = enthalpy_config(term_flags=flags, relative_tolerance=1e-30, absolute_tolerance=0.0)
+    dt = cfg["dt"]
+
+    def make_ops():
+        with contextlib.redirect_stdout(io.StringIO()):
+            g = Grid(ny, nx, cfg["dx"])
+            g.state.H.set(st["H"])
+            ops = EnthalpyOperators(g, nz=nz)
+        ops.term_flags = EnthalpyTermFlags(horizontal_advection=bool(flags & 1), omega=bool(flags & 2),
+                                           drainage=bool(flags & 4))
+        es, ev, ef = ops.enthalpy_state, ops.enthalpy_velocity, ops.enthalpy_forcing
+        es.E[:] = st["E"]
+        es.E_prev[:] = st["E_prev"]
+        ops.f_E[:] = st["f_E"]
+        ev.u3d[:] = st["u3d"]
+        ev.v3d[:] = st["v3d"]
+        ev.omega[:] = st["omega"]
+        ops.H_prev[:] = st["H_prev"]
+        ef.E_surface[:] = st["E_surface"]
+        ops.smoother_config.relative_tolerance = 1e-30
+        ops.smoother_config.absolute_tolerance = 0.0
+        return ops
+
+    s = {k: np.ascontiguousarray(v.copy()) for k, v in st.items()}
+    ops = make_ops()
+    with contextlib.redirect_stdout(io.StringIO()):
+        ops.compute_residual(dt)
+    assert rel_err(eo.residual(s, cfg), np.array(ops.r_E)) <= 1e-12
+    with contextlib.redirect_stdout(io.StringIO()):
+        ops.column_smooth(dt)
+    assert rel_err(eo.column_smooth(s, cfg), np.array(ops.delta_E)) <= 1e-12
+    with contextlib.redirect_stdout(io.StringIO()):
+        ops.layer_smooth(dt)
+    assert rel_err(eo.layer_smooth(s, cfg), np.array(ops.delta_E)) <= 1e-12
+    ops = make_ops()
+    with contextlib.redirect_stdout(io.StringIO()):
+        ops.column_sweep(dt, 3, alternating=True)
+    eo.column_sweep(s, cfg, 3, alternating=True)
+    assert rel_err(s["E"], np.array(ops.enthalpy_state.E)) <= 1e-10

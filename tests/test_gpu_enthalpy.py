@@ -151,3 +151,19 @@ def test_cold_column_analytic():
     E = _np(ops.enthalpy_state.E[ny // 2, nx // 2, :]) * E_SCALE
     Ea = C_I * (Ts - T_REF) + C_I * Q * H / K_I * (1 - sigma)
     assert np.max(np.abs(E[:-1] - Ea[:-1]) / np.abs(Ea[:-1])) < 5e-3
+
+
+@pytest.mark.parametrize("nz", [3, 4, 17])
+def test_column_sweeps_match_oracle_across_nz(nz):
+    """A 3-sweep column solve at the smallest column heights and an odd one
+    (thin-ice columns included) against the oracle at 1e-10."""
+    from oracle import enthalpy_oracle as eo
+    st = enthalpy_state(24, 40, nz, seed=13)
+    cfg = enthalpy_config(relative_tolerance=1e-30, absolute_tolerance=0.0)
+    ops = _ops(st, cfg["dx"], nz)
+    ops.smoother_config.relative_tolerance = 1e-30
+    ops.smoother_config.absolute_tolerance = 0.0
+    ops.column_sweep(cfg["dt"], 3)
+    s = {k: v.copy() for k, v in st.items()}
+    eo.column_sweep(s, cfg, 3)
+    assert rel_err(_np(ops.enthalpy_state.E), s["E"]) <= 1e-10
