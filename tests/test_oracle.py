@@ -158,3 +158,84 @@ def test_vanka_dump_matches_reference():
     J, r = lev.vanka_dump(5.0)
     assert rel_err(J, g["out_J"]) <= 1e-12
     assert rel_err(r, g["out_r"]) <= 1e-12
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "glide", "cuda")),
+                    reason="reference checkout not present")
+def test_oracle_operators_match_live_reference_on_new_shape():
+    """A non-square 28 x 44 state on a seed no fixture uses, the reference
+    run live: the masked residual and the forcing-free operator with
+    calving (1e-13), then the transpose product, adjoint residual, two
+    adjoint sweeps and the beta / bed gradients (1e-12)."""
+    import contextlib
+    import io
+
+    from cases import random_state
+    from oracle import build_oracle
+    from oracle.refpy import load_reference
+    build_oracle.build_reference(REF)
+    load_reference(fp64=True, reference=REF)
+    from glide.grid import Grid
+    st = random_state(28, 44, seed=321)
+    ny, nx = st["H"].shape
+    dt = 3.0
+
+    def grid(calving):
+        with contextlib.redirect_stdout(io.StringIO()):
+            g = Grid(ny, nx, 1500.0)
+        for k in ("u", "v", "H", "H_prev", "mask"):
+            getattr(g.state, k).set(st[k])
+        g.geometry.bed.set(st["bed"]); g.rheology.B.set(st["B"])
+        g.sliding.beta.set(st["beta"]); g.forcing.smb.set(st["smb"])
+        g.calving.calving_rate.set(calving)
+        g.forward_operators.f_u[:, :] = st["f_u"]
+        g.forward_operators.f_v[:, :] = st["f_v"]
+        return g
+
+    inp = {f"in_{k}": v for k, v in st.items()}
+    g = grid(1.0)
+    ops = g.forward_operators
+    ops.set_rhs(dt)
+    ops.compute_residual(dt, use_mask=True)
+    lev = oracle_single_level(inp, 1500.0, calving=1.0).levels[0]
+    lev.f_H[...] = lev.H_prev / dt + lev.smb
+    lev.residual(dt, use_mask=True)
+    for k in ("r_u", "r_v", "r_H"):
+        assert rel_err(getattr(lev, k), np.array(getattr(ops, k))) <= 1e-13, k
+    ops.compute_residual(dt, use_mask=False, operator_only=True, freeze_phi=True)
+    lev.residual(dt, use_mask=False, operator_only=True, freeze_phi=True)
+    for k in ("F_u", "F_v", "F_H"):
+        assert rel_err(getattr(lev, k), np.array(getattr(ops, k))) <= 1e-13, k
+
+    rng = np.random.default_rng(99)
+    lam = dict(lambda_u=rng.normal(0, 1, (ny, nx + 1)), lambda_v=rng.normal(0, 1, (ny + 1, nx)),
+               lambda_H=rng.normal(0, 1, (ny, nx)))
+    af = dict(adj_f_u=rng.normal(0, 1, (ny, nx + 1)), adj_f_v=rng.normal(0, 1, (ny + 1, nx)),
+              adj_f_H=rng.normal(0, 1, (ny, nx)))
+    g = grid(0.0)
+    g.forward_operators.compute_phi()
+    for k, v in lam.items():
+        getattr(g.adjoint, k).set(v)
+    aops = g.adjoint_operators
+    aops.f_u[:, :], aops.f_v[:, :], aops.f_H[:, :] = af["adj_f_u"], af["adj_f_v"], af["adj_f_H"]
+    lev = oracle_single_level(inp, 1500.0).levels[0]
+    lev.compute_phi()
+    lev.l_u[...], lev.l_v[...], lev.l_H[...] = lam["lambda_u"], lam["lambda_v"], lam["lambda_H"]
+    lev.af_u[...], lev.af_v[...], lev.af_H[...] = af["adj_f_u"], af["adj_f_v"], af["adj_f_H"]
+    aops.compute_vjp(dt)
+    lev.adj_vjp(dt)
+    for k in ("vjp_u", "vjp_v", "vjp_H"):
+        assert rel_err(getattr(lev, k), np.array(getattr(aops, k))) <= 1e-12, k
+    aops.compute_residual(dt)
+    lev.adj_residual(dt)
+    for k, r in (("ar_u", "r_u"), ("ar_v", "r_v"), ("ar_H", "r_H")):
+        assert rel_err(getattr(lev, k), np.array(getattr(aops, r))) <= 1e-12, k
+    aops.vanka_sweep(dt, 2)
+    lev.adj_sweep(dt, 2)
+    for k, r in (("l_u", "lambda_u"), ("l_v", "lambda_v"), ("l_H", "lambda_H")):
+        assert rel_err(getattr(lev, k), np.array(getattr(g.adjoint, r).data)) <= 1e-12, k
+    aops.compute_gradient_beta()
+    aops.compute_gradient_bed()
+    lev.gradients()
+    assert rel_err(lev.g_beta, np.array(g.sliding.beta.grad)) <= 1e-12
+    assert rel_err(lev.g_bed, np.array(g.geometry.bed.grad)) <= 1e-12
