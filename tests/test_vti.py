@@ -102,3 +102,39 @@ def test_release_staging_without_buffers():
     from glide_b200 import io as gio
     gio.release_staging()
     assert getattr(gio._sync_staging, "buf", None) is None
+
+
+def test_pack_size_query_and_argument_errors_without_gpu():
+    """glide_vti_pack through the C ABI with no destination (a size query,
+    no device work): the block's byte count, and the argument checks."""
+    import ctypes
+
+    from glide_b200 import _lib
+    if not _lib.LIB_PATH.exists():
+        pytest.skip("library not built")
+    lib = _lib.load()
+    arrays = (_lib.VtiArray * 3)()
+    for a, nc in zip(arrays, (1, 2, 3)):
+        a.n_components = nc
+        for q in range(nc):
+            a.comp[q] = _lib.VtiComponent(None, _lib.GLIDE_F64, _lib.VTI_PLAIN, 5, 1, 0)
+    n = ctypes.c_size_t()
+    ny, nx, nz = 6, 5, 2
+    assert lib.glide_vti_pack(ny, nx, nz, 1, arrays, 3, None, 0, ctypes.byref(n), None) == _lib.GLIDE_OK
+    assert n.value == sum(4 + 4 * ny * nx * nz * c for c in (1, 2, 3))
+    assert lib.glide_vti_pack(0, nx, nz, 1, arrays, 3, None, 0, ctypes.byref(n), None) == _lib.GLIDE_ERR_SHAPE
+    assert lib.glide_vti_pack(ny, nx, nz, 1, arrays, 0, None, 0, ctypes.byref(n), None) == _lib.GLIDE_ERR_ARG
+    assert lib.glide_vti_pack(ny, nx, nz, 1, arrays, 17, None, 0, ctypes.byref(n), None) == _lib.GLIDE_ERR_ARG
+    assert b"n_arrays" in lib.glide_io_last_error()
+    arrays[0].comp[0].dtype = 7
+    assert lib.glide_vti_pack(ny, nx, nz, 1, arrays, 3, None, 0, ctypes.byref(n), None) == _lib.GLIDE_ERR_ARG
+    arrays[0].comp[0].dtype = _lib.GLIDE_F32
+    arrays[0].comp[0].kind = 3
+    assert lib.glide_vti_pack(ny, nx, nz, 1, arrays, 3, None, 0, ctypes.byref(n), None) == _lib.GLIDE_ERR_ARG
+    arrays[0].comp[0].kind = _lib.VTI_XFACE
+    arrays[1].n_components = 4
+    assert lib.glide_vti_pack(ny, nx, nz, 1, arrays, 3, None, 0, ctypes.byref(n), None) == _lib.GLIDE_ERR_ARG
+    arrays[1].n_components = 2
+    # values of 2^32 bytes or more do not fit the 32-bit count word
+    assert lib.glide_vti_pack(1 << 15, 1 << 15, 1, 1, arrays, 1, None, 0, ctypes.byref(n), None) == \
+        _lib.GLIDE_ERR_SHAPE
