@@ -12,11 +12,11 @@
 // 16 x 16 tile -- lives in the file-scope device array below, so this entry
 // point calls no allocating routine at all.  Its size bounds the grid:
 // kNoAllocMaxTiles tiles, i.e. up to 65,536 tiles of 16 x 16 cells
-// (4096 x 4096 cells), 1.5 MiB per device, held by every GPU that loads the
-// library until the process exits.
+// (4096 x 4096 cells, for example), 1.5 MiB per device, held by every GPU that
+// loads the library until the process exits.  Independently, a grid has at
+// most 65,535 rows.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "glide_b200.h"
@@ -25,7 +25,8 @@
 namespace glide {
 namespace noalloc {
 
-constexpr int kNoAllocMaxTiles = 65536;
+constexpr long long kNoAllocMaxTiles = 65536;
+constexpr long long kNoAllocMaxRows = 65535;
 
 // 3 partial sums per tile; every call rewrites each slot it later reads, so
 // nothing needs clearing between calls.  Calls that overlap on the GPU
@@ -34,34 +35,22 @@ static __device__ __align__(256) double g_tile_sums[3 * kNoAllocMaxTiles];
 
 static thread_local std::string t_err;
 
-// Device address of g_tile_sums, looked up once per device with that device
-// current.  In host code the symbol itself is only a host-side stand-in.
-constexpr int kMaxDevices = 64;
-static std::mutex g_mu;
-static void* g_addr[kMaxDevices] = {nullptr};
-
+// Device address of g_tile_sums in the CUDA context current on this thread.
+// In host code the symbol itself is only a host-side stand-in, so every call
+// looks the address up again: the array belongs to the module loaded in a
+// context, not to a device ordinal, and a cached pointer would go stale after
+// cudaDeviceReset or point into another context when the host switches
+// driver-API contexts on one device.  The lookup allocates nothing.  The first
+// lookup in a context loads the module (and with it this array), which is why
+// the first call on a device should come before any stream capture.
 static int scratch_address(double** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        t_err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_tile_sums);
+    if (e != cudaSuccess || !p) {
+        t_err = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e);
         return GLIDE_ERR_CUDA;
     }
-    if (dev < 0 || dev >= kMaxDevices) {
-        t_err = "device ordinal beyond the supported range";
-        return GLIDE_ERR_ARG;
-    }
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_tile_sums);
-        if (e != cudaSuccess || !p) {
-            t_err = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e);
-            return GLIDE_ERR_CUDA;
-        }
-        g_addr[dev] = p;
-    }
-    *out = static_cast<double*>(g_addr[dev]);
+    *out = static_cast<double*>(p);
     return GLIDE_OK;
 }
 
@@ -115,14 +104,25 @@ extern "C" int glide_residual_norms_noalloc(int ny, int nx, double dx, double dt
         t_err = "forcing arrays are required unless GLIDE_OPERATOR_ONLY is set";
         return GLIDE_ERR_ARG;
     }
-    if (ny < 2 || nx < 2 || !(dx > 0) || !(dt > 0) || ld_u < nx + 1 || ld_v < nx || ld_c < nx) {
+    // All size arithmetic in 64 bits, so that nx or ny near INT_MAX cannot
+    // wrap around and slip past the checks.
+    const long long nyl = ny, nxl = nx;
+    if (nyl < 2 || nxl < 2 || !(dx > 0) || !(dt > 0) || (long long)ld_u < nxl + 1 || (long long)ld_v < nxl ||
+        (long long)ld_c < nxl) {
         t_err = "bad sizes: need ny, nx >= 2, dx, dt > 0, ld_u >= nx + 1, ld_v >= nx, ld_c >= nx";
         return GLIDE_ERR_SHAPE;
     }
-    const long tiles_x = (nx + kTile - 1) / kTile, tiles_y = (ny + kTile - 1) / kTile;
+    // The grounded-fraction launch puts one grid row per block row, and a
+    // grid's y extent is at most 65,535.
+    if (nyl > noalloc::kNoAllocMaxRows) {
+        t_err = "grid too tall for the no-allocation residual: at most " +
+                std::to_string(noalloc::kNoAllocMaxRows) + " rows";
+        return GLIDE_ERR_SHAPE;
+    }
+    const long long tiles_x = (nxl + kTile - 1) / kTile, tiles_y = (nyl + kTile - 1) / kTile;
     if (tiles_x * tiles_y > noalloc::kNoAllocMaxTiles) {
         t_err = "grid too large for the no-allocation residual: at most " +
-                std::to_string(noalloc::kNoAllocMaxTiles) + " tiles of 16 x 16 cells (4096 x 4096 cells)";
+                std::to_string(noalloc::kNoAllocMaxTiles) + " tiles of 16 x 16 cells (e.g. 4096 x 4096 cells)";
         return GLIDE_ERR_SHAPE;
     }
     double* sums = nullptr;

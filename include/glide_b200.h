@@ -215,10 +215,9 @@ int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, gl
 int glide_vcycle(glide_handle h, int which, int level, int finest, double dt, void* stream);
 
 /* Residual and its norms on caller-owned device arrays, allocating nothing.
- * No counterpart in the reference: it is glide_residual (the reference's
- * ForwardOperators.compute_residual, glide/operators.py:71-127) for hosts that
- * may not allocate device memory after start-up and so cannot create a
- * handle.  All arrays are binary64 device memory, row-major with leading
+ * No counterpart in the reference.  It computes what glide_residual computes
+ * for one level, for hosts that may not allocate device memory after start-up
+ * and so cannot create a handle.  All arrays are binary64 device memory, row-major with leading
  * dimensions ld_u (u, f_u, r_u: ny x (nx+1)), ld_v (v, f_v, r_v: (ny+1) x nx)
  * and ld_c (cell arrays: ny x nx).  Unless flags has GLIDE_FREEZE_PHI, phi is
  * first recomputed from H and bed (it is in/out, and must hold finite values
@@ -226,10 +225,12 @@ int glide_vcycle(glide_handle h, int which, int level, int finest, double dt, vo
  * GLIDE_OPERATOR_ONLY (f_* may then be NULL) and GLIDE_FREEZE_CALVING act as
  * in glide_residual.  norms (device, 4 doubles) receives |r_u|, |r_v|, |r_H|
  * and the combined norm; it is written on `stream`, not synchronised.
- * Limit: at most 65,536 tiles of 16 x 16 cells (4096 x 4096 cells);
- * larger grids return GLIDE_ERR_SHAPE.  The scratch is one static device
- * array per GPU; the first call on each device looks up its address, so make
- * that call before any stream capture.  Nothing needs zeroing beforehand.
+ * Limits: at most 65,536 tiles of 16 x 16 cells (4096 x 4096 cells, for
+ * example) and at most 65,535 rows; larger grids return GLIDE_ERR_SHAPE.  The
+ * scratch is one static device array per GPU (1.5 MiB).  Every call looks up
+ * its address in the current context; the first call in a context also loads
+ * the module that holds it, so make that call before any stream capture.
+ * Nothing needs zeroing beforehand.
  * Calls that overlap in time on one GPU share that scratch and race. */
 int glide_residual_norms_noalloc(int ny, int nx, double dx, double dt, const glide_phys* phys,
                                  const double* u, int ld_u, const double* v, int ld_v, const double* H,

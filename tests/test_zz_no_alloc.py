@@ -78,9 +78,22 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     lib = _lib.load()
     phys = _lib.Phys()
     fake = ctypes.c_void_p(256)  # never dereferenced: the size check comes first
-    ny = nx = 4097
-    rc = lib.glide_residual_norms_noalloc(
-        ny, nx, 1000.0, DT, ctypes.byref(phys), fake, nx + 1, fake, nx, fake, fake, fake, fake, fake,
-        fake, fake, fake, fake, fake, nx, 0, fake, fake, fake, fake, None)
-    assert rc == _lib.GLIDE_ERR_SHAPE
+
+    def call(ny, nx, ld_u, ld_v, ld_c):
+        return lib.glide_residual_norms_noalloc(
+            ny, nx, 1000.0, DT, ctypes.byref(phys), fake, ld_u, fake, ld_v, fake, fake, fake, fake, fake,
+            fake, fake, fake, fake, fake, ld_c, 0, fake, fake, fake, fake, None)
+
+    # too many tiles
+    assert call(4097, 4097, 4098, 4097, 4097) == _lib.GLIDE_ERR_SHAPE
     assert b"4096 x 4096" in lib.glide_noalloc_last_error()
+    # few tiles, but more rows than one launch's grid can hold
+    assert call(70000, 16, 17, 16, 16) == _lib.GLIDE_ERR_SHAPE
+    assert b"65535 rows" in lib.glide_noalloc_last_error()
+    # nx near INT_MAX: nx + 1 must not wrap around and pass the pitch check
+    big = 2**31 - 1
+    assert call(16, big, -(2**31), big, big) == _lib.GLIDE_ERR_SHAPE
+    assert b"ld_u >= nx + 1" in lib.glide_noalloc_last_error()
+    # ... nor may the tile count wrap when every pitch is large enough
+    assert call(16, big - 1, big, big - 1, big - 1) == _lib.GLIDE_ERR_SHAPE
+    assert b"tiles" in lib.glide_noalloc_last_error()
