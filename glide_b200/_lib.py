@@ -142,7 +142,7 @@ SIGNATURES = {
     "glide_forward": ([_H, _D, _I, ctypes.POINTER(Stats), _P], _I),
     "glide_adjoint_residual": ([_H, _I, _D, ctypes.POINTER(_D), _P], _I),
     "glide_vjp": ([_H, _I, _D, _P], _I),
-    "glide_jvp": ([_H, _I, _D, _I, _P], _I),
+    "glide_jvp": ([_H, _I, _D, _I, _I, _P], _I),
     "glide_adjoint_sweep": ([_H, _I, _D, _I, _P], _I),
     "glide_gradients": ([_H, _I, _D, _I, _P], _I),
     "glide_backward": ([_H, _D, _I, _I, ctypes.POINTER(Stats), _P], _I),

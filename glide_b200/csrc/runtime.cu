@@ -887,8 +887,10 @@ struct Solver : SolverBase {
     }
 
     // out = Op(x) [- f] [- sub], Op = J^T (vjp) or J (jvp) at the level's state
+    // jvp_flags (the JVP only): GLIDE_USE_MASK and GLIDE_FREEZE_CALVING as in
+    // glide_jvp; the solver's own tangent operator keeps the mask and calving.
     void lin_op(int l, double dt, const Lin& L, const int* out, const int* sub, bool use_forcing, bool norms,
-                bool ref_rows, cudaStream_t s) {
+                bool ref_rows, cudaStream_t s, int jvp_flags = GLIDE_USE_MASK) {
         Level<R>& v = lv[l];
         VjpArgs<R> a;
         a.u = v.a[GLIDE_U]; a.v = v.a[GLIDE_V]; a.H = v.a[GLIDE_H];
@@ -900,7 +902,7 @@ struct Solver : SolverBase {
         if (sub) { a.s_u = v.a[sub[0]]; a.s_v = v.a[sub[1]]; a.s_H = v.a[sub[2]]; }
         a.partial = norms ? partial : nullptr;
         a.err = err_dev;
-        a.p = physr(l, dt, false);
+        a.p = physr(l, dt, !L.tr && (jvp_flags & GLIDE_FREEZE_CALVING));
         a.ny = v.ny; a.nx = v.nx; a.use_forcing = use_forcing;
         dim3 g((a.nx + kTileA - 1) / kTileA, (a.ny + kTileA - 1) / kTileA);
         if (L.tr) {
@@ -911,7 +913,8 @@ struct Solver : SolverBase {
         } else {
             const int fl[JvpTile<R>::NB] = {GLIDE_U, GLIDE_V, L.x[0], L.x[1], GLIDE_H, GLIDE_PHI, GLIDE_BED,
                                             GLIDE_BETA, GLIDE_B, L.x[2]};
-            k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, ref_rows ? 1 : 0, box_maps(l, fl));
+            const int mode = (ref_rows ? 1 : 0) | ((jvp_flags & GLIDE_USE_MASK) ? 0 : 2);
+            k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, mode, box_maps(l, fl));
             counted("jvp");
         }
         if (norms) {
@@ -1472,7 +1475,7 @@ int glide_vjp(glide_handle h, int level, double dt, void* stream) {
     });
 }
 
-int glide_jvp(glide_handle h, int level, double dt, int reference_rows, void* stream) {
+int glide_jvp(glide_handle h, int level, double dt, int reference_rows, int flags, void* stream) {
     return guarded([&] {
         dispatch(h, [&](auto& s) {
             s.check_level(level);
@@ -1480,7 +1483,9 @@ int glide_jvp(glide_handle h, int level, double dt, int reference_rows, void* st
             typename SolverT::Lin L = SolverT::tan_sys();
             L.x[0] = GLIDE_VAR_U; L.x[1] = GLIDE_VAR_V; L.x[2] = GLIDE_VAR_H;
             const int out[3] = {GLIDE_JVP_U, GLIDE_JVP_V, GLIDE_JVP_H};
-            s.lin_op(level, dt, L, out, nullptr, false, false, reference_rows != 0, S(stream));
+            if (flags & ~(GLIDE_USE_MASK | GLIDE_FREEZE_CALVING))
+                fail(GLIDE_ERR_ARG, "glide_jvp flags: only GLIDE_USE_MASK and GLIDE_FREEZE_CALVING apply");
+            s.lin_op(level, dt, L, out, nullptr, false, false, reference_rows != 0, S(stream), flags);
         });
     });
 }

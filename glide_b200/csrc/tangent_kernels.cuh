@@ -192,7 +192,10 @@ __device__ __forceinline__ void eta_and_dot(const S& s, R Bc, const PhysR<R>& p,
 // phi, bed, beta, B, e_H.
 template <class R>
 __global__ void __launch_bounds__(kTileA * kTileA)
-    k_jvp(VjpArgs<R> a, int ref_rows, const __grid_constant__ BoxMaps<JvpTile<R>::NB> maps) {
+    k_jvp(VjpArgs<R> a, int mode, const __grid_constant__ BoxMaps<JvpTile<R>::NB> maps) {
+    // mode bit 0: the reference's row conventions; bit 1: mask ignored
+    // (the reference's use_mask = False, which reads the mask as 0)
+    const bool ref_rows = (mode & 1) != 0, use_mask = (mode & 2) == 0;
     using TT = JvpTile<R>;
     constexpr int NC = TT::NC;
     __shared__ __align__(128) TT T;
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(kTileA * kTileA)
         ss += double(r) * double(r);
     };
     if (I < ny && J < nx) {
-        const R mk = a.mask.at(I, J);
+        const R mk = use_mask ? a.mask.at(I, J) : R(0);
         R dH = mass_jvp<R>(s, a.p, I, J);
         if (ref_rows) dH = (R(1) - mk) * dH;
         else if (mk > R(0.5)) dH = s.EH(I, J);

@@ -257,8 +257,9 @@ class Hierarchy:
     def vjp(self, level: int, dt: float):
         call("glide_vjp", self._h, int(level), float(dt), _stream_ptr())
 
-    def jvp(self, level: int, dt: float, reference_rows: bool = True):
-        call("glide_jvp", self._h, int(level), float(dt), int(bool(reference_rows)), _stream_ptr())
+    def jvp(self, level: int, dt: float, reference_rows: bool = True, flags: int = _lib.USE_MASK):
+        """flags: USE_MASK (the default) and FREEZE_CALVING, as glide_jvp."""
+        call("glide_jvp", self._h, int(level), float(dt), int(bool(reference_rows)), int(flags), _stream_ptr())
 
     def adjoint_sweep(self, level: int, dt: float, n: int):
         call("glide_adjoint_sweep", self._h, int(level), float(dt), int(n), _stream_ptr())

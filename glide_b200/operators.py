@@ -102,10 +102,14 @@ class ForwardOperators:
 
     def compute_jvp(self, dt, use_mask=True, freeze_calving=False, freeze_phi=False, return_norms=False):
         """jvp = J(x) var with the reference's row conventions
-        (glide/operators.py:129-171); phi is recomputed first unless frozen."""
+        (glide/operators.py:129-171); phi is recomputed first unless frozen.
+        use_mask=False reads the mask as 0 and freeze_calving=True sets the
+        calving rate to 0, as the reference does.  return_norms is accepted
+        and, as in the reference, nothing is returned."""
         if not freeze_phi:
             self.compute_phi()
-        self._h.jvp(self._l, dt, reference_rows=True)
+        flags = (_lib.USE_MASK if use_mask else 0) | (_lib.FREEZE_CALVING if freeze_calving else 0)
+        self._h.jvp(self._l, dt, reference_rows=True, flags=flags)
 
     def compute_residual(self, dt, use_mask=True, operator_only=False, freeze_calving=False,
                          freeze_phi=False, return_norms=False):

@@ -198,8 +198,11 @@ int glide_vjp(glide_handle h, int level, double dt, void* stream);
  * fixed.  reference_rows = 1 follows ForwardOperators.compute_jvp
  * (glide/operators.py:129-171, glide/cuda/residuals.cu:341-660): zero on the
  * Dirichlet faces, (1 - mask) times the mass rows.  reference_rows = 0 gives
- * the Jacobian the Newton iteration uses (identity rows there). */
-int glide_jvp(glide_handle h, int level, double dt, int reference_rows, void* stream);
+ * the Jacobian the Newton iteration uses (identity rows there).  flags are
+ * the reference's keyword arguments: GLIDE_USE_MASK (use_mask=True, its
+ * default; without it the mask reads as 0) and GLIDE_FREEZE_CALVING
+ * (freeze_calving=True: calving rate 0).  Any other flag is GLIDE_ERR_ARG. */
+int glide_jvp(glide_handle h, int level, double dt, int reference_rows, int flags, void* stream);
 int glide_adjoint_sweep(glide_handle h, int level, double dt, int n, void* stream);
 int glide_gradients(glide_handle h, int level, double dt, int grad_mask, void* stream);
 int glide_backward(glide_handle h, double dt, int start_level, int grad_mask, glide_stats* stats,

@@ -163,6 +163,30 @@ def random_cases(glide):
     np.savez_compressed(HERE / "random_adjoint_f64.npz", **out)
 
 
+def jvp_flag_cases(glide):
+    """ForwardOperators.compute_jvp (glide/operators.py:129-171) with its
+    use_mask and freeze_calving flags on the random state with a calving rate
+    of 2: the default flags, use_mask=False, and freeze_calving=True."""
+    st = random_state(40, 56, seed=7)
+    dt = 5.0
+    rng = np.random.default_rng(5)
+    ny, nx = st["H"].shape
+    var = dict(var_u=rng.normal(0, 1, (ny, nx + 1)), var_v=rng.normal(0, 1, (ny + 1, nx)),
+               var_H=rng.normal(0, 10, (ny, nx)))
+    out = {f"in_{k}": v for k, v in {**st, **var}.items()}
+    out["in_calving_rate"] = np.array(2.0)
+    for tag, kw in (("", {}), ("_nomask", dict(use_mask=False)), ("_frozen", dict(freeze_calving=True))):
+        g = random_grid(glide, st, calving=2.0)
+        ops = g.forward_operators
+        ops.set_rhs(dt)
+        for k, v in var.items():
+            getattr(ops, k)[:, :] = v
+        ops.compute_jvp(dt, **kw)
+        for k in ("jvp_u", "jvp_v", "jvp_H"):
+            out[f"out_{k}{tag}"] = np.array(getattr(ops, k))
+    np.savez_compressed(HERE / "random_jvp_flags_f64.npz", **out)
+
+
 def vanka_dump_case(glide):
     """ForwardOperators.vanka_dump (glide/operators.py:253-273) on the random
     state: the local 5x5 systems of every cell."""
@@ -302,8 +326,11 @@ def enthalpy_cases(glide):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", default=None, help="enthalpy | dump | transfers: only those fixtures")
+    ap.add_argument("--only", default=None, help="enthalpy | dump | transfers | jvp_flags: only those fixtures")
     a = ap.parse_args(argv)
+    if a.only == "jvp_flags":
+        jvp_flag_cases(load_reference(fp64=True, reference=a.reference))
+        return
     if a.only == "enthalpy":
         enthalpy_cases(load_reference(fp64=True, reference=a.reference))
         return
@@ -316,6 +343,7 @@ def main(argv=None):
     glide = load_reference(fp64=True, reference=a.reference)
     c1_forward_and_adjoint(glide, "f64")
     random_cases(glide)
+    jvp_flag_cases(glide)
     enthalpy_cases(glide)
     vanka_dump_case(glide)
     transfer_cases(glide)

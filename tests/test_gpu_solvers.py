@@ -48,6 +48,34 @@ def test_jvp_matches_reference():
         assert rel_err(_np(h.view(k, 0)), g[f"out_{k}"]) <= 1e-12, k
 
 
+@pytest.mark.parametrize("tag,kw", [("", {}), ("_nomask", dict(use_mask=False)),
+                                    ("_frozen", dict(freeze_calving=True))])
+def test_compute_jvp_flags_match_reference(tag, kw):
+    """ForwardOperators.compute_jvp's use_mask and freeze_calving, through
+    the reference-facing Grid API, against the reference's own compute_jvp
+    run with the same keywords (calving rate 2, so freezing it matters)."""
+    from glide_b200.grid import Grid
+    g = load_golden("random_jvp_flags_f64")
+    ny, nx = g["in_H"].shape
+    gr = Grid(ny, nx, 1500.0)
+    for k in ("u", "v", "H", "H_prev", "mask"):
+        getattr(gr.state, k).set(torch.as_tensor(g[f"in_{k}"]))
+    gr.geometry.bed.set(torch.as_tensor(g["in_bed"]))
+    gr.rheology.B.set(torch.as_tensor(g["in_B"]))
+    gr.sliding.beta.set(torch.as_tensor(g["in_beta"]))
+    gr.forcing.smb.set(torch.as_tensor(g["in_smb"]))
+    gr.calving.calving_rate.set(float(g["in_calving_rate"]))
+    ops = gr.forward_operators
+    ops.f_u[:, :] = torch.as_tensor(g["in_f_u"])
+    ops.f_v[:, :] = torch.as_tensor(g["in_f_v"])
+    ops.set_rhs(DT)
+    for k in ("var_u", "var_v", "var_H"):
+        getattr(ops, k)[:, :] = torch.as_tensor(g[f"in_{k}"])
+    assert ops.compute_jvp(DT, return_norms=True, **kw) is None
+    for k in ("jvp_u", "jvp_v", "jvp_H"):
+        assert rel_err(_np(getattr(ops, k)), g[f"out_{k}{tag}"]) <= 1e-12, (tag, k)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_jvp_tma_staging_equals_scalar_staging(precision):
     """The JVP's halo tiles staged by TMA bulk copies (edge tiles fixed up to
