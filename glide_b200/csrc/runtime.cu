@@ -212,6 +212,7 @@ struct Solver : SolverBase {
     std::vector<CUtensorMap> tmaps[3];
     std::vector<unsigned char> tmap_done[3];
     bool use_tma = true;
+    int tma_wait_polls = kTmaWaitPolls;  // 0 under GLIDE_TUNE_TMA_GIVE_UP
     // one captured V-cycle per cycle kind (0 FAS, 1 adjoint, 2 mixed FAS,
     // 3 mixed adjoint, 4 Newton), each valid for the (version, dt, start) it
     // was captured with, so that solves alternating kinds replay, not recapture
@@ -403,7 +404,12 @@ struct Solver : SolverBase {
         for (int q = 0; q < 4; ++q) out[q] = norms_host[q];
         int e;
         std::memcpy(&e, norms_host + 4, sizeof(int));
-        if (e) fail(GLIDE_ERR_TIMEOUT, "a kernel's bounded wait for its tile copies gave up");
+        if (e) {
+            // clear the word, so the next call on this handle starts clean
+            GCU(cudaMemsetAsync(err_dev, 0, sizeof(int), s));
+            GCU(cudaStreamSynchronize(s));
+            fail(GLIDE_ERR_TIMEOUT, "a kernel's bounded wait for its tile copies gave up");
+        }
     }
 
     // TMA staging needs a level at least one box wide and high
@@ -441,6 +447,7 @@ struct Solver : SolverBase {
     BoxMaps<N> box_maps(int l, const int (&fields)[N], int bh = kBoxH) {
         BoxMaps<N> m;
         m.use = tma_level(l, bh) ? 1 : 0;
+        m.wait_polls = tma_wait_polls;
         if (m.use)
             for (int q = 0; q < N; ++q) m.m[q] = tmap(l, fields[q], bh);
         return m;
@@ -673,6 +680,7 @@ struct Solver : SolverBase {
         f.sweep_blocks_per_sm = sweep_blocks_per_sm;
         f.use_graphs = 0;
         f.use_tma = use_tma;
+        f.tma_wait_polls = tma_wait_polls;
         f.err_dev = err_dev;  // shadow kernels report into this handle's error word
         f.launch_sink = &launches;  // and count into its launches (captured cycles included)
         for (int l = 0; l < n_levels; ++l) {
@@ -1365,6 +1373,9 @@ int glide_set_tuning(glide_handle h, int key, int value) {
             } else if (key == GLIDE_TUNE_TMA_STAGING) {
                 if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "TMA staging must be 0 or 1");
                 s.use_tma = value != 0;
+            } else if (key == GLIDE_TUNE_TMA_GIVE_UP) {
+                if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "TMA give-up must be 0 or 1");
+                s.tma_wait_polls = value ? 0 : kTmaWaitPolls;
             } else if (key == GLIDE_TUNE_REPORT_NOT_CONVERGED) {
                 if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "report-not-converged must be 0 or 1");
                 s.report_not_converged = value;

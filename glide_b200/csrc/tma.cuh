@@ -58,9 +58,12 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
     return ok != 0;
 }
 
-// Waits for the phase with the given parity; gives up after `limit` polls
-// (each poll itself suspends for a bounded, hardware-defined time).
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit = 1 << 22) {
+// Polls a staged-tile wait makes before it gives up (each poll itself
+// suspends for a bounded, hardware-defined time).
+constexpr int kTmaWaitPolls = 1 << 22;
+
+// Waits for the phase with the given parity; gives up after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit = kTmaWaitPolls) {
     for (int k = 0; k < limit; ++k)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
@@ -81,6 +84,10 @@ template <int N>
 struct BoxMaps {
     CUtensorMap m[N];
     int use;  // 0: stage with clamped scalar loads instead (small levels)
+    // polls of the first wait for the copies (kTmaWaitPolls unless a test
+    // lowers it to make that wait give up); the wait that lets copies still
+    // in flight land after a give-up always uses kTmaWaitPolls
+    int wait_polls = kTmaWaitPolls;
 };
 
 // Scalar staging of one array into the box layout, indices clamped.
@@ -137,7 +144,7 @@ __device__ __forceinline__ bool stage_boxes(BoxT<R, BH>* const (&dst)[N], const 
 #pragma unroll
         for (int q = 0; q < N; ++q) tma_load_2d(dst[q], &maps.m[q], j0 - kBoxX, i0 - BY, bar);
     }
-    const bool ok = __syncthreads_and(mbar_wait(bar, 0));
+    const bool ok = __syncthreads_and(mbar_wait(bar, 0, maps.wait_polls));
     if (!ok) {
         if (threadIdx.x == 0) atomicOr(err, 1);
         mbar_wait(bar, 0);  // let copies still in flight land before the block exits

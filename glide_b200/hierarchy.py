@@ -190,14 +190,17 @@ class Hierarchy:
     def set_tuning(self, sweep_blocks_per_sm: int | None = None, mixed_inner_vcycles: int | None = None,
                    forward_method: str | None = None, newton_switch_exp10: int | None = None,
                    tangent_vcycles: int | None = None, tma_staging: bool | None = None,
-                   report_not_converged: bool | None = None):
+                   report_not_converged: bool | None = None, tma_give_up: bool | None = None):
         """Solver knobs with no counterpart in the reference (see glide_set_tuning).
         forward_method: "fascd" (the reference's V-cycles only) or "newton"
         (FASCD until 10^-newton_switch_exp10, then Newton steps whose correction
         comes from the tangent linear multigrid).  report_not_converged: forward
         and backward raise NotConverged (with the solve's stats, after writing
         every output) when a solve stops at its cycle cap short of its
-        tolerances; off by default, as the reference reports nothing."""
+        tolerances; off by default, as the reference reports nothing.
+        tma_give_up: every stencil block's first wait for its staged tiles
+        gives up at once, so the call fails with GLIDE_ERR_TIMEOUT (a test of
+        that path; the blocks still let their copies land before returning)."""
         if sweep_blocks_per_sm is not None:
             call("glide_set_tuning", self._h, 1, int(sweep_blocks_per_sm))
         if mixed_inner_vcycles is not None:
@@ -212,6 +215,8 @@ class Hierarchy:
             call("glide_set_tuning", self._h, 6, int(bool(tma_staging)))
         if report_not_converged is not None:
             call("glide_set_tuning", self._h, 7, int(bool(report_not_converged)))
+        if tma_give_up is not None:
+            call("glide_set_tuning", self._h, 8, int(bool(tma_give_up)))
 
     def launch_count(self) -> int:
         c = ctypes.c_longlong()

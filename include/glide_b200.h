@@ -178,6 +178,13 @@ int glide_launch_count(glide_handle h, long long* count);
  * return GLIDE_ERR_NOT_CONVERGED when the solve ends short of its
  * tolerances; 0 (default) returns GLIDE_OK as the reference would. */
 #define GLIDE_TUNE_REPORT_NOT_CONVERGED 7
+/* GLIDE_TUNE_TMA_GIVE_UP: a stencil block's first wait for its staged tile
+ * copies polls at most 2^22 times, then gives up, sets the handle's error
+ * word and returns; the call fails with GLIDE_ERR_TIMEOUT at its next norm
+ * read, and the word is cleared when reported.  1 makes that first wait give
+ * up at once, which tests the path (the block still waits, bounded, for its
+ * copies to land before it returns); 0 restores the default. */
+#define GLIDE_TUNE_TMA_GIVE_UP 8
 int glide_set_tuning(glide_handle h, int key, int value);
 
 int glide_set_rhs(glide_handle h, int level, double dt, void* stream);
