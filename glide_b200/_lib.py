@@ -133,6 +133,7 @@ SIGNATURES = {
     "glide_set_reference_quirks": ([_H, _I], _I),
     "glide_set_use_graphs": ([_H, _I], _I),
     "glide_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], _I),
+    "glide_alg_bytes": ([_H, ctypes.POINTER(ctypes.c_double)], _I),
     "glide_set_tuning": ([_H, _I, _I], _I),
     "glide_set_rhs": ([_H, _I, _D, _P], _I),
     "glide_compute_phi": ([_H, _I, _D, _P], _I),
@@ -189,6 +190,7 @@ SIGNATURES.update({
     "glide_enthalpy_compute_omega": ([_H, _P, _I, _P, _I, _D, _D, _P], _I),
     "glide_enthalpy_frictional_heating": ([_H, _P, _I, _D, _D, _P], _I),
     "glide_enthalpy_arrhenius": ([_H, _D, _D, _P, _I, _P], _I),
+    "glide_enthalpy_counters": ([_H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)], _I),
 })
 
 

@@ -120,6 +120,15 @@ struct Handle {
     glide_enthalpy_config cfg;
     glide_enthalpy_inputs in;
     int point_blocks = 3;   // resident blocks per SM of the residual / layer kernels (3 to 6)
+    // Kernels launched and their algorithmic bytes: the binary64 values each
+    // must read and write once.  A residual, column or layer pass moves
+    // (5 nz + 7) values per column: E, E_prev, f_E, omega and the output at
+    // every level; H, H_prev, E_surface, u, v and two neighbour reads per
+    // column.  Sweeps skipped by the device-side stop test move nothing.
+    long long launches = 0;
+    double alg_bytes = 0;
+    void acct(long long n, double bytes) { launches += n; alg_bytes += bytes; }
+    double pass_bytes() const { return double(5 * nz + 7) * 8.0 * double(plane); }
     int column_blocks = 4;  // of the column kernel (2 to 6)
 
     Handle(int ny_, int nx_, int nz_, double dx_) : ny(ny_), nx(nx_), nz(nz_), dx(dx_) {
@@ -350,6 +359,7 @@ int glide_enthalpy_snapshot(glide_enthalpy_handle h, void* stream) {
         k_enth_snapshot<<<1184, 256, 0, S(stream)>>>(e->f[GLIDE_ENTH_E_PREV], e->f[GLIDE_ENTH_E], e->n3,
                                                      e->f[GLIDE_ENTH_H_PREV], e->in.H, e->in.ld_H, e->ny, e->nx);
         check_launch("enthalpy snapshot");
+        e->acct(1, 16.0 * (double(e->n3) + double(e->plane)));  // E -> E_prev, H -> H_prev
     });
 }
 
@@ -362,6 +372,7 @@ int glide_enthalpy_set_rhs(glide_enthalpy_handle h, void* stream) {
             a, e->f[GLIDE_ENTH_F_E], e->f[GLIDE_ENTH_PHI_STRAIN], e->f[GLIDE_ENTH_Q_GEO], e->f[GLIDE_ENTH_Q_FH],
             e_scale);
         check_launch("enthalpy set_rhs");
+        e->acct(1, 8.0 * (2.0 * double(e->n3) + 2.0 * double(e->plane)));  // strain heating, Q_geo, Q_fh in; f_E out
     });
 }
 
@@ -371,7 +382,9 @@ int glide_enthalpy_residual(glide_enthalpy_handle h, double dt, int use_forcing,
         if (!(dt > 0)) fail(GLIDE_ERR_ARG, "dt must be positive");
         EnthArgs a = e->args(dt, e->f[GLIDE_ENTH_E], false);
         e->residual(a, use_forcing, S(stream));
+        e->acct(1, e->pass_bytes());
         if (max_abs) {
+            e->acct(1, 8.0 * e->nblocks);
             e->finish(2, S(stream));
             e->read_ctl(S(stream));
             *max_abs = e->ctl_host->last;
@@ -385,6 +398,7 @@ int glide_enthalpy_column_smooth(glide_enthalpy_handle h, double dt, void* strea
         if (!(dt > 0)) fail(GLIDE_ERR_ARG, "dt must be positive");
         EnthArgs a = e->args(dt, e->f[GLIDE_ENTH_E], false);
         e->column(a, e->f[GLIDE_ENTH_DELTA_E], 0, S(stream));
+        e->acct(1, e->pass_bytes());
     });
 }
 
@@ -394,6 +408,7 @@ int glide_enthalpy_layer_smooth(glide_enthalpy_handle h, double dt, void* stream
         if (!(dt > 0)) fail(GLIDE_ERR_ARG, "dt must be positive");
         EnthArgs a = e->args(dt, e->f[GLIDE_ENTH_E], false);
         e->layer(a, e->f[GLIDE_ENTH_DELTA_E], 0, S(stream));
+        e->acct(1, e->pass_bytes());
     });
 }
 
@@ -425,6 +440,9 @@ int glide_enthalpy_column_sweep(glide_enthalpy_handle h, double dt, int n_iter, 
         }
         e->read_ctl(s);
         const SweepCtl& c = *e->ctl_host;
+        // every launch counts; bytes only for the sweeps that ran (later
+        // launches see the stop flag and return at once)
+        e->acct(2 + 3LL * n_iter, e->pass_bytes() * (1.0 + 3.0 * c.iters) + 8.0 * e->nblocks * (1.0 + c.iters));
         if (stats) {
             stats->iterations = c.iters;
             stats->initial_norm = c.r0;
@@ -446,6 +464,7 @@ int glide_enthalpy_compute_omega(glide_enthalpy_handle h, const double* dh_dt, i
         k_enth_omega<<<e->col_grid(), kColThreads, 0, S(stream)>>>(a, e->f[GLIDE_ENTH_OMEGA], dh_dt, ld_dh, bmb,
                                                                   ld_bmb, dh_div, omega_div);
         check_launch("enthalpy omega");
+        e->acct(1, 8.0 * (double(e->n3) + 4.0 * double(e->plane)));  // u, v, H, dH/dt in; omega out
     });
 }
 
@@ -458,6 +477,7 @@ int glide_enthalpy_frictional_heating(glide_enthalpy_handle h, const double* bet
         k_enth_friction<<<e->col_grid(), kColThreads, 0, S(stream)>>>(a, e->f[GLIDE_ENTH_Q_FH], beta, ld_beta, m,
                                                                      u_reg);
         check_launch("enthalpy frictional heating");
+        e->acct(1, 8.0 * 4.0 * double(e->plane));  // beta, u, v in; Q_fh out
     });
 }
 
@@ -470,6 +490,15 @@ int glide_enthalpy_arrhenius(glide_enthalpy_handle h, double n_glen, double scal
         EnthArgs a = e->args(1.0, e->f[GLIDE_ENTH_E], false);
         k_enth_arrhenius<<<e->col_grid(), kColThreads, 0, S(stream)>>>(a, B, ld_B, n_glen, scale);
         check_launch("enthalpy arrhenius");
+        e->acct(1, 8.0 * (double(e->n3) + 2.0 * double(e->plane)));  // E, H in; B out
+    });
+}
+
+int glide_enthalpy_counters(glide_enthalpy_handle h, long long* launches, double* alg_bytes) {
+    return guarded([&] {
+        Handle* e = H(h);
+        if (launches) *launches = e->launches;
+        if (alg_bytes) *alg_bytes = e->alg_bytes;
     });
 }
 

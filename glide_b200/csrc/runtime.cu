@@ -223,22 +223,37 @@ struct Solver : SolverBase {
         double dt = 0;
         int start = -1;
         long long launches = 0;  // kernels inside the graph
+        double bytes = 0;        // their algorithmic bytes
     };
     CachedGraph graphs[kKinds];
     cudaStream_t own_stream = nullptr;
     long long launches = 0;        // kernels issued by this handle (graph replays included)
     long long* launch_sink = nullptr;  // a binary32 shadow also counts into its handle's solver
+    // Algorithmic bytes of those kernels: the values each must read and write
+    // once (N = cells of the level, face arrays counted as N, s = value size).
+    double alg_bytes = 0;
+    double* bytes_sink = nullptr;
     long long newton_rejects = 0;  // Newton steps undone by the growth guard
     int report_not_converged = 0;  // GLIDE_TUNE_REPORT_NOT_CONVERGED
     bool last_not_converged = false;  // the last solve_loop ended short of its tolerances
     double last_relative = 0.0;
     int last_cycles = 0;
 
-    void counted(const char* what) {
+    void counted(const char* what, double bytes) {
         check_launch(what);
         ++launches;
         if (launch_sink) ++*launch_sink;
+        traffic(bytes);
     }
+
+    // bytes moved without a kernel of ours (device-to-device copies)
+    void traffic(double bytes) {
+        alg_bytes += bytes;
+        if (bytes_sink) *bytes_sink += bytes;
+    }
+
+    // `arrays` values per cell of level l
+    double lb(int l, double arrays) const { return arrays * double(lv[l].ny) * double(lv[l].nx) * sizeof(R); }
 
     Solver(int ny, int nx, double dx, int L) {
         dtype = sizeof(R) == 8 ? GLIDE_F64 : GLIDE_F32;
@@ -306,12 +321,13 @@ struct Solver : SolverBase {
 
     void fill(const Arr<R>& a, R val, cudaStream_t s) {
         k_fill<R><<<pw_grid(a.rows, a.cols), 256, 0, s>>>(a, val, a.rows, a.cols);
-        counted("fill");
+        counted("fill", double(a.rows) * a.cols * sizeof(R));
     }
 
     void copy(const Arr<R>& dst, const Arr<R>& src, cudaStream_t s) {
         GCU(cudaMemcpy2DAsync(dst.p, size_t(dst.pitch) * sizeof(R), src.p, size_t(src.pitch) * sizeof(R),
                               size_t(src.cols) * sizeof(R), src.rows, cudaMemcpyDeviceToDevice, s));
+        traffic(2.0 * src.rows * src.cols * sizeof(R));
     }
 
     void restrict_field(int f, int l, cudaStream_t s, Arr<R> copy_to = Arr<R>()) {
@@ -328,7 +344,14 @@ struct Solver : SolverBase {
         else if (fa.rows == lv[l].ny + 1) kind = kFaceV;
         else kind = cell_kind >= 0 ? cell_kind : kCellAvg;
         k_restrict<R><<<pw_grid(C.ny + 1, C.nx + 1), 256, 0, s>>>(fa, ca, copy_to, kind, C.ny, C.nx);
-        counted("restrict");
+        counted("restrict", restrict_bytes(l, kind, copy_to.p != nullptr));
+    }
+
+    // one restriction into level l + 1: 2 fine faces or 4 fine cells read
+    // per coarse value, the coarse value written (and its copy)
+    double restrict_bytes(int l, int kind, bool copy) const {
+        const double per = (kind == kFaceU || kind == kFaceV) ? 3.0 : 5.0;
+        return lb(l + 1, per + (copy ? 1.0 : 0.0));
     }
 
     PhysR<R> physr(int l, double dt, bool freeze_calving) const {
@@ -343,14 +366,14 @@ struct Solver : SolverBase {
         Level<R>& v = lv[l];
         k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_PHI], v.a[GLIDE_H], v.a[GLIDE_BED],
                                                           R(v.phys.flotation_reg_driving), R(relax), v.ny, v.nx);
-        counted("grounded");
+        counted("grounded", lb(l, 4));  // H, bed, phi read; phi written
     }
 
     void set_rhs(int l, double dt, cudaStream_t s) {
         Level<R>& v = lv[l];
         k_set_rhs<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_F_H], v.a[GLIDE_H_PREV], v.a[GLIDE_SMB],
                                                          R(dt), v.ny, v.nx);
-        counted("set_rhs");
+        counted("set_rhs", lb(l, 3));
     }
 
     // residual into (o_*) = R(x) [- f] [- sub]; norms into norms_dev when asked
@@ -374,10 +397,12 @@ struct Solver : SolverBase {
         a.active_set = active_set ? 1 : 0;
         dim3 g(v.blocks_x(), v.blocks_y());
         k_residual<R><<<g, 256, 0, s>>>(a, box_maps(l, kStateBoxes));
-        counted("residual");
+        // u, v, H, phi, mask, bed, B, beta, gamma; forcing; subtrahend; 3 rows
+        // written (and the active set)
+        counted("residual", lb(l, 9 + (use_forcing ? 3 : 0) + (sub ? 3 : 0) + 3 + (active_set ? 1 : 0)));
         if (norms) {
             k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
-            counted("finish_norms");
+            counted("finish_norms", 24.0 * g.x * g.y + 32.0);
         }
     }
 
@@ -394,7 +419,7 @@ struct Solver : SolverBase {
         a.ny = v.ny; a.nx = v.nx;
         a.use_forcing = 1; a.use_mask = 0; a.active_set = 0;
         k_vanka_dump<R><<<dim3(v.blocks_x(), v.blocks_y()), 256, 0, s>>>(a, J, r);
-        counted("vanka_dump");
+        counted("vanka_dump", lb(l, 11 + 30));
     }
 
     // the norm vector and, in the same copy, the error word behind it
@@ -492,9 +517,9 @@ struct Solver : SolverBase {
                 k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_PHI], v.a[ih], v.a[GLIDE_BED],
                                                                   R(v.phys.flotation_reg_driving), R(c.relax_phi),
                                                                   v.ny, v.nx);
-                counted("grounded");
+                counted("grounded", lb(l, 4));
             }
-            launch_sweep(a, gmode, phi_live, g, s);
+            launch_sweep(a, gmode, phi_live, g, s, lb(l, 15));
         }
     }
 
@@ -507,10 +532,12 @@ struct Solver : SolverBase {
 #undef GLIDE_SWEEP
     }
 
-    void launch_sweep(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s) {
+    // one fused sweep: u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, phi read;
+    // u, v, H, mask written (15 N s)
+    void launch_sweep(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s, double bytes) {
         if (sweep_blocks_per_sm >= 2) launch_sweep_occ<2>(a, gmode, phi_live, g, s);
         else launch_sweep_occ<1>(a, gmode, phi_live, g, s);
-        counted("vanka_sweep");
+        counted("vanka_sweep", bytes);
     }
 
     // Restrictions of several fields of level l in one launch; each job is
@@ -536,7 +563,9 @@ struct Solver : SolverBase {
         dim3 g = pw_grid(C.ny + 1, C.nx + 1);
         g.z = n;
         k_restrict_batch<R><<<g, 256, 0, s>>>(b);
-        counted("restrict_batch");
+        double bytes = 0;
+        for (int q = 0; q < n; ++q) bytes += restrict_bytes(l, b.kind[q], jobs[q].copy_to >= 0);
+        counted("restrict_batch", bytes);
     }
 
     // the u, v and H corrections of level l (fields x, snapshots w, kinds k)
@@ -552,7 +581,8 @@ struct Solver : SolverBase {
         dim3 g = pw_grid(F.ny + 1, F.nx + 1);
         g.z = 3;
         k_correct_batch<R><<<g, 256, 0, s>>>(b);
-        counted("correct_batch");
+        // per field: fine x and w read, x written; coarse x and w read
+        counted("correct_batch", 3 * (lb(l, 3) + lb(l + 1, 2)));
     }
 
 
@@ -567,7 +597,7 @@ struct Solver : SolverBase {
             k_snapshot<R><<<pw_grid(v.ny + 1, v.nx + 1), 256, 0, s>>>(
                 v.a[GLIDE_U], v.a[GLIDE_V], v.a[GLIDE_H], v.a[F_W_U], v.a[F_W_V], v.a[F_W_H], v.a[F_CHI],
                 R(v.phys.thklim), v.ny, v.nx);
-            counted("snapshot");
+            counted("snapshot", lb(l, 7));  // u, v, H read; w_u, w_v, w_H, chi written
         }
         if (l == n_levels - 1) {
             sweeps(l, dt, c.coarsest_steps, kGammaWChi, fcal, fphi, nullptr, s);
@@ -635,6 +665,7 @@ struct Solver : SolverBase {
             if (cg.exec) { cudaGraphExecDestroy(cg.exec); cg.exec = nullptr; }
             cudaGraph_t g;
             const long long before = launches;
+            const double bytes_before = alg_bytes;
             GCU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             try {
                 body();
@@ -642,10 +673,13 @@ struct Solver : SolverBase {
                 cudaStreamEndCapture(s, &g);
                 if (g) cudaGraphDestroy(g);
                 launches = before;
+                alg_bytes = bytes_before;
                 throw;
             }
             cg.launches = launches - before;
+            cg.bytes = alg_bytes - bytes_before;
             launches = before;
+            alg_bytes = bytes_before;
             GCU(cudaStreamEndCapture(s, &g));
             cudaError_t e = cudaGraphInstantiate(&cg.exec, g, 0);
             cudaGraphDestroy(g);
@@ -654,6 +688,7 @@ struct Solver : SolverBase {
         }
         GCU(cudaGraphLaunch(cg.exec, s));
         launches += cg.launches;
+        alg_bytes += cg.bytes;
     }
 
     // ------------------------------------------------ mixed precision
@@ -670,7 +705,7 @@ struct Solver : SolverBase {
     template <class D, class Src>
     void convert(const Arr<D>& d, const Arr<Src>& src, double scale, cudaStream_t s) {
         k_convert<D, Src><<<pw_grid(src.rows, src.cols), 256, 0, s>>>(d, src, scale, src.rows, src.cols);
-        counted("convert");
+        counted("convert", double(src.rows) * src.cols * (sizeof(D) + sizeof(Src)));
     }
 
     void sync_shadow() {
@@ -683,6 +718,7 @@ struct Solver : SolverBase {
         f.tma_wait_polls = tma_wait_polls;
         f.err_dev = err_dev;  // shadow kernels report into this handle's error word
         f.launch_sink = &launches;  // and count into its launches (captured cycles included)
+        f.bytes_sink = &alg_bytes;
         for (int l = 0; l < n_levels; ++l) {
             if (f.lv[l].phys.thklim != lv[l].phys.thklim)
                 f.fill(f.lv[l].a[GLIDE_GAMMA], float(lv[l].phys.thklim), nullptr);
@@ -714,7 +750,9 @@ struct Solver : SolverBase {
         k_defect_update<R, float><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
             D.a[GLIDE_U], D.a[GLIDE_V], D.a[GLIDE_H], D.a[GLIDE_MASK], D.a[GLIDE_GAMMA], F.a[GLIDE_U],
             F.a[GLIDE_V], F.a[GLIDE_H], F.a[GLIDE_MASK], D.ny, D.nx);
-        counted("defect_update");
+        // binary64 u, v, H, mask, gamma read and u, v, H, mask written;
+        // binary32 u, v, H, mask read
+        counted("defect_update", lb(l, 9) + double(D.ny) * D.nx * 4 * sizeof(float));
         residual(l, dt, true, true, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
     }
 
@@ -737,7 +775,7 @@ struct Solver : SolverBase {
     template <class Src>
     void convert_add(const Arr<R>& d, const Arr<Src>& src, cudaStream_t s) {
         k_add_converted<R, Src><<<pw_grid(src.rows, src.cols), 256, 0, s>>>(d, src, src.rows, src.cols);
-        counted("add_converted");
+        counted("add_converted", double(src.rows) * src.cols * (2 * sizeof(R) + sizeof(Src)));
     }
 
     void forward_mixed(double dt, int start, glide_stats* st, cudaStream_t s) {
@@ -913,21 +951,24 @@ struct Solver : SolverBase {
         a.p = physr(l, dt, !L.tr && (jvp_flags & GLIDE_FREEZE_CALVING));
         a.ny = v.ny; a.nx = v.nx; a.use_forcing = use_forcing;
         dim3 g((a.nx + kTileA - 1) / kTileA, (a.ny + kTileA - 1) / kTileA);
+        // u, v, H, phi, mask, bed, beta, B and the three unknowns read, the
+        // forcing and the subtrahend when given, three rows written
+        const double lin_bytes = lb(l, 11 + (use_forcing ? 3 : 0) + (sub ? 3 : 0) + 3);
         if (L.tr) {
             const int fl[AdjTile<R>::NB] = {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_BED, GLIDE_BETA,
                                             GLIDE_B, L.x[0], L.x[1]};
             k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a, box_maps(l, fl, AdjTile<R>::BH));
-            counted("vjp");
+            counted("vjp", lin_bytes);
         } else {
             const int fl[JvpTile<R>::NB] = {GLIDE_U, GLIDE_V, L.x[0], L.x[1], GLIDE_H, GLIDE_PHI, GLIDE_BED,
                                             GLIDE_BETA, GLIDE_B, L.x[2]};
             const int mode = (ref_rows ? 1 : 0) | ((jvp_flags & GLIDE_USE_MASK) ? 0 : 2);
             k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, mode, box_maps(l, fl));
-            counted("jvp");
+            counted("jvp", lin_bytes);
         }
         if (norms) {
             k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
-            counted("finish_norms");
+            counted("finish_norms", 24.0 * g.x * g.y + 32.0);
         }
     }
 
@@ -979,7 +1020,7 @@ struct Solver : SolverBase {
         const BoxMaps<7> m = box_maps(l, kStateBoxes);
         if (L.tr) k_block_factor<R, true><<<g, kTile * kTile, 0, s>>>(a, m);
         else k_block_factor<R, false><<<g, kTile * kTile, 0, s>>>(a, m);
-        counted("block_factor");
+        counted("block_factor", lb(l, 9 + 25));  // state read, 25 factor planes written
     }
 
     // n linear smoother sweeps (residual, then block solve and update); the
@@ -993,7 +1034,7 @@ struct Solver : SolverBase {
             lin_residual(l, dt, L, false, s);
             if (L.tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
             else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
-            counted("linear_sweep");
+            counted("linear_sweep", lb(l, 34));  // 25 factors, r, x read; x written
         }
     }
 
@@ -1054,13 +1095,13 @@ struct Solver : SolverBase {
         k_tangent_rhs<T, R><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
             F.a[F_TF_U], F.a[F_TF_V], F.a[F_TF_H], D.a[GLIDE_R_U], D.a[GLIDE_R_V], D.a[GLIDE_R_H], D.a[GLIDE_H],
             D.a[GLIDE_GAMMA], D.a[GLIDE_MASK], D.ny, D.nx);
-        counted("tangent_rhs");
+        counted("tangent_rhs", double(D.ny) * D.nx * (6 * sizeof(R) + 3 * sizeof(T)));
         for (int fld : {F_E_U, F_E_V, F_E_H}) ts.fill(F.a[fld], T(0), s);
         for (int k = 0; k < tangent_vcycles; ++k) ts.lin_vcycle(l, true, dt, Solver<T>::tan_sys(), s);
         k_newton_update<R, T><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
             D.a[GLIDE_U], D.a[GLIDE_V], D.a[GLIDE_H], D.a[GLIDE_GAMMA], F.a[F_E_U], F.a[F_E_V], F.a[F_E_H],
             D.ny, D.nx);
-        counted("newton_update");
+        counted("newton_update", double(D.ny) * D.nx * (7 * sizeof(R) + 3 * sizeof(T)));
         residual(l, dt, true, false, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s, true);
     }
 
@@ -1108,7 +1149,7 @@ struct Solver : SolverBase {
         a.dt = R(dt);
         a.ny = v.ny; a.nx = v.nx;
         k_gradients<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(a);
-        counted("gradients");
+        counted("gradients", lb(l, 9 + __builtin_popcount(unsigned(mask) & 15u)));
     }
 };
 
@@ -1525,6 +1566,13 @@ int glide_launch_count(glide_handle h, long long* count) {
     return guarded([&] {
         if (!count) fail(GLIDE_ERR_ARG, "null count");
         dispatch(h, [&](auto& s) { *count = s.launches; });
+    });
+}
+
+int glide_alg_bytes(glide_handle h, double* bytes) {
+    return guarded([&] {
+        if (!bytes) fail(GLIDE_ERR_ARG, "null output");
+        dispatch(h, [&](auto& s) { *bytes = s.alg_bytes; });
     });
 }
 

@@ -262,6 +262,13 @@ class EnthalpyOperators:
         if column_prefers_l1 is not None:
             _ecall("glide_enthalpy_set_tuning", self._h, 3, int(bool(column_prefers_l1)))
 
+    def counters(self):
+        """(kernels launched, their algorithmic bytes) so far on this
+        handle (glide_enthalpy_counters; instrumentation)."""
+        n, b = ctypes.c_longlong(), ctypes.c_double()
+        _ecall("glide_enthalpy_counters", self._h, ctypes.byref(n), ctypes.byref(b))
+        return n.value, b.value
+
     def _materialize_velocity(self):
         if not self._broadcast:
             return

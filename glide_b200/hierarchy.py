@@ -223,6 +223,12 @@ class Hierarchy:
         call("glide_launch_count", self._h, ctypes.byref(c))
         return c.value
 
+    def alg_bytes(self) -> float:
+        """Algorithmic bytes of every kernel launched so far (glide_alg_bytes)."""
+        c = ctypes.c_double()
+        call("glide_alg_bytes", self._h, ctypes.byref(c))
+        return c.value
+
     # -- operators -----------------------------------------------------
     def set_rhs(self, level: int, dt: float):
         call("glide_set_rhs", self._h, int(level), float(dt), _stream_ptr())

@@ -155,6 +155,12 @@ int glide_set_use_graphs(glide_handle h, int use_graphs);
  * every kernel node; a GLIDE_MIXED handle's binary32 kernels included).
  * No counterpart in the reference: instrumentation. */
 int glide_launch_count(glide_handle h, long long* count);
+/* Algorithmic bytes of those kernels so far: for each launch, the values its
+ * kernel must read and write once (N values per array of a level, face arrays
+ * counted as N), plus the handle's device-to-device copies.  Divided by a
+ * time it gives the achieved HBM bandwidth of a whole solve.  No counterpart
+ * in the reference: instrumentation. */
+int glide_alg_bytes(glide_handle h, double* bytes);
 /* Kernel tuning knobs (no counterpart in the reference).
  * GLIDE_TUNE_SWEEP_BLOCKS_PER_SM: 1 or 2 resident Vanka-sweep blocks per SM.
  * GLIDE_TUNE_MIXED_INNER_VCYCLES: binary32 V-cycles per defect correction

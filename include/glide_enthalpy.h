@@ -145,6 +145,11 @@ int glide_enthalpy_frictional_heating(glide_enthalpy_handle h, const double* bet
 /* B (ny, nx, leading dimension ld_B) = mean_k(A(T, water))^(-1/n_glen) / scale. */
 int glide_enthalpy_arrhenius(glide_enthalpy_handle h, double n_glen, double scale, double* B, int ld_B,
                              void* stream);
+/* Kernels this handle has launched so far, and their algorithmic bytes (the
+ * binary64 values each must read and write once; column-sweep passes skipped
+ * by the stop test count as launches but move no bytes).  Either pointer may
+ * be NULL.  No counterpart in the reference: instrumentation. */
+int glide_enthalpy_counters(glide_enthalpy_handle h, long long* launches, double* alg_bytes);
 
 #ifdef __cplusplus
 }

@@ -122,37 +122,77 @@ def arrhenius_B(E, H, nz, n_glen=3.0):
     return np.mean(A, axis=2) ** (-1.0 / n_glen)
 
 
+def _cfg(dx, dt):
+    """EnthalpyOperators' default term and smoother settings
+    (glide/enthalpy.py:205-300)."""
+    return dict(dx=dx, dt=dt, drain_rate=0.01 / SEC_PER_YR, h_thin=25.0, lf_c=1e-12, term_flags=7, omega=1.0,
+                n_newton=3, relaxation=1.0, relative_tolerance=1e-5, absolute_tolerance=1e-2)
+
+
+class OracleThermal:
+    """ThermalModel (glide/model.py:97-222) over the restated kernels, with
+    state kept between steps: initialize, pre_momentum, step."""
+
+    def __init__(self, dx, nz, n_smooth=10, m=1.0, u_reg=1.0, rho_i=917.0, n_glen=3.0):
+        self.dx, self.nz, self.n_smooth = dx, nz, n_smooth
+        self.m, self.u_reg, self.rho_i, self.n_glen = m, u_reg, rho_i, n_glen
+        self.sigma = np.linspace(0.0, 1.0, nz)
+
+    def set_surface_temperature(self, T_s):
+        """set_surface_enthalpy_from_temperature (glide/enthalpy.py:521-530)."""
+        self.E_s = 2009.0 * (np.minimum(T_s, 273.15) - 223.15) / E_SCALE_HOST
+
+    def initialize(self, T_s, H, Q_geo):
+        """ThermalModel.initialize (glide/model.py:134-153) with T_field =
+        T_surface, capped at the pressure-melting point of each level."""
+        ny, nx = H.shape
+        T = np.broadcast_to(T_s[:, :, None], (ny, nx, self.nz)).copy()
+        for k in range(self.nz):
+            T_pmp = 273.15 - 7.9e-8 * 910.0 * 9.81 * ((1.0 - float(self.sigma[k])) * H)
+            T[:, :, k] = np.minimum(T[:, :, k], T_pmp)
+        self.E = 2009.0 * (T - 223.15) / E_SCALE_HOST
+        self.E_prev, self.H_prev = self.E.copy(), H.copy()
+        self.set_surface_temperature(T_s)
+        self.Q_geo = Q_geo
+
+    def pre_momentum(self, H):
+        """glide/model.py:155-164."""
+        self.E_prev = self.E.copy()
+        self.H_prev = H.copy()
+
+    def step(self, u, v, H1, beta, dt):
+        """ThermalModel.step (glide/model.py:166-222): omega from the realised
+        thickness change in m/a, the velocity in m/s, frictional heating,
+        forcing, column sweeps; returns B in the momentum solver's units."""
+        ny, nx = H1.shape
+        nz = self.nz
+        u3 = np.ascontiguousarray(np.broadcast_to(u, (nz,) + u.shape))
+        v3 = np.ascontiguousarray(np.broadcast_to(v, (nz,) + v.shape))
+        dt_yr = dt / SEC_PER_YR
+        omega = compute_omega(u3, v3, H1, (H1 - self.H_prev) / dt_yr, np.zeros((ny, nx)), self.dx) / SEC_PER_YR
+        u3 = u3 / SEC_PER_YR
+        v3 = v3 / SEC_PER_YR
+        uc = 0.5 * (u3[0][:, 1:] + u3[0][:, :-1])
+        vc = 0.5 * (v3[0][1:, :] + v3[0][:-1, :])
+        self.Q_fh = beta * np.sqrt(uc ** 2 + vc ** 2 + self.u_reg ** 2) ** (self.m + 1.0)
+        dsig_half = 0.5 * (1.0 / (nz - 1))
+        f_E = np.zeros((ny, nx, nz))
+        f_E[:, :, 0] += (self.Q_geo + self.Q_fh) / (dsig_half * E_SCALE_HOST)
+        st = dict(E=self.E, E_prev=self.E_prev, f_E=f_E, u3d=u3, v3d=v3, omega=np.ascontiguousarray(omega), H=H1,
+                  H_prev=self.H_prev, E_surface=self.E_s)
+        self.sweep_norms = column_sweep(st, _cfg(self.dx, dt), self.n_smooth)
+        self.E = st["E"]
+        self.omega = omega
+        return arrhenius_B(self.E, H1, nz, self.n_glen) / (self.rho_i * 9.81 * SEC_PER_YR ** (1.0 / self.n_glen))
+
+
 def thermal_step(u, v, H0, H1, beta, T_s, Q_geo, dx, nz, n_smooth, dt, m=1.0, u_reg=1.0, rho_i=917.0,
                  n_glen=3.0):
     """ThermalModel initialize -> pre_momentum -> (H0 becomes H1) -> step(dt)
     (glide/model.py:134-222), with the restated kernels; returns E, omega,
     Q_fh, B, T in the reference's layouts."""
-    ny, nx = H0.shape
-    sigma = np.linspace(0.0, 1.0, nz)
-    T = np.broadcast_to(T_s[:, :, None], (ny, nx, nz)).copy()
-    for k in range(nz):
-        T_pmp = 273.15 - 7.9e-8 * 910.0 * 9.81 * ((1.0 - float(sigma[k])) * H0)
-        T[:, :, k] = np.minimum(T[:, :, k], T_pmp)
-    E = 2009.0 * (T - 223.15) / E_SCALE_HOST
-    E_s = 2009.0 * (np.minimum(T_s, 273.15) - 223.15) / E_SCALE_HOST
-    E_prev, H_prev = E.copy(), H0.copy()
-    # omega from the realised thickness change, in m/a, then m/s
-    u3 = np.ascontiguousarray(np.broadcast_to(u, (nz,) + u.shape))
-    v3 = np.ascontiguousarray(np.broadcast_to(v, (nz,) + v.shape))
-    dt_yr = dt / SEC_PER_YR
-    omega = compute_omega(u3, v3, H1, (H1 - H_prev) / dt_yr, np.zeros((ny, nx)), dx) / SEC_PER_YR
-    u3 = u3 / SEC_PER_YR
-    v3 = v3 / SEC_PER_YR
-    uc = 0.5 * (u3[0][:, 1:] + u3[0][:, :-1])
-    vc = 0.5 * (v3[0][1:, :] + v3[0][:-1, :])
-    Q_fh = beta * np.sqrt(uc ** 2 + vc ** 2 + u_reg ** 2) ** (m + 1.0)
-    dsig_half = 0.5 * (1.0 / (nz - 1))
-    f_E = np.zeros((ny, nx, nz))
-    f_E[:, :, 0] += (Q_geo + Q_fh) / (dsig_half * E_SCALE_HOST)
-    s = dict(E=E, E_prev=E_prev, f_E=f_E, u3d=u3, v3d=v3, omega=np.ascontiguousarray(omega), H=H1,
-             H_prev=H_prev, E_surface=E_s)
-    cfg = dict(dx=dx, dt=dt, drain_rate=0.01 / SEC_PER_YR, h_thin=25.0, lf_c=1e-12, term_flags=7, omega=1.0,
-               n_newton=3, relaxation=1.0, relative_tolerance=1e-5, absolute_tolerance=1e-2)
-    column_sweep(s, cfg, n_smooth)
-    B = arrhenius_B(s["E"], H1, nz, n_glen) / (rho_i * 9.81 * SEC_PER_YR ** (1.0 / n_glen))
-    return dict(E=s["E"], omega=omega, Q_fh=Q_fh, B=B, T=temperature(s["E"], H1, nz))
+    tm = OracleThermal(dx, nz, n_smooth, m=m, u_reg=u_reg, rho_i=rho_i, n_glen=n_glen)
+    tm.initialize(T_s, H0, Q_geo)
+    tm.pre_momentum(H0)
+    B = tm.step(u, v, H1, beta, dt)
+    return dict(E=tm.E, omega=tm.omega, Q_fh=tm.Q_fh, B=B, T=temperature(tm.E, H1, nz))

@@ -115,3 +115,83 @@ def enthalpy_config(**kw):
                relative_tolerance=1e-5, absolute_tolerance=1e-2)
     cfg.update(kw)
     return cfg
+
+
+def surface_temperature(H, bed):
+    """The large thermomechanical run's surface temperature in K:
+    -30 + 6e-3 (2000 - s) C with s = max(bed + H, (1 - 0.917) H).  Works on
+    torch tensors and NumPy arrays alike (same operations in the same order)."""
+    if isinstance(H, np.ndarray):
+        s = np.maximum(bed + H, (1.0 - 0.917) * H)
+    else:
+        import torch
+        s = torch.maximum(bed + H, (1.0 - 0.917) * H)
+    return 273.15 + (-30.0 + 6e-3 * (2000.0 - s))
+
+
+def configure_fast(h, mixed_inner=2):
+    """The bench's fast solver form on a Hierarchy handle: corrected
+    transfers, FASCD 4/4/0/50 with the local Newton capped at 3 iterations,
+    guarded Newton from the first cycle with a 4/4/0/10 tangent multigrid."""
+    h.set_reference_quirks(False)
+    h.set_fas(False, pre_steps=4, post_steps=4, finest_steps=0, coarsest_steps=50)
+    h.set_vanka(False, -1, newton_steps=3)
+    h.set_tuning(forward_method="newton", newton_switch_exp10=0, mixed_inner_vcycles=mixed_inner)
+    h.set_fas(2, pre_steps=4, post_steps=4, finest_steps=0, coarsest_steps=10)
+
+
+class CoupledRun:
+    """Coupled thermomechanical time steps through the public API, in the
+    order of the reference's coupled example
+    (examples/thermal/coupled_dome.py:258-272): ThermalModel.pre_momentum,
+    IceDynamics.forward, the surface enthalpy from the new geometry,
+    ThermalModel.step (which feeds B back into the finest grid).
+
+    f: dome fields; precision "fp64" or "mixed" for the momentum solve (the
+    enthalpy solve is binary64 either way); configure(h) sets solver options
+    on the model's Hierarchy handle (None keeps the reference's algorithm)."""
+
+    def __init__(self, f, dx, n_levels, nz, precision="fp64", quirks=True, configure=None, rtol=1e-8,
+                 max_vcycles=40, dt_yr=5.0, n_smooth=10, Q_geo=0.05):
+        import torch
+        from glide_b200.model import IceDynamics, ThermalModel
+        ny, nx = f["H"].shape
+        self.model = IceDynamics(n_levels=n_levels, ny=ny, nx=nx, dx=dx, reference_quirks=quirks,
+                                 precision=precision)
+        mg = self.model.mg
+        for k, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
+            getattr(grp, k).set(torch.as_tensor(f[k]))
+        mg.state.H.set(torch.as_tensor(f["H"]))
+        mg.state.H_prev.set(torch.as_tensor(f["H_prev"]))
+        self.model.forward_solver.fas_options.set(maximum_vcycles=max_vcycles, relative_tolerance=rtol,
+                                                  absolute_tolerance=0.0, report_norms=False)
+        if configure is not None:
+            configure(mg.hierarchy)
+        self.grid = mg.levels[0]
+        self.thermal = ThermalModel(self.grid, nz=nz, n_smooth=n_smooth)
+        self.thermal.initialize(self.surface_T(), Q_geo=Q_geo)
+        self.dt_yr = dt_yr
+        self.dt_s = dt_yr * SEC_PER_YR
+        self.t = 0.0
+
+    def surface_T(self):
+        return surface_temperature(self.grid.state.H.data, self.grid.geometry.bed.data)
+
+    def step(self):
+        """One coupled step; returns the momentum solve's stats and the
+        number of enthalpy column sweeps it took."""
+        tm = self.thermal
+        tm.pre_momentum()
+        st = self.model.forward(self.t, self.dt_yr)
+        tm.ops.set_surface_enthalpy_from_temperature(self.surface_T())
+        tm.step(self.dt_s)
+        self.t += self.dt_yr
+        ls = getattr(tm.ops, "last_stats", None)
+        return st, (int(ls.iterations) if ls is not None else None)
+
+    def fields(self):
+        """Level-0 u, v, H, the enthalpy (ny, nx, nz) and B, as NumPy arrays."""
+        g = self.grid
+        return {"u": g.state.u.data.cpu().numpy(), "v": g.state.v.data.cpu().numpy(),
+                "H": g.state.H.data.cpu().numpy(), "E": self.thermal.enthalpy.cpu().numpy(),
+                "B": g.rheology.B.data.cpu().numpy()}
