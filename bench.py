@@ -77,6 +77,10 @@ def parse(argv=None):
     ap.add_argument("--no-thermal", action="store_true", help="skip timing the enthalpy (thermal) step")
     ap.add_argument("--no-vti", action="store_true", help="skip timing the VTI output of the solved state")
     ap.add_argument("--nz", type=int, default=41, help="sigma levels of the enthalpy columns")
+    ap.add_argument("--coupled-steps", type=int, default=50,
+                    help="coupled thermomechanical steps of the coupled leg (after one untimed step)")
+    ap.add_argument("--no-coupled", action="store_true", help="skip the coupled thermomechanical leg")
+    ap.add_argument("--no-fp64-fast", action="store_true", help="skip timing the fast form in binary64")
     ap.add_argument("--members", type=int, default=64, help="ensemble mode: members")
     ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
@@ -330,8 +334,13 @@ def kernel_roofline(a, h, stream, fields=None, probe=False):
     """Time the step's hot kernels alone on the step-start state, in the
     precision the step runs them in (binary32 for the mixed form's smoother
     and tangent operator), with CUDA events: the fused fine-level Vanka
-    sweep, the Jacobian-vector product and the residual.  Algorithmic bytes:
-    15 N s (sweep, residual), 18 N s (JVP); N = fine cells, s = bytes/value."""
+    sweep, the Jacobian-vector product and the residual.  Algorithmic bytes (N = fine cells, s = bytes per value): residual 15 N s
+    (u, v, H, phi, mask, bed, B, beta, gamma, three forcing arrays read, three
+    rows written); the JVP as timed here, without forcing, 14 N s (u, v, H,
+    phi, mask, bed, beta, B and the direction read, three rows written); the
+    fused Vanka sweep 15 N s; the tangent smoother's block factorisation 34 N s
+    (state read, 25 factor planes written) and its block sweep 34 N s (25
+    factors, residual and unknowns read, unknowns written)."""
     import torch
     from glide_b200.hierarchy import Hierarchy
     prec = "fp32" if a.precision in ("mixed", "fp32") else "fp64"
@@ -367,10 +376,13 @@ def kernel_roofline(a, h, stream, fields=None, probe=False):
         k.vanka_sweep(0, a.dt, 1)
         torch.cuda.synchronize()
     # state-preserving kernels first, then the sweep (which moves the state)
-    for name, fn, nbytes in (
-            ("k_residual", lambda: k.residual(0, a.dt, 8), 15 * n * itemsize),
-            ("k_jvp", lambda: k.jvp(0, a.dt, reference_rows=False), 18 * n * itemsize),
-            ("k_vanka_sweep", lambda: k.vanka_sweep(0, a.dt, 1), 15 * n * itemsize)):
+    kernels = [("k_residual", lambda: k.residual(0, a.dt, 8), 15 * n * itemsize),
+               ("k_jvp", lambda: k.jvp(0, a.dt, reference_rows=False), 14 * n * itemsize)]
+    if hasattr(k, "block_factor"):
+        kernels += [("k_block_factor", lambda: k.block_factor(0, a.dt), 34 * n * itemsize),
+                    ("k_block_sweep", lambda: k.block_sweep(0, a.dt), 34 * n * itemsize)]
+    kernels += [("k_vanka_sweep", lambda: k.vanka_sweep(0, a.dt, 1), 15 * n * itemsize)]
+    for name, fn, nbytes in kernels:
         fn()
         fn()
         ms = event_time(fn, 10, stream)
@@ -413,6 +425,7 @@ def run_ours(a, rank, world):
     sampler.start()
     time.sleep(0.3)
     l0 = h.launch_count()
+    b0 = h.alg_bytes()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     if world > 1:
@@ -426,6 +439,7 @@ def run_ours(a, rank, world):
         dist.barrier()
     torch.cuda.synchronize()
     launches = h.launch_count() - l0
+    step_bytes = (h.alg_bytes() - b0) / a.steps
     clocks = sampler.stop()
     ms = reduce_max(e0.elapsed_time(e1) / a.steps, dev, world)
     vcyc = float(np.mean([s["vcycles"] for s in stats]))
@@ -468,7 +482,7 @@ def run_ours(a, rank, world):
     out_u = torch.empty(h.view("u", 0).shape, dtype=dtype).pin_memory()
     out_v = torch.empty(h.view("v", 0).shape, dtype=dtype).pin_memory()
     out_H = torch.empty(h.view("H", 0).shape, dtype=dtype).pin_memory()
-    k_e2e = max(1, min(a.steps, 2))
+    k_e2e = max(1, a.steps)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -553,7 +567,28 @@ def run_ours(a, rank, world):
                  "final_relative_residual": float(np.max([s["final_norm"] / s["initial_norm"] for s in pst])),
                  "what": "reference algorithm (FASCD 10/20/50/200, 30 local Newton iterations, quirks) in binary64"}
 
+    # the same fast form in binary64: the gain of the precision alone
+    fp64_fast = None
+    if not a.no_fp64_fast and a.precision == "mixed":
+        af = parse(["--size", str(a.size), "--levels", str(a.levels), "--dx", str(a.dx),
+                    "--radius", str(a.radius), "--dt", str(a.dt), "--rtol", str(a.rtol),
+                    "--max-vcycles", str(a.max_vcycles), "--precision", "fp64"])
+        hf = make_solver(af, f)
+        fstep = step_fn(hf, af.dt)
+        for _ in range(2):
+            fstep()
+        fst = []
+        f_ms = reduce_max(event_time(lambda: fst.append(fstep()), 3, stream), dev, world)
+        fp64_fast = {"ms_per_step": f_ms, "steps_per_s": world * 1000.0 / f_ms,
+                     "vcycles_per_step": float(np.mean([s_["vcycles"] for s_ in fst])),
+                     "final_relative_residual": float(np.max([s_["final_norm"] / s_["initial_norm"] for s_ in fst])),
+                     "mixed_speedup": f_ms / ms,
+                     "what": "the fast form (same schedule, guarded Newton, tangent multigrid) all in binary64"}
+        del hf, fstep
+        torch.cuda.empty_cache()
+
     thermal = None if a.no_thermal else thermal_leg(a, h, f, stream, dev, world)
+    coupled = None if a.no_coupled else coupled_leg(a, f, stream, dev, world)
     output = None
     if not a.no_vti:
         import shutil
@@ -592,7 +627,12 @@ def run_ours(a, rank, world):
                    "schedule": {k: fas[k] for k in ("pre_steps", "post_steps", "finest_steps", "coarsest_steps")},
                    "parallelism": f"replicas x{world} (one domain per GPU)",
                    "l2": "inputs larger than L2 (2048^2 state and parameters: ~0.5 GB per fine-level pass)",
-                   "plain_fp64": plain, "grads": grads, "thermal": thermal, "output": output},
+                   "plain_fp64": plain, "fp64_fast": fp64_fast, "grads": grads, "thermal": thermal,
+                   "coupled": coupled, "output": output},
+        "hbm": {"bytes_per_step": step_bytes, "achieved_gbs": step_bytes / ms / 1e6,
+                "frac": step_bytes / ms / 1e6 / measured_peaks()[0], "peak_kind": measured_peaks()[1],
+                "what": "sum of the algorithmic bytes of every kernel the step launched (glide_alg_bytes: the "
+                        "values each kernel must read and write once) over the step's device time"},
         "gpu_launches": int(launches),
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -857,6 +897,82 @@ def thermal_leg(a, h, f, stream, dev, world):
             "sweeps_last_step": int(st.iterations) if st is not None else None,
             "what": f"ThermalModel.step at {a.size}^2 x {a.nz} (binary64)",
             "kernels": kern}
+
+
+def coupled_leg(a, f, stream, dev, world):
+    """The large thermomechanical run: coupled steps at --size^2 with --nz
+    sigma levels in the order of the reference's coupled example
+    (pre_momentum, IceDynamics.forward, surface enthalpy from the new
+    geometry, ThermalModel.step with the B feedback), through the public API
+    (tests/cases.py CoupledRun).  The momentum solve runs in the bench's
+    form; the enthalpy solve is binary64.  One untimed step (the cold start
+    from u = v = 0, graph capture), then --coupled-steps timed steps.  The
+    same steps are then run with the momentum solve in binary64 from the same
+    start, and the line gives the relative max-norm differences of u, v, H, E
+    and B after the last step.  Surface temperature -30 + 6e-3 (2000 - s) C,
+    geothermal flux 0.05 W m^-2, ThermalModel's default 10 sweeps at most."""
+    import torch
+    from cases import CoupledRun
+    n_steps = max(1, a.coupled_steps)
+    peak, peak_kind = measured_peaks()
+
+    def configure(h):
+        if a.inner is not None:
+            h.set_tuning(mixed_inner_vcycles=a.inner)
+        apply_solver_options(h, a)
+
+    legs, fields = {}, {}
+    precisions = [a.precision] + (["fp64"] if a.precision != "fp64" else [])
+    for prec in precisions:
+        run = CoupledRun(f, a.dx, a.levels, a.nz, precision=prec, quirks=not a.native, configure=configure,
+                         rtol=a.rtol, max_vcycles=a.max_vcycles, dt_yr=a.dt)
+        run.thermal.ops.set_tuning(point_blocks_per_sm=a.enth_point_blocks,
+                                   column_blocks_per_sm=a.enth_column_blocks, column_prefers_l1=a.enth_column_l1)
+        run.step()
+        h = run.model.mg.hierarchy
+        torch.cuda.synchronize()
+        b0, l0 = h.alg_bytes(), h.launch_count()
+        tl0, tb0 = run.thermal.ops.counters()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(n_steps)]
+        stats = [run.step(ev[k]) for k in range(n_steps)]
+        torch.cuda.synchronize()
+        total = ev[0][0].elapsed_time(ev[-1][2])
+        ssa = sum(e[0].elapsed_time(e[1]) for e in ev)
+        thermal = sum(e[1].elapsed_time(e[2]) for e in ev)
+        ms = reduce_max(total / n_steps, dev, world)
+        tl1, tb1 = run.thermal.ops.counters()
+        ssa_bytes = (h.alg_bytes() - b0) / n_steps
+        th_bytes = (tb1 - tb0) / n_steps
+        sweeps = [sw for _, sw in stats]
+        legs[prec] = {
+            "ms_per_step": ms, "steps_per_s": world * 1000.0 / ms,
+            "momentum_ms_per_step": ssa / n_steps, "thermal_ms_per_step": thermal / n_steps,
+            "vcycles_per_step": float(np.mean([st["vcycles"] for st, _ in stats])),
+            "final_relative_residual": float(np.max([st["final_norm"] / st["initial_norm"] for st, _ in stats])),
+            "thermal_sweeps_per_step": float(np.mean(sweeps)), "thermal_sweeps_max": int(max(sweeps)),
+            "gpu_launches_per_step": ((h.launch_count() - l0) + (tl1 - tl0)) / n_steps,
+            "hbm": {"bytes_per_step": ssa_bytes + th_bytes, "momentum_bytes_per_step": ssa_bytes,
+                    "thermal_bytes_per_step": th_bytes,
+                    "achieved_gbs": (ssa_bytes + th_bytes) / ms / 1e6,
+                    "frac": (ssa_bytes + th_bytes) / ms / 1e6 / peak, "peak_kind": peak_kind},
+        }
+        fields[prec] = run.fields()
+        del run, h
+        torch.cuda.empty_cache()
+    out = {"what": f"coupled thermomechanical steps at {a.size}^2 x {a.nz} sigma levels: momentum + mass solve "
+                   f"to rel. residual {a.rtol:g} ({a.precision}), then the binary64 enthalpy column solve and "
+                   "the B feedback, in the order of the reference's coupled example",
+           "steps": n_steps, "untimed_steps_before": 1, **legs[a.precision]}
+    if "fp64" in legs and a.precision != "fp64":
+        from util import rel_err
+        out["binary64"] = legs["fp64"]
+        out["speedup_vs_binary64"] = legs["fp64"]["ms_per_step"] / legs[a.precision]["ms_per_step"]
+        out["error_vs_binary64"] = {k: rel_err(fields[a.precision][k], fields["fp64"][k])
+                                    for k in ("u", "v", "H", "E", "B")}
+        out["error_what"] = (f"max |x - x64| / max |x64| after {n_steps + 1} coupled steps from the same start, "
+                             "x64 the same steps with the momentum solve in binary64 (the binary64 path is pinned "
+                             "to the reference at 1e-10)")
+    return out
 
 
 # -------------------------------------------------------------- CPU legs

@@ -134,6 +134,7 @@ SIGNATURES = {
     "glide_set_use_graphs": ([_H, _I], _I),
     "glide_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], _I),
     "glide_alg_bytes": ([_H, ctypes.POINTER(ctypes.c_double)], _I),
+    "glide_block_smoother_part": ([_H, _I, _D, _I, _I, _P], _I),
     "glide_set_tuning": ([_H, _I, _I], _I),
     "glide_set_rhs": ([_H, _I, _D, _P], _I),
     "glide_compute_phi": ([_H, _I, _D, _P], _I),

@@ -1040,6 +1040,22 @@ struct Solver : SolverBase {
 
     void adj_sweeps(int l, double dt, int n, cudaStream_t s) { lin_sweeps(l, dt, n, adj_sys(), s); }
 
+    // one launch of the linear smoother's block factorisation (part 0) or of
+    // its block sweep on the current residual (part 1), nothing else
+    void block_part(int l, double dt, bool adjoint, int part, cudaStream_t s) {
+        ensure_blocks();
+        const Lin L = adjoint ? adj_sys() : tan_sys();
+        if (part == 0) {
+            block_factor(l, dt, L, s);
+            return;
+        }
+        BlockArgs<R> a = block_args(l, dt, L);
+        dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
+        if (L.tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
+        else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
+        counted("linear_sweep", lb(l, 34));
+    }
+
     // glide/multigrid.py:905-973 (linear FAS)
     void lin_vcycle(int l, bool finest, double dt, const Lin& L, cudaStream_t s) {
         const glide_fas_config& c = fas[L.cfg];
@@ -1566,6 +1582,16 @@ int glide_launch_count(glide_handle h, long long* count) {
     return guarded([&] {
         if (!count) fail(GLIDE_ERR_ARG, "null count");
         dispatch(h, [&](auto& s) { *count = s.launches; });
+    });
+}
+
+int glide_block_smoother_part(glide_handle h, int level, double dt, int adjoint, int part, void* stream) {
+    return guarded([&] {
+        if (part < 0 || part > 1) fail(GLIDE_ERR_ARG, "part must be 0 (factorisation) or 1 (sweep)");
+        dispatch(h, [&](auto& s) {
+            s.check_level(level);
+            s.block_part(level, dt, adjoint != 0, part, S(stream));
+        });
     });
 }
 

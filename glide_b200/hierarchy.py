@@ -272,6 +272,15 @@ class Hierarchy:
         """flags: USE_MASK (the default) and FREEZE_CALVING, as glide_jvp."""
         call("glide_jvp", self._h, int(level), float(dt), int(bool(reference_rows)), int(flags), _stream_ptr())
 
+    def block_factor(self, level: int, dt: float, adjoint: bool = False):
+        """One launch of the linear smoother's block factorisation alone
+        (glide_block_smoother_part; instrumentation)."""
+        call("glide_block_smoother_part", self._h, int(level), float(dt), int(bool(adjoint)), 0, _stream_ptr())
+
+    def block_sweep(self, level: int, dt: float, adjoint: bool = False):
+        """One launch of the linear smoother's block sweep alone."""
+        call("glide_block_smoother_part", self._h, int(level), float(dt), int(bool(adjoint)), 1, _stream_ptr())
+
     def adjoint_sweep(self, level: int, dt: float, n: int):
         call("glide_adjoint_sweep", self._h, int(level), float(dt), int(n), _stream_ptr())
 

@@ -161,6 +161,14 @@ int glide_launch_count(glide_handle h, long long* count);
  * time it gives the achieved HBM bandwidth of a whole solve.  No counterpart
  * in the reference: instrumentation. */
 int glide_alg_bytes(glide_handle h, double* bytes);
+/* One launch of the linear smoother's block factorisation (part 0) or of its
+ * block sweep x -= omega B^-1 r over the current residual (part 1), on the
+ * tangent system (adjoint = 0) or the adjoint system (adjoint = 1) of
+ * `level`, nothing before or after it: for timing the two kernels alone.  A
+ * sweep without a preceding factorisation of the same state reads whatever
+ * the factor buffers hold.  No counterpart in the reference:
+ * instrumentation. */
+int glide_block_smoother_part(glide_handle h, int level, double dt, int adjoint, int part, void* stream);
 /* Kernel tuning knobs (no counterpart in the reference).
  * GLIDE_TUNE_SWEEP_BLOCKS_PER_SM: 1 or 2 resident Vanka-sweep blocks per SM.
  * GLIDE_TUNE_MIXED_INNER_VCYCLES: binary32 V-cycles per defect correction

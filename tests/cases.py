@@ -177,14 +177,22 @@ class CoupledRun:
     def surface_T(self):
         return surface_temperature(self.grid.state.H.data, self.grid.geometry.bed.data)
 
-    def step(self):
+    def step(self, marks=None):
         """One coupled step; returns the momentum solve's stats and the
-        number of enthalpy column sweeps it took."""
+        number of enthalpy column sweeps it took.  marks: optional list of
+        three CUDA events, recorded before the momentum solve, between it and
+        the thermal half, and at the end."""
         tm = self.thermal
+        if marks:
+            marks[0].record()
         tm.pre_momentum()
         st = self.model.forward(self.t, self.dt_yr)
+        if marks:
+            marks[1].record()
         tm.ops.set_surface_enthalpy_from_temperature(self.surface_T())
         tm.step(self.dt_s)
+        if marks:
+            marks[2].record()
         self.t += self.dt_yr
         ls = getattr(tm.ops, "last_stats", None)
         return st, (int(ls.iterations) if ls is not None else None)
