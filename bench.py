@@ -90,7 +90,8 @@ def parse(argv=None):
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
     ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
-    ap.add_argument("--mode", default="step", choices=["step", "sweeps", "kernels", "thermal", "ensemble", "vti"],
+    ap.add_argument("--mode", default="step",
+                    choices=["step", "sweeps", "kernels", "thermal", "ensemble", "vti", "coupled"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -1094,6 +1095,13 @@ def main():
         return 0
     if a.mode == "vti":
         run_vti(a)
+        return 0
+    if a.mode == "coupled":
+        import torch
+        from cases import dome
+        f = dome(a.size, a.dx, a.radius, seed=0)
+        out = coupled_leg(a, f, torch.cuda.current_stream(), torch.device("cuda", 0), 1)
+        print(json.dumps({"mode": "coupled", "size": a.size, **out}), flush=True)
         return 0
     if a.mode == "ensemble":
         print(json.dumps({"mode": "ensemble", **run_ensemble(a)}), flush=True)

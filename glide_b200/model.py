@@ -88,7 +88,12 @@ class ThermalModel:
 
     step(dt): omega from the realised thickness change, frictional heating,
     forcing, column sweeps, then the depth-averaged rate factor fed back into
-    the finest grid's B (coarser levels keep theirs, as in the reference).
+    the grid's B.  In reference mode (the hierarchy's reference quirks on)
+    only that grid's B changes and coarser levels keep theirs, as in the
+    reference (glide/model.py:216-222).  In native mode the new B is also
+    restricted to every coarser level, so the coarse-grid corrections of the
+    next momentum solve use the same viscosity as the fine level; with stale
+    coarse B a large change of the rate factor stalls the multigrid solve.
     The SSA velocity is read in place for every sigma layer (no layer copies);
     the m/a -> m/s conversion is applied by the kernels as they read it.
     """
@@ -140,6 +145,9 @@ class ThermalModel:
             n = float(ops.grid.rheology.n.value)
             scale = self.rho_i * self.g * sec ** (1.0 / n)
             ops.get_arrhenius_factor(out=ops.grid.rheology.B.data, scale=scale)
+            hier = getattr(ops.grid, "_hier", None)
+            if hier is not None and not getattr(hier, "reference_quirks", True):
+                hier.restrict("B", ops.grid.level)
 
     @property
     def B_scale(self):

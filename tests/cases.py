@@ -149,10 +149,12 @@ class CoupledRun:
 
     f: dome fields; precision "fp64" or "mixed" for the momentum solve (the
     enthalpy solve is binary64 either way); configure(h) sets solver options
-    on the model's Hierarchy handle (None keeps the reference's algorithm)."""
+    on the model's Hierarchy handle (None keeps the reference's algorithm).
+    init_B: start from the rate factor of the initial temperature on every
+    level (f's B is used only when False)."""
 
     def __init__(self, f, dx, n_levels, nz, precision="fp64", quirks=True, configure=None, rtol=1e-8,
-                 max_vcycles=40, dt_yr=5.0, n_smooth=10, Q_geo=0.05):
+                 max_vcycles=40, dt_yr=5.0, n_smooth=10, Q_geo=0.05, init_B=True):
         import torch
         from glide_b200.model import IceDynamics, ThermalModel
         ny, nx = f["H"].shape
@@ -170,6 +172,11 @@ class CoupledRun:
         self.grid = mg.levels[0]
         self.thermal = ThermalModel(self.grid, nz=nz, n_smooth=n_smooth)
         self.thermal.initialize(self.surface_T(), Q_geo=Q_geo)
+        if init_B:
+            # B from the initial temperature on every level, as the
+            # reference's coupled example starts (coupled_dome.py:144-146)
+            tm = self.thermal
+            mg.rheology.B.set(tm.ops.get_arrhenius_factor(scale=tm.B_scale))
         self.dt_yr = dt_yr
         self.dt_s = dt_yr * SEC_PER_YR
         self.t = 0.0
