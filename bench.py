@@ -885,13 +885,20 @@ def thermal_leg(a, h, f, stream, dev, world):
     nbytes = (5 * a.nz + 7) * 8 * ncol
     peak, _ = measured_peaks()
     kern = {}
-    for name, fn in (("k_enth_column", lambda: ops.column_smooth(dt_s)),
+    def column(kind):
+        def fn():
+            ops.set_tuning(column_kernel=kind)
+            ops.column_smooth(dt_s)
+        return fn
+    for name, fn in (("k_enth_column_s", column("smem")),
+                     ("k_enth_column (per-thread arrays)", column("local")),
                      ("k_enth_layer", lambda: ops.layer_smooth(dt_s)),
                      ("k_enth_residual", lambda: ops.compute_residual(dt_s))):
         fn()
         ms = event_time(fn, 5, stream)
         gbs = nbytes / (ms * 1e-3) / 1e9
         kern[name] = {"launch_ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
+    ops.set_tuning(column_kernel="smem")
     # the residual call also reads the norm back (one small copy and a sync)
     st = getattr(ops, "last_stats", None)
     return {"ms_per_step": t_ms, "steps_per_s": world * 1000.0 / t_ms, "nz": a.nz, "columns": ncol,

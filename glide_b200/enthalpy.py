@@ -253,8 +253,13 @@ class EnthalpyOperators:
         inp.vel_div = self._vel_div
         _ecall("glide_enthalpy_set_inputs", self._h, ctypes.byref(inp))
 
-    def set_tuning(self, point_blocks_per_sm=None, column_blocks_per_sm=None, column_prefers_l1=None):
-        """Launch shapes of the kernels (no counterpart in the reference)."""
+    def set_tuning(self, point_blocks_per_sm=None, column_blocks_per_sm=None, column_prefers_l1=None,
+                   column_kernel=None):
+        """Launch shapes of the kernels (no counterpart in the reference).
+        column_kernel: "smem" (default; Thomas factors in shared memory) or
+        "local" (per-thread arrays)."""
+        if column_kernel is not None:
+            _ecall("glide_enthalpy_set_tuning", self._h, 4, {"local": 0, "smem": 1}[column_kernel])
         if point_blocks_per_sm is not None:
             _ecall("glide_enthalpy_set_tuning", self._h, 1, int(point_blocks_per_sm))
         if column_blocks_per_sm is not None:

@@ -167,3 +167,38 @@ def test_column_sweeps_match_oracle_across_nz(nz):
     s = {k: v.copy() for k, v in st.items()}
     eo.column_sweep(s, cfg, 3)
     assert rel_err(_np(ops.enthalpy_state.E), s["E"]) <= 1e-10
+
+
+@pytest.mark.parametrize("nz", [3, 4, 17, 41])
+@pytest.mark.parametrize("flat", [True, False])
+def test_column_kernels_agree_and_match_oracle(nz, flat):
+    """The column smoother with its factors in shared memory (the default)
+    against the one-thread-per-column kernel (1e-12) and, over three
+    alternating sweeps, against the oracle (1e-10).  flat: one velocity for
+    every layer, read in place from the grid (the coupled model's case,
+    where the horizontal flux of the frozen neighbours is folded into the
+    row constants); otherwise a velocity per layer."""
+    from oracle import enthalpy_oracle as eo
+    st = enthalpy_state(40, 52, nz, seed=nz)
+    if flat:
+        st["u3d"] = np.ascontiguousarray(np.broadcast_to(st["u3d"][0], st["u3d"].shape))
+        st["v3d"] = np.ascontiguousarray(np.broadcast_to(st["v3d"][0], st["v3d"].shape))
+    cfg = enthalpy_config(relative_tolerance=1e-30, absolute_tolerance=0.0)
+    out = {}
+    for kernel in ("local", "smem"):
+        ops = _ops(st, cfg["dx"], nz)
+        if flat:
+            ops.grid.state.u.set(torch.as_tensor(st["u3d"][0]))
+            ops.grid.state.v.set(torch.as_tensor(st["v3d"][0]))
+            ops.broadcast_velocity()
+        ops.set_tuning(column_kernel=kernel)
+        ops.column_smooth(cfg["dt"])
+        out[kernel] = _np(ops.delta_E).copy()
+        if kernel == "smem":
+            ops.smoother_config.relative_tolerance = 1e-30
+            ops.smoother_config.absolute_tolerance = 0.0
+            ops.column_sweep(cfg["dt"], 3)
+            s = {k: v.copy() for k, v in st.items()}
+            eo.column_sweep(s, cfg, 3)
+            assert rel_err(_np(ops.enthalpy_state.E), s["E"]) <= 1e-10
+    assert rel_err(out["smem"], out["local"]) <= 1e-12
