@@ -41,8 +41,10 @@ def test_coupled_binary64_matches_oracle():
 
 
 # mixed (binary32 smoother and tangent multigrid, binary64 residual and
-# state) against binary64 after five coupled steps, both to 1e-8
-MIXED_TOL = {"u": 1e-5, "v": 1e-5, "H": 1e-7, "E": 1e-7, "B": 1e-7}
+# state) against binary64 after five coupled steps, both to 1e-8.  Both end
+# in Newton steps on the same binary64 residual, which overshoot the solve
+# tolerance; measured differences are ~1e-14 (u, v) and ~1e-15 (H, E, B).
+MIXED_TOL = {"u": 1e-8, "v": 1e-8, "H": 1e-9, "E": 1e-9, "B": 1e-9}
 
 
 def test_coupled_mixed_matches_binary64():
