@@ -11,6 +11,11 @@ Outputs:
                                     the reference checkout and executed by the
                                     fiber emulator in simt_host.cpp; built only
                                     when the reference checkout is present.
+  oracle/_ref/libglide_ref_gpu.so -- the same sources compiled unmodified for
+                                    sm_100a with --use_fast_math (ref_gpu.cu),
+                                    for timing the reference's kernels on the
+                                    GPU (oracle/ref_gpu.py); built by nvcc when
+                                    it and the reference checkout are present.
 
 Usage: python oracle/build_oracle.py [--reference DIR] [--force]
 """
@@ -99,6 +104,15 @@ def build_reference(reference: str, force: bool = False) -> list[Path]:
         if force or _stale(out, srcs):
             _run([CXX, *BASE_FLAGS, "-w", f"-I{cuda_dir}", f"-I{HERE}", f"-I{REF_OUT}", *defs,
                   str(HERE / "ref_harness.cpp"), str(HERE / "simt_host.cpp"), "-o", str(out)])
+        outs.append(out)
+    nvcc = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    if Path(nvcc).exists():
+        out = REF_OUT / "libglide_ref_gpu.so"
+        gsrcs = [HERE / "ref_gpu.cu", *sorted(cuda_dir.glob("*.cu"))]
+        if force or _stale(out, gsrcs):
+            _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "--use_fast_math",
+                  "-Xcompiler", "-fPIC", "-shared", "-w", f"-I{cuda_dir}", str(HERE / "ref_gpu.cu"), "-o",
+                  str(out), "-lcudart"])
         outs.append(out)
     return outs
 
