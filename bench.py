@@ -442,6 +442,11 @@ def run_ours(a, rank, world):
     launches = h.launch_count() - l0
     step_bytes = (h.alg_bytes() - b0) / a.steps
     clocks = sampler.stop()
+    # the solved state, from which the CPU baseline's sample starts
+    warm_state = None
+    if world == 1 and not a.no_cpu_baseline:
+        warm_state = {k: h.view(k, 0).detach().cpu().numpy().astype(np.float64)
+                      for k in ("u", "v", "H", "mask", "H_prev")}
     ms = reduce_max(e0.elapsed_time(e1) / a.steps, dev, world)
     vcyc = float(np.mean([s["vcycles"] for s in stats]))
     final_rel = float(np.max([s["final_norm"] / s["initial_norm"] for s in stats]))
@@ -450,7 +455,7 @@ def run_ours(a, rank, world):
                 "precision": a.precision, "method": a.method, "switch": a.switch,
                 "schedule": a.schedule, "omega": a.omega, "relax": a.relax, "native": a.native,
                 "newton_steps": a.newton_steps,
-                "tangent": [a.tangent_vcycles, a.tangent_schedule, a.tangent_omega]}, None
+                "tangent": [a.tangent_vcycles, a.tangent_schedule, a.tangent_omega]}, None, None
 
     # gradients: adjoint solve to the same tolerance, forcing -dJ/du of
     # J = 0.5 |u - 0.95 u*|^2 at the solved state, from lambda = 0 each time
@@ -646,7 +651,7 @@ def run_ours(a, rank, world):
                      "algorithmic_bytes_per_launch": kd["algorithmic_bytes"], "kernels": kernels},
         "clocks": clocks,
     }
-    return res, plain
+    return res, plain, warm_state
 
 
 def run_thermal(a):
@@ -984,11 +989,24 @@ def coupled_leg(a, f, stream, dev, world):
 
 
 # -------------------------------------------------------------- CPU legs
-def cpu_oracle_sample(a, plain, budget_s):
+def sweep_cost_model(levels, pre, post, finest, coarsest):
+    """(fine-sweep equivalents, fine-residual equivalents) of one V-cycle
+    of the reference's FASCD schedule: level l costs 4^-l of the fine level;
+    every level above the coarsest evaluates its residual (phi frozen) and
+    the next level's operator, and the solve evaluates one convergence
+    residual per cycle."""
+    sweeps = sweeps_per_vcycle(levels, pre, post, finest, coarsest)
+    res = 1.0 + sum(4.0 ** (-l) + 4.0 ** (-(l + 1)) for l in range(levels - 1))
+    return sweeps, res
+
+
+def cpu_oracle_sample(a, plain, budget_s, warm=None):
     """binary64 C++/OpenMP oracle (the reference's algorithm restated): timed
-    fine-level Vanka sweeps from the workload's start state, scaled to a step
-    by the reference form's V-cycles per step (measured on the GPU in this
-    run) times its fine-sweep equivalents per V-cycle."""
+    fine-level Vanka sweeps and one residual evaluation from `warm` -- the
+    state the GPU arm solved (u, v, H, mask after its timed steps) -- scaled
+    to a step by the reference form's V-cycles per step (measured on the GPU
+    in this run, binary64 to the same tolerance) and the V-cycle's cost in
+    fine-sweep and fine-residual equivalents."""
     from cases import dome
     from oracle.glide_oracle import OracleHierarchy
     f = dome(a.size, a.dx, a.radius, seed=0)
@@ -996,7 +1014,15 @@ def cpu_oracle_sample(a, plain, budget_s):
     for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
         o.set_field(k, f[k])
     lev = o.levels[0]
+    start = "the workload's start state (u = v = 0)"
+    if warm is not None:
+        for k in ("u", "v", "H", "mask", "H_prev"):
+            getattr(lev, k)[...] = warm[k]
+        start = "the warm state the GPU arm solved"
     lev.f_H[...] = lev.H_prev / a.dt + lev.smb
+    t0 = time.perf_counter()
+    lev.residual(a.dt)
+    t_res = time.perf_counter() - t0
     n, t0 = 0, time.perf_counter()
     while True:
         lev.vanka_sweep(a.dt, 1)
@@ -1005,81 +1031,180 @@ def cpu_oracle_sample(a, plain, budget_s):
         if el > budget_s or n >= 50:
             break
     per_sweep = el / n
-    vcyc = plain["vcycles_per_step"] if plain else REF_VCYCLES_PER_STEP
-    spv = sweeps_per_vcycle(a.levels)
-    per_step = per_sweep * spv * vcyc
+    if plain is None:
+        return None
+    vcyc = plain["vcycles_per_step"]
+    spv, rpv = sweep_cost_model(a.levels, 10, 20, 50, 200)
+    per_step = vcyc * (per_sweep * spv + t_res * rpv) + t_res
     cores = len(os.sched_getaffinity(0))
     return {"value": 1.0 / per_step, "unit": "steps/s", "cores": cores, "kind": "port",
-            "sample": f"{n} fine-level Vanka sweeps of the binary64 oracle at {a.size}^2 from the start state "
-                      f"({per_sweep:.3f} s each), x {spv:.1f} fine-sweep equivalents per V-cycle x {vcyc:g} "
-                      f"V-cycles per step (reference algorithm, binary64)"}
+            "sample": f"{n} fine-level Vanka sweeps ({per_sweep:.3f} s each) and one residual ({t_res:.3f} s) of "
+                      f"the binary64 oracle at {a.size}^2 from {start}; a step = {vcyc:g} V-cycles (the "
+                      f"reference algorithm's count to {a.rtol:g} on the GPU in this run) x ({spv:.1f} sweeps + "
+                      f"{rpv:.2f} residuals, fine-level equivalents) + the initial residual"}
 
 
-# V-cycles per step to 1e-8 of this workload with the reference algorithm in
-# binary64, measured on a B200 (the binary32 reference stalls above 1e-8, so
-# its work to 1e-8 is taken as this count).
-REF_VCYCLES_PER_STEP = 8.0
+# The binary32 reference stalls near 4e-5 relative on this workload (its
+# residual floor is an absolute ~0.8 against ~2e4 at a warm step's start), so
+# its own runs use the tightest relative tolerance it reaches reliably.
+REF_RTOL = 1e-4
+REF_MAX_VCYCLES = 20
+
+
+def reference_gpu_leg(a, f):
+    """The reference's own kernels on the GPU (oracle/ref_gpu.py: its
+    glide/cuda/*.cu built unmodified for sm_100a, driven by its host
+    sequence restated on device arrays): W warm-up steps, then K forward
+    steps (IceDynamics.forward, FASCD to REF_RTOL) and K forward + adjoint
+    steps (the adjoint of J = 0.5 |u - 0.95 u*|^2 to REF_RTOL, then the beta
+    and bed gradients), timed with CUDA events.  Returns the timings and the
+    warm state (after the warm-up steps) as binary32 host arrays."""
+    import torch
+    from oracle import ref_gpu
+    n = a.size
+    m = ref_gpu.RefGpuModel(n, n, a.dx, a.levels)
+    for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+        m.set_field(k, torch.as_tensor(f[k], device="cuda"))
+    for cfg in (m.fas, m.adj):
+        cfg.maximum_vcycles, cfg.relative_tolerance, cfg.absolute_tolerance = REF_MAX_VCYCLES, REF_RTOL, 0.0
+    for _ in range(max(1, a.warmup)):
+        m.forward(a.dt)
+    torch.cuda.synchronize()
+    top = m.levels[0]
+    warm = {k: getattr(top, k).cpu().numpy().copy() for k in ("u", "v", "H", "mask", "phi", "H_prev")}
+    k_steps = max(1, a.steps)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fwd = []
+    e0.record()
+    for _ in range(k_steps):
+        fwd.append((m.forward(a.dt), m.history[-1] / m.history[0]))
+    e1.record()
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / k_steps
+    adj = []
+    e0.record()
+    for _ in range(k_steps):
+        m.forward(a.dt)
+        it, _ = m.backward(a.dt, dJdu=0.05 * top.u, dJdv=0.05 * top.v)
+        adj.append((it, m.adj_history[-1] / m.adj_history[0]))
+    e1.record()
+    torch.cuda.synchronize()
+    fa_ms = e0.elapsed_time(e1) / k_steps
+    out = {"what": "the reference's own glide/cuda/*.cu kernels, built unmodified for sm_100a with --use_fast_math, "
+                   "driven by its host sequence (FASCDSolver / FASAdjointSolver, default 10/20/50/200 schedule, "
+                   "30 local Newton iterations) restated on torch float32 device arrays (oracle/ref_gpu.py)",
+           "forward": {"ms_per_step": fwd_ms, "steps_per_s": 1000.0 / fwd_ms,
+                       "vcycles_per_step": float(np.mean([c for c, _ in fwd])),
+                       "worst_relative_residual": float(max(r for _, r in fwd))},
+           "forward_adjoint": {"ms_per_step": fa_ms, "steps_per_s": 1000.0 / fa_ms,
+                               "adjoint_vcycles_per_step": float(np.mean([c for c, _ in adj])),
+                               "worst_adjoint_relative_residual": float(max(r for _, r in adj))},
+           "relative_tolerance": REF_RTOL, "max_vcycles": REF_MAX_VCYCLES,
+           "tolerance_note": "binary32: its residual stalls near 4e-5 relative on this workload, so 1e-8 is out "
+                             "of its reach; these are its own runs at 1e-4",
+           "steps": k_steps, "warmup": max(1, a.warmup)}
+    del m
+    torch.cuda.empty_cache()
+    return out, warm
 
 
 def run_reference(a):
-    """The reference's own kernels (oracle/_ref, host build of its CUDA
-    sources, binary32 as written) with its host loop -- compute_grounded,
-    vanka_smooth, the omega axpys -- timed on all host cores."""
+    """The reference arm.  `value`: the reference's own kernels compiled for
+    the host (oracle/_ref, binary32 as written) with its host loop -- one
+    compute_grounded, the delta fills, vanka_smooth and the omega axpys per
+    sweep -- timed on all host cores from the warm state its own GPU run
+    reached, scaled to a step by the V-cycles per step that run needed and
+    the V-cycle's cost in fine-sweep and fine-residual equivalents.  With a
+    GPU present, `reference_gpu` times the same kernels built for sm_100a."""
     from cases import dome
     from oracle.refpy import RefKernels
     lib_path = ROOT / "oracle" / "_ref" / "libglide_ref32.so"
     if not lib_path.exists():
         return {"impl": "reference", "unavailable": "oracle/_ref/libglide_ref32.so was not built "
                                                     "(reference checkout absent at build time)"}
-    k = RefKernels(fp64=False)
     f = dome(a.size, a.dx, a.radius, seed=0)
     n = a.size
-    z = lambda *s: np.zeros(s, np.float32)
-    u, v, H = z(n, n + 1), z(n + 1, n), f["H"].astype(np.float32)
-    phi, mask = z(n, n), z(n, n)
+    gpu, warm = None, None
+    try:
+        import torch
+        from oracle import ref_gpu
+        if torch.cuda.is_available() and ref_gpu.LIB_PATH.exists():
+            gpu, warm = reference_gpu_leg(a, f)
+    except ImportError:
+        pass
+    k = RefKernels(fp64=False)
+    z = lambda *s_: np.zeros(s_, np.float32)
+    if warm is not None:
+        u, v, H, mask, H_prev = (warm[x].astype(np.float32) for x in ("u", "v", "H", "mask", "H_prev"))
+        vcyc = gpu["forward"]["vcycles_per_step"]
+        start = "the warm state of the reference's own GPU run after its warm-up steps"
+        vsrc = f"the V-cycles per step its GPU run needed to reach {REF_RTOL:g}"
+    else:
+        u, v, H, mask, H_prev = z(n, n + 1), z(n + 1, n), f["H"].astype(np.float32), z(n, n), \
+            f["H_prev"].astype(np.float32)
+        vcyc = 4.0
+        start = "the workload's start state (no GPU: u = v = 0)"
+        vsrc = "4 V-cycles per step (its GPU runs' count at 1e-4 on this workload)"
+    phi = z(n, n)
     fu, fv = z(n, n + 1), z(n + 1, n)
-    fH = (f["H_prev"] / a.dt + f["smb"]).astype(np.float32)
+    fH = (H_prev / np.float32(a.dt) + f["smb"].astype(np.float32)).astype(np.float32)
     bed, B, beta = (f[x].astype(np.float32) for x in ("bed", "B", "beta"))
     gamma = np.full((n, n), 0.1, np.float32)
     du, dv, dH = z(n, n + 1), z(n + 1, n), z(n, n)
+    ru, rv, rH = z(n, n + 1), z(n + 1, n), z(n, n)
     grid = (n // 14 + 1, n // 14 + 1)
     phys = (3.0, 1e-6, 0.1, 1.0, 1.0, 1e-5, 0.1, 0.0, 0.1, a.dx, a.dt)
-    spv = sweeps_per_vcycle(a.levels)
-    steps_t = []
+    spv, rpv = sweep_cost_model(a.levels, 10, 20, 50, 200)
     cores = len(os.sched_getaffinity(0))
-    nsweeps = 0
+
+    def sweep():
+        k.launch("compute_grounded", grid, (16, 16), (phi, H, bed, 0.1, 0.0, n, n, 14, 1))
+        du.fill(0); dv.fill(0); dH.fill(0)
+        k.launch("vanka_smooth", grid, (16, 16),
+                 (du, dv, dH, mask, u, v, H, phi, fu, fv, fH, bed, B, beta, gamma, *phys,
+                  n, n, 14, 1, 30, 0.5, 0.01, 1.0))
+        u[...] += np.float32(0.5) * du
+        v[...] += np.float32(0.5) * dv
+        H[...] += np.float32(0.5) * dH
+
+    def residual():
+        k.launch("compute_grounded", grid, (16, 16), (phi, H, bed, 0.1, 0.0, n, n, 14, 1))
+        k.launch("compute_residual", grid, (16, 16),
+                 (ru, rv, rH, u, v, H, phi, mask, fu, fv, fH, bed, B, beta, gamma, True, True, *phys,
+                  n, n, 14, 1))
+        return float(np.sqrt(np.sum(ru.astype(np.float64) ** 2) + np.sum(rv.astype(np.float64) ** 2) +
+                             np.sum(rH.astype(np.float64) ** 2)))
+
+    t0 = time.perf_counter()
+    residual()
+    t_res = time.perf_counter() - t0
+    sweep()  # untimed
+    steps_t = []
     for _ in range(max(1, a.steps)):
-        nsw, t0 = 0, time.perf_counter()
-        while True:
-            k.launch("compute_grounded", grid, (16, 16), (phi, H, bed, 0.1, 0.0, n, n, 14, 1))
-            du.fill(0); dv.fill(0); dH.fill(0)
-            k.launch("vanka_smooth", grid, (16, 16),
-                     (du, dv, dH, mask, u, v, H, phi, fu, fv, fH, bed, B, beta, gamma, *phys,
-                      n, n, 14, 1, 30, 0.5, 0.01, 1.0))
-            u += np.float32(0.5) * du
-            v += np.float32(0.5) * dv
-            H += np.float32(0.5) * dH
-            nsw += 1
-            el = time.perf_counter() - t0
-            if el > a.cpu_seconds / max(1, a.steps) or nsw >= 20:
-                break
-        nsweeps += nsw
-        steps_t.append(el / nsw * spv * REF_VCYCLES_PER_STEP)
+        t0 = time.perf_counter()
+        sweep()
+        t_sweep = time.perf_counter() - t0
+        steps_t.append(vcyc * (t_sweep * spv + t_res * rpv) + t_res)
     step_s = float(np.median(steps_t))
     val = 1.0 / step_s
-    return {
+    out = {
         "metric": METRIC, "value": val, "unit": "steps/s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dome)", "impl": "reference",
         "config": {"workload": f"dome {a.size}x{a.size}, dx={a.dx:g} m, {a.levels} levels, dt={a.dt:g} a, "
-                               f"forward solve to rel. residual {a.rtol:g}",
-                   "vcycles_per_step_assumed": REF_VCYCLES_PER_STEP},
+                               f"forward solve to rel. residual {REF_RTOL:g} (binary32: 1e-8 is out of its reach)",
+                   "relative_tolerance": REF_RTOL, "vcycles_per_step": vcyc},
         "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "reference",
-                         "sample": f"{nsweeps} reference vanka_smooth sweeps (host build of glide/cuda/*.cu, "
-                                   f"binary32, {cores} threads) at {n}^2 from the start state, per-step work = "
-                                   f"{REF_VCYCLES_PER_STEP:g} V-cycles x {spv:.1f} fine-sweep equivalents"},
+                         "sample": f"per step one reference vanka_smooth sweep (host build of glide/cuda/*.cu, "
+                                   f"binary32, {cores} threads) at {n}^2 from {start}, and one residual "
+                                   f"({t_res:.2f} s) timed once; a step = {vcyc:g} V-cycles ({vsrc}) x "
+                                   f"({spv:.1f} sweeps + {rpv:.2f} residuals, fine-level equivalents) + the "
+                                   f"initial residual"},
         "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if gpu is not None:
+        out["reference_gpu"] = gpu
+    return out
 
 
 def main():
@@ -1115,9 +1240,9 @@ def main():
         return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    res, plain = run_ours(a, rank, world)
+    res, plain, warm_state = run_ours(a, rank, world)
     if rank == 0 and world == 1 and not a.no_cpu_baseline and not a.quick:
-        res["cpu_baseline"] = cpu_oracle_sample(a, plain, a.cpu_seconds)
+        res["cpu_baseline"] = cpu_oracle_sample(a, plain, a.cpu_seconds, warm=warm_state)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

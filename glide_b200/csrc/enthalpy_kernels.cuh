@@ -605,11 +605,31 @@ __global__ void __launch_bounds__(kColSmemThreads, MINB)
         } else {
             El[size_t(nz - 1) * plane] = en;
         }
-        for (int k = nz - 2; k >= 0; --k) {
+        // The iterate (and, on the last Newton step, the input state) of row
+        // k is loaded kPre rows ahead, into a register ring, so the serial
+        // substitution does not wait on a load at every row.
+        constexpr int kPre = 4;
+        const bool want_e = last && !first;
+        double ps[kPre], pe[kPre];
+#pragma unroll
+        for (int q = 0; q < kPre; ++q) {
+            const int k = nz - 2 - q;
+            ps[q] = k >= 0 ? src[size_t(k) * plane] : 0.0;
+            pe[q] = (want_e && k >= 0) ? E[size_t(k) * plane] : 0.0;
+        }
+#pragma unroll kPre
+        for (int q = 0; q < nz - 1; ++q) {
+            const int k = nz - 2 - q, slot = q % kPre;
+            const double sk = ps[slot], ek = pe[slot];
+            const int kn = k - kPre;
+            if (kn >= 0) {
+                ps[slot] = src[size_t(kn) * plane];
+                if (want_e) pe[slot] = E[size_t(kn) * plane];
+            }
             xk = dps[size_t(k) * bd] - cps[size_t(k) * bd] * xk;
-            en = src[size_t(k) * plane] + a.relaxation * xk;
+            en = sk + a.relaxation * xk;
             if (last) {
-                const double E0 = first ? src[size_t(k) * plane] : E[size_t(k) * plane];
+                const double E0 = first ? sk : ek;
                 El[size_t(k) * plane] = mode ? E0 + a.omega_relax * (en - E0) : en - E0;
             } else {
                 El[size_t(k) * plane] = en;
