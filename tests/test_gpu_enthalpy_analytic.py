@@ -1,0 +1,245 @@
+"""Known answers of the enthalpy column solver, on the GPU path, restated from
+the mathematics of the reference's own enthalpy tests at their tolerances:
+
+- polythermal (Stefan) slab, tests/test_enthalpy_stefan.py: a temperate bed
+  still feels the geothermal Neumann flux; smoothing from a temperate state
+  does not clamp the bed to the pressure-melting point; the steady profile
+  matches the two-zone semi-analytical solution (T within 0.1 K; E and the
+  basal water content within 2 %);
+- constant downward sigma velocity, tests/test_enthalpy_advection.py: the
+  steady profile matches E = A + B exp(Pe sigma), Pe = -5 (E within 2 %);
+- horizontal advection, tests/test_enthalpy_horiz_advection.py: a divergent
+  velocity under uniform E stays bounded; a y-invariant step advected by a
+  uniform velocity stays y-invariant (rows within 1 J/kg); the interior
+  energy sum of H E changes by less than 1 % over a step.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+SEC_PER_KYR = 1000.0 * 365.25 * 86400.0
+
+
+def _slab(ny, nx, nz, H, dx=1000.0):
+    """A flat slab of thickness H on a flat bed, its EnthalpyOperators."""
+    from glide_b200.enthalpy import EnthalpyOperators
+    from glide_b200.grid import Grid
+    g = Grid(ny, nx, dx)
+    full = lambda x: torch.full((ny, nx), float(x), dtype=torch.float64)
+    g.state.H.set(full(H))
+    g.state.H_prev.set(full(H))
+    g.geometry.bed.set(full(0.0))
+    g.forcing.smb.set(full(0.0))
+    g.sliding.beta.set(full(1.0))
+    g.sliding.m.set(1.0)
+    g.sliding.u_reg.set(1.0)
+    return EnthalpyOperators(g, nz=nz)
+
+
+def _static_column(nz, T_s, Q, H=1000.0):
+    """A 4 x 4 static column problem: no horizontal transport, no
+    drainage, no sources but the geothermal flux Q at the bed."""
+    ops = _slab(4, 4, nz, H)
+    ops.term_flags.horizontal_advection = False
+    ops.initialize_from_temperature(T_s)
+    ops.set_surface_enthalpy_from_temperature(torch.full((4, 4), T_s, dtype=torch.float64))
+    f = ops.enthalpy_forcing
+    f.Q_geo[:, :] = Q
+    f.phi_strain.fill_(0.0)
+    f.drain_rate.set(0.0)
+    f.Q_fh.fill_(0.0)
+    v = ops.enthalpy_velocity
+    v.u3d.fill_(0.0)
+    v.v3d.fill_(0.0)
+    v.omega.fill_(0.0)
+    return ops
+
+
+def _steady(ops, tol, max_steps=5000):
+    """Implicit steps with a growing time step until the column's relative
+    change per step falls below tol: dt starts at 100 kyr and grows by half
+    whenever the change is below 1 %, up to 1e6 kyr.  Returns (steps,
+    converged)."""
+    E = ops.enthalpy_state.E
+    dt, dt_max = 100.0 * SEC_PER_KYR, 1e6 * SEC_PER_KYR
+    for step in range(1, max_steps + 1):
+        before = E[2, 2, :].clone()
+        ops.set_rhs()
+        ops.column_sweep(dt, 20)
+        after = E[2, 2, :]
+        change = float((after - before).abs().max()) / (float(after.abs().max()) + 1.0)
+        if change < 1e-2:
+            dt = min(1.5 * dt, dt_max)
+        if change < tol:
+            return step, True
+    return max_steps, False
+
+
+# ------------------------------------------------------------ Stefan slab
+STEFAN_T_S, STEFAN_Q = 223.15, 0.5
+
+
+def _e_pmp(sigma, H):
+    from glide_b200.enthalpy import BETA_CC, C_I, GRAVITY, RHO_I, T_MELT, T_REF
+    return C_I * (T_MELT - BETA_CC * RHO_I * GRAVITY * (1.0 - sigma) * H - T_REF)
+
+
+def test_temperate_bed_keeps_geothermal_flux():
+    from glide_b200.enthalpy import E_SCALE
+    ops = _static_column(21, STEFAN_T_S, STEFAN_Q)
+    Ew = (_e_pmp(0.0, 1000.0) + 1000.0) / E_SCALE  # 1 kJ/kg above melting at the bed
+    ops.enthalpy_state.E.fill_(Ew)
+    ops.enthalpy_state.E_prev.fill_(Ew)
+    ops.set_rhs()
+    ops.compute_residual(1000.0 * SEC_PER_KYR)
+    r_bed = float(ops.r_E[2, 2, 0])
+    # uniform state: only the Neumann flux over the half cell at the bed
+    half = 0.5 * float(ops.sigma[1] - ops.sigma[0])
+    expected = -STEFAN_Q / (half * E_SCALE)
+    assert np.isclose(r_bed, expected, rtol=1e-3, atol=1e-2), (r_bed, expected)
+
+
+def test_temperate_bed_not_clamped_to_melting_point():
+    from glide_b200.enthalpy import E_SCALE
+    ops = _static_column(21, STEFAN_T_S, STEFAN_Q)
+    Ew = (_e_pmp(0.0, 1000.0) + 1000.0) / E_SCALE
+    ops.enthalpy_state.E.fill_(Ew)
+    ops.enthalpy_state.E_prev.fill_(Ew)
+    ops.set_rhs()
+    ops.column_sweep(1000.0 * SEC_PER_KYR, 5)
+    assert float(ops.enthalpy_state.E[0, 0, 0]) * E_SCALE > _e_pmp(0.0, 1000.0)
+
+
+def test_stefan_steady_polythermal_profile():
+    from scipy.optimize import brentq
+
+    from glide_b200.enthalpy import C_I, E_SCALE, K_COLD, K_I, K_TEMP, L_HEAT, T_REF
+    H, nz = 1000.0, 41
+    ops = _static_column(nz, STEFAN_T_S, STEFAN_Q)
+    sigma = np.linspace(0.0, 1.0, nz)
+    T_pmp = lambda s: _e_pmp(s, H) / C_I + T_REF
+    # the flux must exceed what a cold column can conduct
+    assert STEFAN_Q > K_I * (T_pmp(0.0) - STEFAN_T_S) / H
+    # cold-temperate transition: where the cold zone's linear profile meets melting
+    s_star = brentq(lambda s: STEFAN_Q * H * (1.0 - s) / K_I - (T_pmp(s) - STEFAN_T_S), 0.0, 1.0 - 1e-10)
+    E_ref = np.where(sigma <= s_star,
+                     _e_pmp(s_star, H) + STEFAN_Q * H / K_TEMP * (s_star - sigma),
+                     C_I * (STEFAN_T_S - T_REF) + STEFAN_Q * H / K_COLD * (1.0 - sigma))
+    T_ref = np.minimum(E_ref / C_I + T_REF, np.array([T_pmp(s) for s in sigma]))
+    w_ref_bed = max(E_ref[0] - _e_pmp(0.0, H), 0.0) / L_HEAT
+    steps, ok = _steady(ops, 1e-5)
+    assert ok, steps
+    E = ops.enthalpy_state.E[2, 2, :].cpu().numpy() * E_SCALE
+    T = ops.get_temperature()[2, 2, :].cpu().numpy()
+    w_bed = float(ops.get_water_content()[2, 2, 0])
+    T_err = np.abs(T[:-1] - T_ref[:-1]).max()
+    E_err = np.abs(E[:-1] - E_ref[:-1]).max() / np.abs(E_ref[:-1]).max()
+    w_err = abs(w_bed - w_ref_bed) / w_ref_bed
+    print(f"Stefan column: {steps} steps, T {T_err:.2e} K, E {E_err:.2e}, basal water {w_err:.2e}")
+    assert T_err < 0.1 and E_err < 0.02 and w_err < 0.02, (T_err, E_err, w_err)
+
+
+# ------------------------------------------------------ sigma advection
+def test_constant_sigma_advection_profile():
+    """Steady rho w dE/dsigma = (K / H^2) d2E/dsigma2 with w constant and
+    downward, Pe = rho w H^2 / K = -5: E = A + B exp(Pe sigma) with
+    E(1) = E_s and dE/dsigma(0) = -H Q / K."""
+    from glide_b200.enthalpy import BETA_CC, C_I, E_SCALE, GRAVITY, K_COLD, RHO_I, T_MELT, T_REF
+    H, nz, T_s, Q, Pe = 1000.0, 41, 243.15, 0.04, -5.0
+    ops = _static_column(nz, T_s, Q)
+    ops.enthalpy_velocity.omega.fill_(float(np.float32(Pe * K_COLD / (RHO_I * H))))  # omega = H w
+    sigma = np.linspace(0.0, 1.0, nz)
+    B = -H * Q / (K_COLD * Pe)
+    A = C_I * (T_s - T_REF) - B * np.exp(Pe)
+    E_ref = A + B * np.exp(Pe * sigma)
+    assert E_ref[0] / C_I + T_REF < T_MELT - BETA_CC * RHO_I * GRAVITY * H  # the bed stays cold
+    steps, ok = _steady(ops, 1e-6)
+    assert ok, steps
+    E = ops.enthalpy_state.E[2, 2, :].cpu().numpy() * E_SCALE
+    err = np.abs(E[:-1] - E_ref[:-1]).max() / np.abs(E_ref[:-1]).max()
+    print(f"sigma advection Pe = -5: {steps} steps, E {err:.2e}")
+    assert err < 0.02, err
+
+
+# -------------------------------------------------- horizontal advection
+def _advection_slab(ny, nx, nz):
+    ops = _slab(ny, nx, nz, 1000.0)
+    f = ops.enthalpy_forcing
+    f.Q_geo.fill_(0.0)
+    f.Q_fh.fill_(0.0)
+    f.phi_strain.fill_(0.0)
+    f.drain_rate.set(0.0)
+    ops.enthalpy_velocity.omega.fill_(0.0)
+    ops.term_flags.omega = False
+    ops.term_flags.drainage = False
+    return ops
+
+
+def test_divergent_velocity_stays_bounded():
+    ny, nx, nz, T0 = 8, 8, 9, 248.15
+    ops = _advection_slab(ny, nx, nz)
+    ops.initialize_from_temperature(T0)
+    ops.set_surface_enthalpy_from_temperature(torch.full((ny, nx), T0, dtype=torch.float64))
+    # u = alpha x on the u faces, in m/s: div(H u) != 0, so uniform E
+    # sees a nonzero conservative flux divergence
+    u = torch.as_tensor(np.float32(1e-10) * np.arange(nx + 1, dtype=np.float32) * np.float32(1000.0),
+                        dtype=torch.float64, device="cuda")
+    ops.enthalpy_velocity.u3d[:] = u.expand(nz, ny, nx + 1)
+    ops.enthalpy_velocity.v3d.fill_(0.0)
+    dt = 100.0 * 365.25 * 86400.0
+    ops.set_rhs()
+    r0 = float(ops.compute_residual(dt))
+    ops.set_rhs()
+    ops.column_sweep(dt, 5)
+    E = ops.enthalpy_state.E.cpu().numpy()
+    assert np.isfinite(r0) and np.isfinite(E).all()
+    assert (E.max() - E.min()) < 1.0  # bounded: within E_SCALE of the start (scaled units)
+
+
+def _step_state(ny, nx, nz, T_of_j):
+    from glide_b200.enthalpy import C_I, E_SCALE, T_REF
+    ops = _advection_slab(ny, nx, nz)
+    T = np.array([T_of_j(j) for j in range(nx)], dtype=np.float32)
+    E = torch.as_tensor(C_I * (np.broadcast_to(T[None, :, None], (ny, nx, nz)) - T_REF) / E_SCALE,
+                        dtype=torch.float64, device="cuda")
+    ops.enthalpy_state.E[:] = E
+    ops.enthalpy_state.E_prev[:] = ops.enthalpy_state.E
+    ops.enthalpy_velocity.v3d.fill_(0.0)
+    return ops
+
+
+def test_uniform_velocity_keeps_rows_identical():
+    from glide_b200.enthalpy import E_SCALE
+    ny, nx, nz = 8, 16, 9
+    ops = _step_state(ny, nx, nz, lambda j: 260.0 if j >= nx // 2 else 240.0)
+    ops.set_surface_enthalpy_from_temperature(torch.full((ny, nx), 240.0, dtype=torch.float64))
+    ops.enthalpy_velocity.u3d.fill_(float(np.float32(100.0 / (365.25 * 86400.0))))
+    for _ in range(3):
+        ops.set_rhs()
+        ops.column_sweep(10.0 * 365.25 * 86400.0, 20)
+    E = ops.enthalpy_state.E[:, :, nz // 2].cpu().numpy()
+    spread = (E.max(axis=0) - E.min(axis=0)).max()
+    assert spread < 1.0, spread
+
+
+def test_interior_energy_conserved():
+    ny, nx, nz = 8, 16, 5
+    mid, amp = 250.0, 10.0
+    ops = _step_state(ny, nx, nz, lambda j: mid + amp * np.sin(2 * np.pi * j / nx))
+    ops.set_surface_enthalpy_from_temperature(torch.full((ny, nx), mid, dtype=torch.float64))
+    ops.enthalpy_velocity.u3d.fill_(float(np.float32(50.0 / (365.25 * 86400.0))))
+    H = ops.grid.state.H.data
+
+    def interior_energy():
+        # away from the domain edges, below the surface Dirichlet layer
+        return float((H[2:-2, 2:-2, None] * ops.enthalpy_state.E[2:-2, 2:-2, :-1]).sum())
+
+    e0 = interior_energy()
+    ops.set_rhs()
+    ops.column_sweep(365.25 * 86400.0, 20)
+    change = abs(interior_energy() - e0) / abs(e0)
+    assert change < 0.01, change
