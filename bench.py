@@ -896,6 +896,7 @@ def thermal_leg(a, h, f, stream, dev, world):
             ops.column_smooth(dt_s)
         return fn
     for name, fn in (("k_enth_column_s", column("smem")),
+                     ("k_enth_column_s (6 blocks per SM)", column("smem6")),
                      ("k_enth_column (per-thread arrays)", column("local")),
                      ("k_enth_layer", lambda: ops.layer_smooth(dt_s)),
                      ("k_enth_residual", lambda: ops.compute_residual(dt_s))):

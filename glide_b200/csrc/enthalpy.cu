@@ -114,6 +114,7 @@ struct Handle {
     double* f[GLIDE_ENTH_N_FIELDS] = {};
     double* E_alt = nullptr;
     double* rowc = nullptr;  // per-row constants of the on-chip column smoother
+    double* dpr = nullptr;   // its Thomas factors d'_k
     double* partial = nullptr;
     SweepCtl* ctl = nullptr;
     SweepCtl* ctl_host = nullptr;
@@ -121,7 +122,6 @@ struct Handle {
     glide_enthalpy_config cfg;
     glide_enthalpy_inputs in;
     int point_blocks = 3;   // resident blocks per SM of the residual / layer kernels (3 to 6)
-    bool smem_attr_set = false;
     // Kernels launched and their algorithmic bytes: the binary64 values each
     // must read and write once.  A residual, column or layer pass moves
     // (5 nz + 7) values per column: E, E_prev, f_E, omega and the output at
@@ -132,7 +132,7 @@ struct Handle {
     void acct(long long n, double bytes) { launches += n; alg_bytes += bytes; }
     double pass_bytes() const { return double(5 * nz + 7) * 8.0 * double(plane); }
     int column_blocks = 4;  // of the column kernel (2 to 6)
-    int column_kernel = 1;  // 1: factors in shared memory (k_enth_column_s); 0: per-thread arrays
+    int column_kernel = 1;  // 1 / 2: k_enth_column_s at 8 / 6 blocks per SM; 0: per-thread arrays
 
     Handle(int ny_, int nx_, int nz_, double dx_) : ny(ny_), nx(nx_), nz(nz_), dx(dx_) {
         plane = size_t(ny) * nx;
@@ -141,7 +141,7 @@ struct Handle {
         nv3 = size_t(nz) * (ny + 1) * nx;
         nblocks = int((plane + kColThreads - 1) / kColThreads);
         auto up = [](size_t n) { return (n + 31) / 32 * 32; };  // 256-byte aligned starts
-        size_t total = 9 * up(n3) + up(nu3) + up(nv3) + 4 * up(plane) + up(size_t(nblocks)) +
+        size_t total = 10 * up(n3) + up(nu3) + up(nv3) + 4 * up(plane) + up(size_t(nblocks)) +
                        up(sizeof(SweepCtl) / sizeof(double) + 1);
         ECU(cudaMalloc(&arena, total * sizeof(double)));
         ECU(cudaMemset(arena, 0, total * sizeof(double)));
@@ -152,6 +152,7 @@ struct Handle {
             f[fld] = take(n3);
         E_alt = take(n3);
         rowc = take(n3);
+        dpr = take(n3);
         f[GLIDE_ENTH_U3D] = take(nu3);
         f[GLIDE_ENTH_V3D] = take(nv3);
         for (int fld : {GLIDE_ENTH_H_PREV, GLIDE_ENTH_E_SURFACE, GLIDE_ENTH_Q_GEO, GLIDE_ENTH_Q_FH})
@@ -226,15 +227,11 @@ struct Handle {
         check_launch("enthalpy residual");
     }
     void column(const EnthArgs& a, double* out, int mode, cudaStream_t s) {
-        if (column_kernel == 1) {
-            const size_t smem = size_t(2) * nz * kColSmemThreads * sizeof(double);
-            if (!smem_attr_set) {
-                ECU(cudaFuncSetAttribute(k_enth_column_s<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(size_t(2) * kMaxNz * kColSmemThreads * sizeof(double))));
-                smem_attr_set = true;
-            }
+        if (column_kernel >= 1) {
+            const size_t smem = size_t(nz) * kColSmemThreads * sizeof(double);
             const unsigned blocks = unsigned((plane + kColSmemThreads - 1) / kColSmemThreads);
-            k_enth_column_s<5><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, mode);
+            if (column_kernel == 2) k_enth_column_s<6><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, dpr, mode);
+            else k_enth_column_s<8><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, dpr, mode);
             check_launch("enthalpy column smooth (on-chip factors)");
             return;
         }
@@ -344,7 +341,7 @@ int glide_enthalpy_set_tuning(glide_enthalpy_handle h, int key, int value) {
             if (value < 2 || value > 6) fail(GLIDE_ERR_ARG, "column blocks per SM must lie in [2, 6]");
             e->column_blocks = value;
         } else if (key == GLIDE_ENTH_TUNE_COLUMN_KERNEL) {
-            if (value < 0 || value > 1) fail(GLIDE_ERR_ARG, "column kernel must be 0 or 1");
+            if (value < 0 || value > 2) fail(GLIDE_ERR_ARG, "column kernel must be 0, 1 or 2");
             e->column_kernel = value;
         } else if (key == GLIDE_ENTH_TUNE_COLUMN_L1) {
             const int carve = value ? int(cudaSharedmemCarveoutMaxL1) : int(cudaSharedmemCarveoutDefault);

@@ -470,26 +470,150 @@ __global__ void __launch_bounds__(kColThreads, MINB) k_enth_column(EnthArgs a, d
 // ---------------------------------------- column smoother, on-chip factors
 // The same smoother as k_enth_column, organised so that nothing per column
 // has to live in local memory:
-//  * the Thomas factors c'_k, d'_k sit in shared memory, laid out [k][thread]
-//    so a warp's accesses fall in distinct banks;
-//  * the Newton iterate lives in `out` (layer-major, coalesced), whose
-//    in-flight footprint (nz values per resident column) stays in L2;
+//  * the Thomas factor c'_k sits in shared memory, laid out [k][thread] so a
+//    warp's accesses fall in distinct banks; d'_k goes to a layer-major
+//    scratch array (`dpr`) and the Newton iterate lives in `out`, both
+//    coalesced, with an in-flight footprint (2 nz values per resident
+//    column) that stays in L2;
 //  * on the first Newton iteration the part of each row that does not depend
 //    on the column iterate -- the old time level, the forcing and, for a
 //    layer-independent velocity, the frozen neighbours' share of the
 //    horizontal flux -- is folded into one constant per row, stored in
 //    `rowc`; later iterations read it and omega instead of the seven row
-//    inputs, and the horizontal diagonal is a column constant.
+//    inputs, and the horizontal diagonal is a column constant;
+//  * the back substitution loads d'_k and the iterate four rows ahead, so its
+//    serial chain does not wait on memory at every row.
 // The rows are the same expressions regrouped (the time term split as
 // rho H E / dt - rho H_prev E_prev / dt, the horizontal flux as its diagonal
 // times E plus the neighbours' share), so results agree with k_enth_column
 // to rounding.  The last Newton iteration's back substitution writes the
-// smoother output directly.  Dynamic shared memory: 2 nz blockDim doubles.
+// smoother output directly.  Dynamic shared memory: nz blockDim doubles.
 constexpr int kColSmemThreads = 64;
+
+// Per-column constants of k_enth_column_s.
+struct ColS {
+    double bt, ct_old, hd_flat, Es;
+    bool hadv, fold;
+};
+
+// One Newton step of one column: rows assembled and eliminated upward,
+// then back-substituted.  FIRST: the iterate is E, the row inputs are read
+// and the row constants written; otherwise the iterate is `El` and the row
+// constants are read.
+template <bool FIRST>
+__device__ __forceinline__ void column_newton_step(const EnthArgs& a, const ColumnCtx& x, const Clamped& cl,
+                                                   const HCtx& hc, const ColTerms& ct, const ColS& cs,
+                                                   const double* E, double* El, double* C, double* Dp,
+                                                   double* cps, int bd, bool last, int mode) {
+    const int nz = a.nz;
+    const size_t plane = size_t(a.ny) * a.nx;
+    const double dsig = 1.0 / double(nz - 1);
+    const double* om = a.omega + x.c;
+    const double* src = FIRST ? E : El;
+    double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
+    double K_lo = 0.0, om_m = 0.0, om_k = om[0];
+    double c_prev = 0.0, d_prev = 0.0;
+    double Ekm1 = 0.0, Ek = src[0], Ekp1 = src[plane];
+    // row k + 1's inputs are loaded while row k is assembled
+    RowIn in = FIRST ? row_inputs(a, x, 0, cs.hadv, true) : no_row();
+    double Cn = FIRST ? 0.0 : C[0];
+    double om_n = FIRST ? 0.0 : om[plane];
+    for (int k = 0; k < nz - 1; ++k) {
+        const double E_n = k + 2 < nz ? src[size_t(k + 2) * plane] : 0.0;
+        double ck, om_p;
+        RowIn in_n = no_row();
+        if (FIRST) {
+            if (k + 1 < nz - 1) in_n = row_inputs(a, x, k + 1, cs.hadv, true);
+            // the row constant: old time level, forcing, frozen neighbours
+            ck = -cs.ct_old * in.ep - in.fe;
+            if (cs.fold) ck += row_horiz(a, x, hc, k, 0.0, in.nb).res;
+            C[size_t(k) * plane] = ck;
+            om_p = in.om_p;
+        } else {
+            ck = Cn;
+            om_p = om_n;
+            if (k + 1 < nz - 1) {
+                Cn = C[size_t(k + 1) * plane];
+                om_n = om[size_t(k + 2) * plane];
+            }
+        }
+        const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
+        double r = cs.bt * Ek + ck;
+        double hd = cs.hd_flat;
+        if (cs.fold) {
+            r += cs.hd_flat * Ek;
+        } else if (cs.hadv) {
+            const Nbr nb = FIRST ? in.nb : neighbours(a, x, k);
+            HAdv ha = row_horiz(a, x, hc, k, Ek, nb);
+            r += ha.res;
+            hd = ha.diag;
+        }
+        Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl, ct);
+        r += vt.adv;
+        r += vt.dif;
+        r += vt.drn;
+        const double b = cs.bt + vt.b_dif + vt.b_adv + vt.b_drn + hd;
+        // elimination: b' = b - a c'_{k-1}; c'_k = c / b'; d'_k = (rhs - a d'_{k-1}) / b'
+        const double bp = b - vt.a * c_prev;
+        const double inv = 1.0 / bp;
+        c_prev = vt.c * inv;
+        d_prev = (-r - vt.a * d_prev) * inv;
+        cps[size_t(k) * bd] = c_prev;
+        Dp[size_t(k) * plane] = d_prev;
+        Epk = Epp;
+        Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
+        K_lo = K_up;
+        om_m = om_k; om_k = om_p;
+        Ekm1 = Ek; Ek = Ekp1; Ekp1 = E_n;
+        if (FIRST) in = in_n;
+    }
+    // surface Dirichlet row: E = E_surface (a = c = 0, b = 1), then back
+    // substitution; the last Newton step writes the smoother output.  The
+    // iterate, d'_k and (on the last step) the input state of row k are
+    // loaded kPre rows ahead into a register ring.
+    const double top = src[size_t(nz - 1) * plane];
+    double xk = -(top - cs.Es);
+    double en = top + a.relaxation * xk;
+    if (last) {
+        const double E0 = E[size_t(nz - 1) * plane];
+        El[size_t(nz - 1) * plane] = mode ? E0 + a.omega_relax * (en - E0) : en - E0;
+    } else {
+        El[size_t(nz - 1) * plane] = en;
+    }
+    constexpr int kPre = 4;
+    const bool want_e = last && !FIRST;
+    double ps[kPre], pd[kPre], pe[kPre];
+#pragma unroll
+    for (int q = 0; q < kPre; ++q) {
+        const int k = nz - 2 - q;
+        ps[q] = k >= 0 ? src[size_t(k) * plane] : 0.0;
+        pd[q] = k >= 0 ? Dp[size_t(k) * plane] : 0.0;
+        pe[q] = (want_e && k >= 0) ? E[size_t(k) * plane] : 0.0;
+    }
+#pragma unroll kPre
+    for (int q = 0; q < nz - 1; ++q) {
+        const int k = nz - 2 - q, slot = q % kPre;
+        const double sk = ps[slot], dk = pd[slot], ek = pe[slot];
+        const int kn = k - kPre;
+        if (kn >= 0) {
+            ps[slot] = src[size_t(kn) * plane];
+            pd[slot] = Dp[size_t(kn) * plane];
+            if (want_e) pe[slot] = E[size_t(kn) * plane];
+        }
+        xk = dk - cps[size_t(k) * bd] * xk;
+        en = sk + a.relaxation * xk;
+        if (last) {
+            const double E0 = FIRST ? sk : ek;
+            El[size_t(k) * plane] = mode ? E0 + a.omega_relax * (en - E0) : en - E0;
+        } else {
+            El[size_t(k) * plane] = en;
+        }
+    }
+}
 
 template <int MINB>
 __global__ void __launch_bounds__(kColSmemThreads, MINB)
-    k_enth_column_s(EnthArgs a, double* out, double* rowc, int mode) {
+    k_enth_column_s(EnthArgs a, double* out, double* rowc, double* dpr, int mode) {
     extern __shared__ double sm[];
     if (stopped(a.done)) return;
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -500,7 +624,6 @@ __global__ void __launch_bounds__(kColSmemThreads, MINB)
     const ColumnCtx x = column_ctx(a, i, j);
     const double* E = a.E + x.c;
     double* El = out + x.c;
-    double* C = rowc + x.c;
     const double dsig = 1.0 / double(nz - 1);
     const double Es = a.E_s[x.c];
     if (x.h < a.h_thin) {
@@ -516,126 +639,23 @@ __global__ void __launch_bounds__(kColSmemThreads, MINB)
         for (int k = 0; k < nz; ++k) El[size_t(k) * plane] = mode ? E[size_t(k) * plane] : 0.0;
         return;
     }
-    const int bd = blockDim.x;
-    double* cps = sm + threadIdx.x;                      // c'_k at cps[k * bd]
-    double* dps = sm + size_t(nz) * bd + threadIdx.x;    // d'_k at dps[k * bd]
+    double* cps = sm + threadIdx.x;  // c'_k at cps[k * blockDim.x]
     const Clamped cl;
     const HCtx hc(a, x);
     const ColTerms ct(a, cl, x.h, dsig);
+    ColS cs;
     const double inv_dt = 1.0 / a.dt;
-    const double* om = a.omega + x.c;
-    const double bt = kRhoI * x.h * inv_dt;          // time-term diagonal
-    const double ct_old = kRhoI * x.h_prev * inv_dt;  // time-term weight of E_prev
-    const bool hadv = (a.flags & kTermHorizAdv) != 0;
-    const bool fold = hadv && hc.flat;                // horizontal flux folded into the row constants
-    const double hd_flat = fold ? horiz_vals(a, x, 0.0, Nbr{0.0, 0.0, 0.0, 0.0}, hc.q, hc.sq, hc.dx_inv).diag
-                                : 0.0;
-    for (int it = 0; it < a.n_newton; ++it) {
-        const bool first = it == 0, last = it + 1 == a.n_newton;
-        const double* src = first ? E : El;  // the iterate entering this Newton step
-        double Epk = e_pmp(0.0, x.h), Epp = e_pmp(dsig, x.h);
-        double K_lo = 0.0, om_m = 0.0, om_k = om[0];
-        double c_prev = 0.0, d_prev = 0.0;
-        double Ekm1 = 0.0, Ek = src[0], Ekp1 = src[plane];
-        // row k + 1's inputs are loaded while row k is assembled
-        RowIn in = first ? row_inputs(a, x, 0, hadv, true) : no_row();
-        double Cn = first ? 0.0 : C[0];
-        double om_n = first ? 0.0 : om[plane];
-        for (int k = 0; k < nz - 1; ++k) {
-            RowIn in_n = no_row();
-            double Cnn = 0.0, om_nn = 0.0;
-            if (first) {
-                if (k + 1 < nz - 1) in_n = row_inputs(a, x, k + 1, hadv, true);
-            } else if (k + 1 < nz - 1) {
-                Cnn = C[size_t(k + 1) * plane];
-                om_nn = om[size_t(k + 2) * plane];
-            }
-            const double E_n = k + 2 < nz ? src[size_t(k + 2) * plane] : 0.0;
-            double ck, om_p;
-            if (first) {
-                // the row constant: old time level, forcing, frozen neighbours
-                ck = -ct_old * in.ep - in.fe;
-                if (fold) ck += row_horiz(a, x, hc, k, 0.0, in.nb).res;
-                C[size_t(k) * plane] = ck;
-                om_p = in.om_p;
-            } else {
-                ck = Cn;
-                om_p = om_n;
-            }
-            const double K_up = k_diff(0.5 * (Ek + Ekp1), 0.5 * (Epk + Epp), cl);
-            double r = bt * Ek + ck;
-            double hd = hd_flat;
-            if (fold) {
-                r += hd_flat * Ek;
-            } else if (hadv) {
-                const Nbr nb = first ? in.nb : neighbours(a, x, k);
-                HAdv ha = row_horiz(a, x, hc, k, Ek, nb);
-                r += ha.res;
-                hd = ha.diag;
-            }
-            Vert vt = vertical(a, k, Ekm1, Ek, Ekp1, Epk, K_lo, K_up, om_m, om_k, om_p, x.h, x.h_inv, dsig, cl, ct);
-            r += vt.adv;
-            r += vt.dif;
-            r += vt.drn;
-            const double b = bt + vt.b_dif + vt.b_adv + vt.b_drn + hd;
-            // elimination: b' = b - a c'_{k-1}; c'_k = c / b'; d'_k = (rhs - a d'_{k-1}) / b'
-            const double bp = b - vt.a * c_prev;
-            const double inv = 1.0 / bp;
-            c_prev = vt.c * inv;
-            d_prev = (-r - vt.a * d_prev) * inv;
-            cps[size_t(k) * bd] = c_prev;
-            dps[size_t(k) * bd] = d_prev;
-            Epk = Epp;
-            Epp = e_pmp(double(k + 2 < nz ? k + 2 : nz - 1) * dsig, x.h);
-            K_lo = K_up;
-            om_m = om_k; om_k = om_p;
-            Ekm1 = Ek; Ek = Ekp1; Ekp1 = E_n;
-            in = in_n;
-            Cn = Cnn;
-            om_n = om_nn;
-        }
-        // surface Dirichlet row: E = E_surface (a = c = 0, b = 1), then back
-        // substitution; the last Newton step writes the smoother output
-        const double top = src[size_t(nz - 1) * plane];
-        double xk = -(top - Es);
-        double en = top + a.relaxation * xk;
-        if (last) {
-            const double E0 = E[size_t(nz - 1) * plane];
-            El[size_t(nz - 1) * plane] = mode ? E0 + a.omega_relax * (en - E0) : en - E0;
-        } else {
-            El[size_t(nz - 1) * plane] = en;
-        }
-        // The iterate (and, on the last Newton step, the input state) of row
-        // k is loaded kPre rows ahead, into a register ring, so the serial
-        // substitution does not wait on a load at every row.
-        constexpr int kPre = 4;
-        const bool want_e = last && !first;
-        double ps[kPre], pe[kPre];
-#pragma unroll
-        for (int q = 0; q < kPre; ++q) {
-            const int k = nz - 2 - q;
-            ps[q] = k >= 0 ? src[size_t(k) * plane] : 0.0;
-            pe[q] = (want_e && k >= 0) ? E[size_t(k) * plane] : 0.0;
-        }
-#pragma unroll kPre
-        for (int q = 0; q < nz - 1; ++q) {
-            const int k = nz - 2 - q, slot = q % kPre;
-            const double sk = ps[slot], ek = pe[slot];
-            const int kn = k - kPre;
-            if (kn >= 0) {
-                ps[slot] = src[size_t(kn) * plane];
-                if (want_e) pe[slot] = E[size_t(kn) * plane];
-            }
-            xk = dps[size_t(k) * bd] - cps[size_t(k) * bd] * xk;
-            en = sk + a.relaxation * xk;
-            if (last) {
-                const double E0 = first ? sk : ek;
-                El[size_t(k) * plane] = mode ? E0 + a.omega_relax * (en - E0) : en - E0;
-            } else {
-                El[size_t(k) * plane] = en;
-            }
-        }
-    }
+    cs.bt = kRhoI * x.h * inv_dt;          // time-term diagonal
+    cs.ct_old = kRhoI * x.h_prev * inv_dt;  // time-term weight of E_prev
+    cs.hadv = (a.flags & kTermHorizAdv) != 0;
+    cs.fold = cs.hadv && hc.flat;           // horizontal flux folded into the row constants
+    cs.hd_flat = cs.fold ? horiz_vals(a, x, 0.0, Nbr{0.0, 0.0, 0.0, 0.0}, hc.q, hc.sq, hc.dx_inv).diag : 0.0;
+    cs.Es = Es;
+    double* C = rowc + x.c;
+    double* Dp = dpr + x.c;
+    column_newton_step<true>(a, x, cl, hc, ct, cs, E, El, C, Dp, cps, blockDim.x, a.n_newton == 1, mode);
+    for (int it = 1; it < a.n_newton; ++it)
+        column_newton_step<false>(a, x, cl, hc, ct, cs, E, El, C, Dp, cps, blockDim.x, it + 1 == a.n_newton, mode);
 }
 
 // ---------------------------------------------------------- layer smoother

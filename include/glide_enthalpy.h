@@ -119,10 +119,11 @@ int glide_enthalpy_set_inputs(glide_enthalpy_handle h, const glide_enthalpy_inpu
 #define GLIDE_ENTH_TUNE_POINT_BLOCKS 1
 #define GLIDE_ENTH_TUNE_COLUMN_BLOCKS 2
 #define GLIDE_ENTH_TUNE_COLUMN_L1 3
-/* GLIDE_ENTH_TUNE_COLUMN_KERNEL: 1 (default) runs the column smoother with its
- * Thomas factors in shared memory and the iterate in the output array; 0 runs
- * the one-thread-per-column kernel with per-thread arrays (results agree to
- * rounding). */
+/* GLIDE_ENTH_TUNE_COLUMN_KERNEL: 1 (default) runs the column smoother with one
+ * Thomas factor in shared memory, the other and the iterate in L2-resident
+ * arrays, sized for 8 resident blocks of 64 threads per SM; 2 the same sized
+ * for 6 (more registers per thread); 0 the one-thread-per-column kernel with
+ * per-thread arrays.  Results agree to rounding. */
 #define GLIDE_ENTH_TUNE_COLUMN_KERNEL 4
 int glide_enthalpy_set_tuning(glide_enthalpy_handle h, int key, int value);
 int glide_enthalpy_snapshot(glide_enthalpy_handle h, void* stream);
