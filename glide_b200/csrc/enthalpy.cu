@@ -132,7 +132,7 @@ struct Handle {
     void acct(long long n, double bytes) { launches += n; alg_bytes += bytes; }
     double pass_bytes() const { return double(5 * nz + 7) * 8.0 * double(plane); }
     int column_blocks = 4;  // of the column kernel (2 to 6)
-    int column_kernel = 1;  // 1 / 2: k_enth_column_s at 8 / 6 blocks per SM; 0: per-thread arrays
+    int column_kernel = 1;  // 1 / 2: k_enth_column_s at 6 / 8 blocks per SM; 0: per-thread arrays
 
     Handle(int ny_, int nx_, int nz_, double dx_) : ny(ny_), nx(nx_), nz(nz_), dx(dx_) {
         plane = size_t(ny) * nx;
@@ -230,8 +230,8 @@ struct Handle {
         if (column_kernel >= 1) {
             const size_t smem = size_t(nz) * kColSmemThreads * sizeof(double);
             const unsigned blocks = unsigned((plane + kColSmemThreads - 1) / kColSmemThreads);
-            if (column_kernel == 2) k_enth_column_s<6><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, dpr, mode);
-            else k_enth_column_s<8><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, dpr, mode);
+            if (column_kernel == 2) k_enth_column_s<8><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, dpr, mode);
+            else k_enth_column_s<6><<<blocks, kColSmemThreads, smem, s>>>(a, out, rowc, dpr, mode);
             check_launch("enthalpy column smooth (on-chip factors)");
             return;
         }

@@ -256,11 +256,11 @@ class EnthalpyOperators:
     def set_tuning(self, point_blocks_per_sm=None, column_blocks_per_sm=None, column_prefers_l1=None,
                    column_kernel=None):
         """Launch shapes of the kernels (no counterpart in the reference).
-        column_kernel: "smem" (default; on-chip factors, 8 blocks of 64
-        threads per SM), "smem6" (the same at 6 blocks per SM) or "local"
+        column_kernel: "smem" (default; on-chip factors, 6 blocks of 64
+        threads per SM), "smem8" (the same at 8 blocks per SM) or "local"
         (per-thread arrays)."""
         if column_kernel is not None:
-            _ecall("glide_enthalpy_set_tuning", self._h, 4, {"local": 0, "smem": 1, "smem6": 2}[column_kernel])
+            _ecall("glide_enthalpy_set_tuning", self._h, 4, {"local": 0, "smem": 1, "smem8": 2}[column_kernel])
         if point_blocks_per_sm is not None:
             _ecall("glide_enthalpy_set_tuning", self._h, 1, int(point_blocks_per_sm))
         if column_blocks_per_sm is not None:

@@ -121,8 +121,8 @@ int glide_enthalpy_set_inputs(glide_enthalpy_handle h, const glide_enthalpy_inpu
 #define GLIDE_ENTH_TUNE_COLUMN_L1 3
 /* GLIDE_ENTH_TUNE_COLUMN_KERNEL: 1 (default) runs the column smoother with one
  * Thomas factor in shared memory, the other and the iterate in L2-resident
- * arrays, sized for 8 resident blocks of 64 threads per SM; 2 the same sized
- * for 6 (more registers per thread); 0 the one-thread-per-column kernel with
+ * arrays, sized for 6 resident blocks of 64 threads per SM; 2 the same sized
+ * for 8 (fewer registers per thread); 0 the one-thread-per-column kernel with
  * per-thread arrays.  Results agree to rounding. */
 #define GLIDE_ENTH_TUNE_COLUMN_KERNEL 4
 int glide_enthalpy_set_tuning(glide_enthalpy_handle h, int key, int value);

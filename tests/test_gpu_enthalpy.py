@@ -185,7 +185,7 @@ def test_column_kernels_agree_and_match_oracle(nz, flat):
         st["v3d"] = np.ascontiguousarray(np.broadcast_to(st["v3d"][0], st["v3d"].shape))
     cfg = enthalpy_config(relative_tolerance=1e-30, absolute_tolerance=0.0)
     out = {}
-    for kernel in ("local", "smem6", "smem"):
+    for kernel in ("local", "smem8", "smem"):
         ops = _ops(st, cfg["dx"], nz)
         if flat:
             ops.grid.state.u.set(torch.as_tensor(st["u3d"][0]))
@@ -202,4 +202,4 @@ def test_column_kernels_agree_and_match_oracle(nz, flat):
             eo.column_sweep(s, cfg, 3)
             assert rel_err(_np(ops.enthalpy_state.E), s["E"]) <= 1e-10
     assert rel_err(out["smem"], out["local"]) <= 1e-12
-    assert rel_err(out["smem6"], out["smem"]) <= 1e-15
+    assert rel_err(out["smem8"], out["smem"]) <= 1e-15
