@@ -84,7 +84,8 @@ def parse(argv=None):
     ap.add_argument("--members", type=int, default=64, help="ensemble mode: members")
     ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
-    ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
+    ap.add_argument("--ens-precision", default="mixed", choices=["fp64", "mixed"], help="ensemble members")
+    ap.add_argument("--ens-cold-tune", action="store_true", help="ensemble: autotune on the cold first step")
     ap.add_argument("--ens-adjoint", default="fast", choices=["fast", "reference"],
                     help="ensemble adjoint: 4/4/0/50 cycles with omega 0.8, or the reference's 10/20/50/200")
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
@@ -728,7 +729,7 @@ def run_ensemble(a):
         members.append(m)
     ens = Ensemble(members, workers=a.ens_workers)
     t0 = time.perf_counter()
-    chosen = ens.autotune(a.dt)
+    chosen = ens.autotune(a.dt, warm=not a.ens_cold_tune)
     tune_s = time.perf_counter() - t0
     dJ = lambda k, m: (0.05 * m.mg.levels[0].state.u.data, 0.05 * m.mg.levels[0].state.v.data, None)
 
@@ -755,7 +756,8 @@ def run_ensemble(a):
             "mean_forward_cycles": float(np.mean(fv)), "mean_adjoint_cycles": float(np.mean(bv)),
             "worst_forward_relative_residual": worst, "forward_solves_converged": converged,
             "max_cycles": max_cycles, "workers": ens.workers, "adjoint": a.ens_adjoint,
-            "forward_retries": ens.retries,
+            "forward_retries": ens.retries, "precision": a.ens_precision,
+            "tuned_on": "cold first step" if a.ens_cold_tune else "a warm step of each class's first member",
             "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
 
 

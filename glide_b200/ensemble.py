@@ -8,8 +8,10 @@ calls release the interpreter lock, so the GPU runs kernels of many members
 at once.  A member's convergence checks synchronise only its own stream.
 
 `Ensemble.autotune` picks, per size class, the fastest of a few solver
-schedules by timing one step of the class's first member on a copy of its
-state.
+schedules and FASCD launch shapes (resident Vanka-sweep blocks per SM) by
+timing a step of the class's first member from a warm state: the member is
+first advanced one step, trials run from that state, and the member's
+original state is restored afterwards.
 
 No counterpart in the reference (its models run one grid at a time); the
 members themselves are the reference-compatible `IceDynamics`.
@@ -63,14 +65,17 @@ def member_specs(n_members: int, seed: int = 0, sizes=(128, 192, 256, 384, 512, 
     return out
 
 
-# solver schedules the autotuner chooses among (applied through the options API)
+# solver schedules the autotuner chooses among (applied through the options
+# API); blocks: resident Vanka-sweep blocks per SM of the FASCD smoother
 CANDIDATES = {
     "fast": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="newton", switch=0,
-                 tangent=(4, 4, 0, 20)),
+                 tangent=(4, 4, 0, 10), blocks=2),
     "fascd": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="fascd", switch=None,
-                  tangent=None),
+                  tangent=None, blocks=2),
+    "fascd/1": dict(quirks=False, schedule=(4, 4, 0, 50), newton_steps=3, method="fascd", switch=None,
+                    tangent=None, blocks=1),
     "classic": dict(quirks=False, schedule=(10, 20, 50, 200), newton_steps=30, method="fascd", switch=None,
-                    tangent=None),
+                    tangent=None, blocks=2),
 }
 FALLBACK = "classic"
 
@@ -87,7 +92,8 @@ def apply_schedule(model: IceDynamics, cfg: dict):
     pre, post, fin, coarse = cfg["schedule"]
     h.set_fas(False, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
     h.set_vanka(False, -1, newton_steps=cfg["newton_steps"])
-    h.set_tuning(forward_method=cfg["method"], newton_switch_exp10=cfg["switch"])
+    h.set_tuning(forward_method=cfg["method"], newton_switch_exp10=cfg["switch"],
+                 sweep_blocks_per_sm=cfg.get("blocks", 2))
     if cfg["tangent"]:
         pre, post, fin, coarse = cfg["tangent"]
         h.set_fas(2, pre_steps=pre, post_steps=post, finest_steps=fin, coarsest_steps=coarse)
@@ -188,10 +194,14 @@ class Ensemble:
             return m.backward(t, dt, dJdu=du, dJdv=dv, dJdH=dH)
         return self._run(one)
 
-    def autotune(self, dt: float, candidates: dict | None = None) -> dict[int, str]:
+    def autotune(self, dt: float, candidates: dict | None = None, warm: bool = True) -> dict[int, str]:
         """Per size class: time one forward step of the class's first member
-        from its current state with every candidate schedule (state restored
-        after each trial), keep the fastest for the whole class."""
+        with every candidate schedule, keep the fastest that converges for the
+        whole class.  With `warm`, the member is first advanced one step (the
+        "fast" schedule, the others in turn if it stops short), so the trials
+        time the warm-started steps a run is made of rather than its cold
+        first step; every trial starts from that state and the member's
+        original state is restored at the end."""
         candidates = candidates or CANDIDATES
         classes: dict[int, list[int]] = {}
         for k, m in enumerate(self.members):
@@ -200,7 +210,18 @@ class Ensemble:
         for n, ks in sorted(classes.items()):
             m = self.members[ks[0]]
             h = m.mg.hierarchy
-            saved = {f: h.get(f, 0) for f in STATE}
+            original = {f: h.get(f, 0) for f in STATE}
+            saved = original
+            if warm:
+                for name in list(candidates) + [FALLBACK]:
+                    for f, v in original.items():
+                        h.set(f, 0, v, restrict_down=True)
+                    apply_schedule(m, candidates.get(name, CANDIDATES[FALLBACK]))
+                    st = m.forward(0.0, dt, update_geometry=False)
+                    if _converged(m, st):
+                        break
+                saved = {f: h.get(f, 0) for f in STATE}
+                saved["H_prev"] = saved["H"].clone()  # the next step starts from the solved geometry
             best, best_t = None, float("inf")
             for name, cfg in candidates.items():
                 apply_schedule(m, cfg)
@@ -217,7 +238,7 @@ class Ensemble:
                 if ok and el < best_t:
                     best, best_t = name, el
             best = best or FALLBACK
-            for f, v in saved.items():
+            for f, v in original.items():
                 h.set(f, 0, v, restrict_down=True)
             for k in ks:
                 apply_schedule(self.members[k], candidates[best])
