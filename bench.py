@@ -933,8 +933,19 @@ def thermal_leg(a, h, f, stream, dev, world):
     ops.set_tuning(column_kernel="smem")
     # the residual call also reads the norm back (one small copy and a sync)
     st = getattr(ops, "last_stats", None)
+    sweeps_last = int(st.iterations) if st is not None else None
+    # ten sweeps with the stop test off: the cost of a sweep, what a step
+    # near the temperate transition (where the stop test takes longer) pays
+    cfg = ops.smoother_config
+    rtol, atol = cfg.relative_tolerance, cfg.absolute_tolerance
+    cfg.relative_tolerance, cfg.absolute_tolerance = 0.0, 0.0
+    ops.column_sweep(dt_s, 10)
+    sweep10_ms = event_time(lambda: ops.column_sweep(dt_s, 10), 1, stream)
+    cfg.relative_tolerance, cfg.absolute_tolerance = rtol, atol
+    forced = int(ops.last_stats.iterations)
     return {"ms_per_step": t_ms, "steps_per_s": world * 1000.0 / t_ms, "nz": a.nz, "columns": ncol,
-            "sweeps_last_step": int(st.iterations) if st is not None else None,
+            "sweeps_last_step": sweeps_last,
+            "ten_sweeps_ms": sweep10_ms, "ms_per_sweep": sweep10_ms / max(1, forced), "forced_sweeps": forced,
             "what": f"ThermalModel.step at {a.size}^2 x {a.nz} (binary64)",
             "kernels": kern}
 

@@ -309,3 +309,40 @@ def test_vanka_dump_matches_reference():
     J, r = h.vanka_dump(0, DT)
     assert rel_err(_np(J), g["out_J"]) <= 1e-12
     assert rel_err(_np(r), g["out_r"]) <= 1e-12
+
+
+def test_binary32_operators_against_binary64():
+    """The binary32 fast-math operators the mixed form runs (residual, JVP,
+    VJP) against their binary64 versions on the same solved dome state, at
+    the operator level: relative max-norm differences at the binary32
+    rounding level, stated here as 5e-5."""
+    from cases import dome
+    n, dx = 256, 6000.0
+    f = dome(n, dx, 1200e3, seed=1)
+    h64 = _hier(n, n, dx, levels=4, quirks=False)
+    for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+        h64.set(k, 0, torch.as_tensor(f[k]), restrict_down=True)
+    h64.set_fas(False, maximum_vcycles=4, relative_tolerance=0.0, absolute_tolerance=0.0)
+    h64.forward(DT, 0)
+    h32 = _hier(n, n, dx, precision="fp32", quirks=False)
+    rng = np.random.default_rng(8)
+    fields = ("u", "v", "H", "H_prev", "mask", "bed", "B", "beta", "smb")
+    extra = {"var_u": 50.0 * rng.standard_normal((n, n + 1)), "var_v": 50.0 * rng.standard_normal((n + 1, n)),
+             "var_H": 10.0 * rng.standard_normal((n, n)), "lambda_u": rng.standard_normal((n, n + 1)),
+             "lambda_v": rng.standard_normal((n + 1, n)), "lambda_H": rng.standard_normal((n, n))}
+    for k, v in extra.items():
+        h64.set(k, 0, torch.as_tensor(v))
+    for k in fields + tuple(extra):
+        h32.set(k, 0, h64.get(k, 0).to(torch.float32))
+    errs = {}
+    for h in (h64, h32):
+        h.set_rhs(0, DT)
+        h.compute_phi(0)
+        h.residual(0, DT, 1 | 8)  # USE_MASK | FREEZE_PHI
+        h.jvp(0, DT, reference_rows=False)
+        h.vjp(0, DT)
+    for k in ("r_u", "r_v", "r_H", "jvp_u", "jvp_v", "jvp_H", "vjp_u", "vjp_v", "vjp_H"):
+        errs[k] = rel_err(_np(h32.view(k, 0)).astype(np.float64), _np(h64.view(k, 0)))
+    print("binary32 vs binary64 operators:", {k: f"{e:.1e}" for k, e in errs.items()})
+    for k, e in errs.items():
+        assert e <= 5e-5, (k, e)
