@@ -92,7 +92,7 @@ def parse(argv=None):
     ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
     ap.add_argument("--mode", default="step",
-                    choices=["step", "sweeps", "kernels", "thermal", "ensemble", "vti", "coupled"],
+                    choices=["step", "sweeps", "kernels", "thermal", "columns", "ensemble", "vti", "coupled"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -328,8 +328,11 @@ def run_kernels(a):
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # binary32 fine-level kernels on the 2048^2 workload, from one ncu capture of
-# `python bench.py --mode kernels` on a B200.
-NCU_TRAFFIC_2048_FP32 = {"k_residual": 225.250e6, "k_jvp": 223.709e6, "k_vanka_sweep": 249.812e6}
+# `python bench.py --mode kernels` on a B200 (the command and the figures are
+# in profiles/ssa_kernels_fp32_2048.md, with the commit they were taken at).
+NCU_TRAFFIC_2048_FP32 = {"k_residual": 224.755e6, "k_jvp": 218.257e6, "k_block_factor": 499.247e6,
+                         "k_block_sweep": 563.115e6, "k_vanka_sweep": 246.423e6}
+NCU_TRAFFIC_SOURCE = "profiles/ssa_kernels_fp32_2048.md (ncu, build 494b6d0)"
 
 
 def kernel_roofline(a, h, stream, fields=None, probe=False):
@@ -672,7 +675,8 @@ def run_ours(a, rank, world):
         "roofline": {"bound": "hbm", "kernel": f"{dom} (fine level, {kprec}, step-start state; the top kernel by "
                                                f"share of step time)",
                      "achieved": kd["achieved_gbs"], "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": kd["frac"], "traffic": kd["traffic"], "launch_ms": kd["launch_ms"],
+                     "frac": kd["frac"], "traffic": kd["traffic"], "traffic_source": NCU_TRAFFIC_SOURCE,
+                     "launch_ms": kd["launch_ms"],
                      "algorithmic_bytes_per_launch": kd["algorithmic_bytes"], "kernels": kernels},
         "clocks": clocks,
     }
@@ -693,6 +697,40 @@ def run_thermal(a):
     dev = torch.device("cuda", 0)
     out = thermal_leg(a, h, f, torch.cuda.current_stream(), dev, 1)
     print(json.dumps({"mode": "thermal", "size": a.size, **out}), flush=True)
+
+
+def run_columns(a):
+    """Profiling case: the enthalpy column smoother kernels on the dome at
+    --size (cold ice from the lapse-rate surface temperature, uniform
+    velocity (50, 20) m/a, --nz levels): one ThermalModel step, then one
+    column_smooth with the default on-chip kernel and one with the
+    per-thread-array kernel (the launches a profiler captures after the
+    step's ten)."""
+    import torch
+    from cases import dome
+    from glide_b200.grid import Grid
+    from glide_b200.hierarchy import Hierarchy
+    from glide_b200.model import ThermalModel
+    f = dome(a.size, a.dx, a.radius, seed=0)
+    h = Hierarchy(a.size, a.size, a.dx, 1, precision="fp64")
+    load_dome(h, f)
+    h.set("u", 0, 50.0)
+    h.set("v", 0, 20.0)
+    tm = ThermalModel(Grid(hierarchy=h, level=0), nz=a.nz, n_smooth=10)
+    H = np.asarray(f["H"])
+    surf = np.maximum(f["bed"] + H, (1.0 - 0.917) * H)
+    tm.initialize(torch.as_tensor(273.15 + (-30.0 + 6e-3 * (2000.0 - surf))), Q_geo=0.05)
+    sec = 365.25 * 86400.0
+    tm.pre_momentum()
+    tm.step(a.dt * sec)
+    ops = tm.ops
+    ops._push_config()
+    ops._bind(vel_div=sec)
+    for kind in ("smem", "local"):
+        ops.set_tuning(column_kernel=kind)
+        ops.column_smooth(a.dt * sec)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "columns", "size": a.size, "nz": a.nz}), flush=True)
 
 
 def run_ensemble(a):
@@ -1270,6 +1308,9 @@ def main():
         return 0
     if a.mode == "vti":
         run_vti(a)
+        return 0
+    if a.mode == "columns":
+        run_columns(a)
         return 0
     if a.mode == "coupled":
         import torch
