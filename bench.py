@@ -480,6 +480,7 @@ def run_ours(a, rank, world):
         gstats = []
         g_ms = reduce_max(event_time(lambda: gstats.append(grad()), kg, stream), dev, world)
         grads = {"value": world * 1000.0 / g_ms, "unit": "grads/s", "ms_per_grad": g_ms,
+                 "forward_adjoint_ms_per_step": ms + g_ms,
                  "vcycles_per_grad": float(np.mean([s["vcycles"] for s in gstats])),
                  "adjoint_schedule": a.adj_schedule or "10,20,50,200", "adjoint_omega": a.adj_omega or 0.5,
                  "binary32_vcycles_per_correction": a.inner,
