@@ -187,6 +187,49 @@ def jvp_flag_cases(glide):
     np.savez_compressed(HERE / "random_jvp_flags_f64.npz", **out)
 
 
+C3_STRIDE = 7  # the sampling lattice of the 512^2 fixture (prime: not aligned with any tile)
+
+
+def c3_dome_case(glide):
+    """The C3 dome at full size: 512^2, dx 1500 m, 5 levels, dt 10 a, the
+    reference algorithm (its defaults and quirks), 3 forward V-cycles, then
+    the adjoint of dJ/du = 0.05 u, dJ/dv = 0.05 v with 2 V-cycles and the
+    gradients.  Inputs are regenerated by tests/cases.py dome(512, 1500,
+    600e3, seed=0); the fixture keeps their checksums, every field's
+    max-norm and its values on a stride-7 lattice."""
+    from glide.model import IceDynamics
+    from cases import dome
+    f = dome(512, 1500.0, 600e3, seed=0)
+    with quiet():
+        model = IceDynamics(n_levels=5, ny=512, nx=512, dx=1500.0)
+    mg = model.mg
+    for k, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
+        getattr(grp, k).set(f[k])
+    mg.state.H.set(f["H"])
+    mg.state.H_prev.set(f["H_prev"])
+    model.forward_solver.fas_options.set(maximum_vcycles=3, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                         report_norms=False)
+    with quiet():
+        model.forward(0.0, 10.0, update_geometry=False)
+    lv = mg.levels[0]
+    u, v = np.array(lv.state.u.data), np.array(lv.state.v.data)
+    model.adjoint_solver.fas_options.set(maximum_vcycles=2, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                         report_norms=False)
+    with quiet():
+        model.backward(0.0, 10.0, dJdu=0.05 * u, dJdv=0.05 * v)
+    fields = {"u": lv.state.u.data, "v": lv.state.v.data, "H": lv.state.H.data,
+              "lambda_u": lv.adjoint.lambda_u.data, "lambda_v": lv.adjoint.lambda_v.data,
+              "lambda_H": lv.adjoint.lambda_H.data, "grad_beta": lv.sliding.beta.grad,
+              "grad_bed": lv.geometry.bed.grad}
+    out = {f"in_sum_{k}": np.array([float(np.sum(f[k])), float(np.sum(np.abs(f[k])))])
+           for k in ("bed", "B", "beta", "smb", "H")}
+    for k, a in fields.items():
+        a = np.array(a, dtype=np.float64)
+        out[f"max_{k}"] = np.array(float(np.abs(a).max()))
+        out[f"out_{k}"] = a[::C3_STRIDE, ::C3_STRIDE].copy()
+    np.savez_compressed(HERE / "c3_dome512_f64.npz", **out)
+
+
 def vanka_dump_case(glide):
     """ForwardOperators.vanka_dump (glide/operators.py:253-273) on the random
     state: the local 5x5 systems of every cell."""
@@ -326,8 +369,12 @@ def enthalpy_cases(glide):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", default=None, help="enthalpy | dump | transfers | jvp_flags: only those fixtures")
+    ap.add_argument("--only", default=None,
+                    help="enthalpy | dump | transfers | jvp_flags | c3: only those fixtures")
     a = ap.parse_args(argv)
+    if a.only == "c3":
+        c3_dome_case(load_reference(fp64=True, reference=a.reference))
+        return
     if a.only == "jvp_flags":
         jvp_flag_cases(load_reference(fp64=True, reference=a.reference))
         return
@@ -347,6 +394,7 @@ def main(argv=None):
     enthalpy_cases(glide)
     vanka_dump_case(glide)
     transfer_cases(glide)
+    c3_dome_case(glide)
     glide32 = load_reference(fp64=False, reference=a.reference)
     c1_forward_and_adjoint(glide32, "f32")
     for p in sorted(HERE.glob("*.npz")):

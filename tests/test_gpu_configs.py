@@ -108,3 +108,31 @@ def test_c3_adjoint_gradient_matches_finite_differences():
             best = min(best, abs(adj - fd) / max(abs(fd), 1e-300))
         worst = max(worst, best)
     assert worst <= 5e-2, worst
+
+
+def test_c3_dome_512_matches_reference():
+    """The reference algorithm at the C3 size (512^2, 5 levels, its defaults
+    and quirks): 3 forward V-cycles, then the adjoint of dJ/du = 0.05 u,
+    dJ/dv = 0.05 v with 2 V-cycles and the gradients, against the
+    reference's own run (fixture tests/golden/c3_dome512_f64.npz: values on a
+    stride-7 lattice and each field's max-norm) at 1e-10."""
+    from util import load_golden
+    g = load_golden("c3_dome512_f64")
+    f = dome(N, DX, 600e3, seed=0)
+    for k in ("bed", "B", "beta", "smb", "H"):  # the regenerated inputs are the fixture's
+        np.testing.assert_allclose([np.sum(f[k]), np.sum(np.abs(f[k]))], g[f"in_sum_{k}"], rtol=1e-13)
+    m = _model(f)
+    m.forward_solver.fas_options.set(maximum_vcycles=3, relative_tolerance=0.0, absolute_tolerance=0.0)
+    m.forward(0.0, DT, update_geometry=False)
+    st = m.mg.levels[0].state
+    u, v = st.u.data.clone(), st.v.data.clone()
+    m.adjoint_solver.fas_options.set(maximum_vcycles=2, relative_tolerance=0.0, absolute_tolerance=0.0)
+    m.backward(0.0, DT, dJdu=0.05 * u, dJdv=0.05 * v)
+    lv = m.mg.levels[0]
+    got = {"u": st.u.data, "v": st.v.data, "H": st.H.data, "lambda_u": lv.adjoint.lambda_u.data,
+           "lambda_v": lv.adjoint.lambda_v.data, "lambda_H": lv.adjoint.lambda_H.data,
+           "grad_beta": lv.sliding.beta.grad, "grad_bed": lv.geometry.bed.grad}
+    for k, t in got.items():
+        a = t.detach().cpu().numpy()[::7, ::7]
+        err = float(np.abs(a - g[f"out_{k}"]).max()) / float(g[f"max_{k}"])
+        assert err <= 1e-10, (k, err)
