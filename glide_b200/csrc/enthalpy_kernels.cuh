@@ -30,6 +30,7 @@ constexpr double kRhoI = fRHO_I, kRhoW = fRHO_W, kCI = fC_I, kL = fL_HEAT, kTRef
 constexpr double kKTF = fK_TEMP_FACTOR, kReg = fMASS_FLUX_REG, kRegYr = fMASS_FLUX_REG_YR;
 constexpr double kKCold = double(fK_I / fC_I);                    // (K_I/C_I)
 constexpr double kEScale = double(fC_I * (fT_MELT - fT_REF));     // (C_I * (T_MELT - T_REF))
+constexpr double kCIoverEScale = kCI / kEScale;                    // folded once, not divided per row
 constexpr double kCcRhoG = double(fBETA_CC * fRHO_I * fGRAVITY);  // BETA_CC * RHO_I * GRAVITY
 constexpr double kSharp = double(0.01f);                          // K(E) and drainage sharpness
 
@@ -60,7 +61,7 @@ struct EnthArgs {
 __device__ __forceinline__ double e_pmp(double sigma, double H) {
     double depth = (1.0 - sigma) * H;
     double T_pmp = kTMelt - kCcRhoG * depth;
-    return kCI * (T_pmp - kTRef) / kEScale;
+    return (T_pmp - kTRef) * kCIoverEScale;
 }
 
 // diffusivity of the switch value s (enthalpy.cu:60-66)
