@@ -84,7 +84,7 @@ def parse(argv=None):
     ap.add_argument("--members", type=int, default=64, help="ensemble mode: members")
     ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
-    ap.add_argument("--ens-precision", default="mixed", choices=["fp64", "mixed"], help="ensemble members")
+    ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
     ap.add_argument("--ens-cold-tune", action="store_true", help="ensemble: autotune on the cold first step")
     ap.add_argument("--ens-adjoint", default="fast", choices=["fast", "reference"],
                     help="ensemble adjoint: 4/4/0/50 cycles with omega 0.8, or the reference's 10/20/50/200")

@@ -312,12 +312,13 @@ def test_vanka_dump_matches_reference():
 
 
 def test_binary32_operators_against_binary64():
-    """The binary32 fast-math operators the mixed form runs (the residual
-    operator F(x), JVP, VJP) against their binary64 versions on the same
-    solved dome state, at the operator level: relative max-norm differences
-    at the binary32 rounding level, stated here as 5e-5.  (The residual
-    F(x) - f itself is not compared: at a solved state it is the small
-    difference of large terms, below binary32 resolution.)"""
+    """The binary32 fast-math operators the mixed form runs against their
+    binary64 versions on the same state, at the operator level: the JVP and
+    VJP at a solved dome state, and the residual operator F(x) at that state
+    with u and v perturbed (at the solution F(x) balances the forcing, the
+    small difference of large terms, below binary32 resolution).  Relative
+    max-norm differences at the binary32 rounding level, stated here as
+    5e-5."""
     from cases import dome
     n, dx = 256, 6000.0
     f = dome(n, dx, 1200e3, seed=1)
@@ -340,9 +341,14 @@ def test_binary32_operators_against_binary64():
     for h in (h64, h32):
         h.set_rhs(0, DT)
         h.compute_phi(0)
-        h.residual(0, DT, 1 | 2 | 8)  # USE_MASK | OPERATOR_ONLY | FREEZE_PHI: F(x) into F_*
         h.jvp(0, DT, reference_rows=False)
         h.vjp(0, DT)
+    pu = h64.get("u", 0) + 20.0 * torch.as_tensor(rng.standard_normal((n, n + 1)), device="cuda")
+    pv = h64.get("v", 0) + 20.0 * torch.as_tensor(rng.standard_normal((n + 1, n)), device="cuda")
+    for h in (h64, h32):
+        h.set("u", 0, pu.to(h.dtype))
+        h.set("v", 0, pv.to(h.dtype))
+        h.residual(0, DT, 1 | 2 | 8)  # USE_MASK | OPERATOR_ONLY | FREEZE_PHI: F(x) into F_*
     for k in ("F_u", "F_v", "F_H", "jvp_u", "jvp_v", "jvp_H", "vjp_u", "vjp_v", "vjp_H"):
         errs[k] = rel_err(_np(h32.view(k, 0)).astype(np.float64), _np(h64.view(k, 0)))
     print("binary32 vs binary64 operators:", {k: f"{e:.1e}" for k, e in errs.items()})
