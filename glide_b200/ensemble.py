@@ -76,6 +76,9 @@ CANDIDATES = {
                     tangent=None, blocks=1),
     "classic": dict(quirks=False, schedule=(10, 20, 50, 200), newton_steps=30, method="fascd", switch=None,
                     tangent=None, blocks=2),
+    # guarded Newton whose fallback cycles are the classic schedule
+    "newton/classic": dict(quirks=False, schedule=(10, 20, 50, 200), newton_steps=30, method="newton",
+                           switch=0, tangent=(4, 4, 0, 10), blocks=2),
 }
 FALLBACK = "classic"
 
