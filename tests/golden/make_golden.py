@@ -187,6 +187,44 @@ def jvp_flag_cases(glide):
     np.savez_compressed(HERE / "random_jvp_flags_f64.npz", **out)
 
 
+def coupled_case(glide):
+    """Three coupled thermomechanical steps with the reference's own
+    IceDynamics and ThermalModel, in the order of its coupled example
+    (examples/thermal/coupled_dome.py:258-272): a 32^2 dome (dx 48 km, R =
+    1200 km, seed 3), 3 levels, 9 sigma levels, dt 5 a, each momentum solve 2
+    FASCD V-cycles, surface temperature -30 + 6e-3 (2000 - s) C, geothermal
+    flux 0.05 W m^-2, B first set from the initial temperature on every level
+    (coupled_dome.py:144-146)."""
+    from glide.model import IceDynamics, ThermalModel
+    from cases import dome, surface_temperature
+    n, dx, levels, nz, steps, dt_yr = 32, 48e3, 3, 9, 3, 5.0
+    f = dome(n, dx, 1200e3, seed=3)
+    with quiet():
+        model = IceDynamics(n_levels=levels, ny=n, nx=n, dx=dx)
+    mg = model.mg
+    for k, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
+        getattr(grp, k).set(f[k])
+    mg.state.H.set(f["H"])
+    mg.state.H_prev.set(f["H_prev"])
+    model.forward_solver.fas_options.set(maximum_vcycles=2, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                         report_norms=False)
+    grid = mg.levels[0]
+    tm = ThermalModel(grid, nz=nz, n_smooth=10)
+    tm.initialize(surface_temperature(np.array(grid.state.H.data), np.array(grid.geometry.bed.data)), Q_geo=0.05)
+    mg.rheology.B.set(tm.ops.get_arrhenius_factor() / tm.B_scale)
+    for _ in range(steps):
+        tm.pre_momentum()
+        with quiet():
+            model.forward(0.0, dt_yr)
+        tm.ops.set_surface_enthalpy_from_temperature(
+            surface_temperature(np.array(grid.state.H.data), np.array(grid.geometry.bed.data)))
+        tm.step(dt_yr * SEC_PER_YR)
+    out = {"out_u": np.array(grid.state.u.data), "out_v": np.array(grid.state.v.data),
+           "out_H": np.array(grid.state.H.data), "out_E": np.array(tm.enthalpy),
+           "out_B": np.array(grid.rheology.B.data)}
+    np.savez_compressed(HERE / "coupled_f64.npz", **out)
+
+
 C3_STRIDE = 7  # the sampling lattice of the 512^2 fixture (prime: not aligned with any tile)
 
 
@@ -370,8 +408,11 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--only", default=None,
-                    help="enthalpy | dump | transfers | jvp_flags | c3: only those fixtures")
+                    help="enthalpy | dump | transfers | jvp_flags | c3 | coupled: only those fixtures")
     a = ap.parse_args(argv)
+    if a.only == "coupled":
+        coupled_case(load_reference(fp64=True, reference=a.reference))
+        return
     if a.only == "c3":
         c3_dome_case(load_reference(fp64=True, reference=a.reference))
         return
@@ -395,6 +436,7 @@ def main(argv=None):
     vanka_dump_case(glide)
     transfer_cases(glide)
     c3_dome_case(glide)
+    coupled_case(glide)
     glide32 = load_reference(fp64=False, reference=a.reference)
     c1_forward_and_adjoint(glide32, "f32")
     for p in sorted(HERE.glob("*.npz")):

@@ -4,8 +4,9 @@ reference's coupled example (examples/thermal/coupled_dome.py:258-272).
 
 1. binary64, reference algorithm and quirks, fixed V-cycles: three coupled
    steps on a 32^2 x 9 dome against the oracle's coupled loop
-   (oracle/coupled_oracle.py) at 1e-10 -- the multi-step drift of the B
-   feedback and of omega from the realised dH/dt, checked.
+   (oracle/coupled_oracle.py) and against the reference's own run of the
+   same steps (tests/golden/coupled_f64.npz) at 1e-10 -- the multi-step
+   drift of the B feedback and of omega from the realised dH/dt, checked.
 2. the bench's fast form: five coupled steps on a 256^2 x 41 dome (the
    large run's recipe, coarser cells), mixed precision against binary64,
    both solved to a relative residual of 1e-8; the errors the mixed form
@@ -16,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from util import rel_err
+from util import load_golden, rel_err
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -36,8 +37,10 @@ def test_coupled_binary64_matches_oracle():
     got = run.fields()
     ref = coupled_run(f, dx, levels, nz, 5.0, steps, cycles)
     assert sweeps == ref["sweeps"]
+    g = load_golden("coupled_f64")  # the reference's own run of the same steps
     for k in ("u", "v", "H", "E", "B"):
         assert rel_err(got[k], ref[k]) <= 1e-10, k
+        assert rel_err(got[k], g[f"out_{k}"]) <= 1e-10, k
 
 
 # mixed (binary32 smoother and tangent multigrid, binary64 residual and
