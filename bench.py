@@ -86,6 +86,10 @@ def parse(argv=None):
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
     ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
     ap.add_argument("--ens-cold-tune", action="store_true", help="ensemble: autotune on the cold first step")
+    ap.add_argument("--ens-solo", action="store_true",
+                    help="ensemble: every member solves on its own (no grouped launches)")
+    ap.add_argument("--ens-group-max-n", type=int, default=0,
+                    help="ensemble: only members of at most n x n cells join the grouped solves (0: all)")
     ap.add_argument("--ens-adjoint", default="fast", choices=["fast", "reference"],
                     help="ensemble adjoint: 4/4/0/50 cycles with omega 0.8, or the reference's 10/20/50/200")
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
@@ -766,7 +770,8 @@ def run_ensemble(a):
             m.adjoint_solver.fas_options.set(pre_steps=4, post_steps=4, finest_steps=0, coarsest_steps=50)
             m.adjoint_solver.vanka_options.set(omega=0.8)
         members.append(m)
-    ens = Ensemble(members, workers=a.ens_workers)
+    ens = Ensemble(members, workers=a.ens_workers, grouped=not a.ens_solo,
+                   group_max_cells=a.ens_group_max_n ** 2 if a.ens_group_max_n else None)
     t0 = time.perf_counter()
     chosen = ens.autotune(a.dt, warm=not a.ens_cold_tune)
     tune_s = time.perf_counter() - t0
@@ -781,8 +786,16 @@ def run_ensemble(a):
     stats = []
     ens.retries = 0
     ms = event_time(lambda: stats.append(step(0.0)), a.ens_steps, stream)
+    group_cycles = None
+    if ens.grouped:
+        group_cycles = {"forward": ens._fwd_group.counters()["forward_cycle"] if ens._fwd_group else None,
+                        "adjoint": ens._adj_group.counters()["adjoint_cycle"] if ens._adj_group else None,
+                        "what": "grouped launches of one cycle, and the members' launches they carry"}
     ens.close()
     cells = sum(sp.n * sp.n for sp in specs)
+    # the members' forward steps one after another, each at its class's tuned warm-step time
+    solo = {n: t[chosen[n]]["ms"] for n, t in ens.trials.items() if chosen[n] in t}
+    serial_fwd = sum(solo.get(sp.n, float("nan")) for sp in specs)
     fv = [s["vcycles"] for fs, _ in stats for s in fs]
     bv = [s["vcycles"] for _, bs in stats for s in bs]
     rels = [s["final_norm"] / s["initial_norm"] for fs, _ in stats for s in fs if s["initial_norm"] > 0]
@@ -796,8 +809,19 @@ def run_ensemble(a):
             "worst_forward_relative_residual": worst, "forward_solves_converged": converged,
             "max_cycles": max_cycles, "workers": ens.workers, "adjoint": a.ens_adjoint,
             "forward_retries": ens.retries, "precision": a.ens_precision,
+            "grouped": ens.grouped,
+            "grouped_forward_members": len(ens._fwd_keys),
+            "grouped_adjoint_members": len(ens._adj_keys),
+            "group_max_n": a.ens_group_max_n or None,
+            "group_cycles": group_cycles,
+            "autotune_trials": {str(n): {k: dict(v, ms=round(v["ms"], 2)) for k, v in t.items()}
+                                for n, t in ens.trials.items()},
+            "serial_forward_ms": serial_fwd,
             "tuned_on": "cold first step" if a.ens_cold_tune else "a warm step of each class's first member",
-            "what": "forward + adjoint solve per member and step, members concurrent on per-worker streams"}
+            "what": ("forward + adjoint solve per member and step; grouped: FASCD-scheduled members' forward solves "
+                     "and every adjoint solve in grouped launches (one launch per kind for all members), the "
+                     "others concurrent on per-worker streams" if ens.grouped else
+                     "forward + adjoint solve per member and step, members concurrent on per-worker streams")}
 
 
 def vti_leg(a, h, stream, tmp):

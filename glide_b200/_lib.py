@@ -153,6 +153,11 @@ SIGNATURES = {
     "glide_noalloc_last_error": ([], ctypes.c_char_p),
     "glide_vcycle": ([_H, _I, _I, _I, _D, _P], _I),
     "glide_transfer": ([_I, _I, _I, _I, _P, _I, _P, _I, _P], _I),
+    "glide_group_create": ([ctypes.POINTER(_H), _I, ctypes.POINTER(_H)], _I),
+    "glide_group_destroy": ([_H], _I),
+    "glide_group_forward": ([_H, _D, _I, ctypes.POINTER(Stats), _P], _I),
+    "glide_group_backward": ([_H, _D, _I, _I, ctypes.POINTER(Stats), _P], _I),
+    "glide_group_counters": ([_H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I)], _I),
 }
 
 class EnthalpyConfig(ctypes.Structure):

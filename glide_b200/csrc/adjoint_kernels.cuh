@@ -265,14 +265,14 @@ struct VjpArgs {
 
 // Box maps in AdjTile staging order: u, v, H, phi, bed, beta, B, lambda_u,
 // lambda_v.  Each warp computes a 4 x 8 patch of the 16 x 16 tile.
-template <class R>
-__global__ void __launch_bounds__(kTileA * kTileA) k_vjp(VjpArgs<R> a, const __grid_constant__ BoxMaps<9> maps) {
+template <class R, class BLK>
+__device__ __forceinline__ void vjp_tile(const VjpArgs<R>& a, const BoxMaps<9>& maps, BLK blk) {
     using TT = AdjTile<R>;
     constexpr int NC = TT::NC;
     __shared__ __align__(128) TT T;
     __shared__ double red[3][kTileA * kTileA / 32];
     __shared__ unsigned long long bar;
-    const int i0 = blockIdx.y * kTileA, j0 = blockIdx.x * kTileA;
+    const int i0 = blk.y() * kTileA, j0 = blk.x() * kTileA;
     const int ny = a.ny, nx = a.nx;
     {
         BoxT<R, TT::BH>* const dst[TT::NB] = {&T.u, &T.v, &T.H, &T.phi, &T.bed, &T.beta, &T.B, &T.lu, &T.lv};
@@ -373,9 +373,15 @@ __global__ void __launch_bounds__(kTileA * kTileA) k_vjp(VjpArgs<R> a, const __g
         if (threadIdx.x < 3) {
             double acc = 0;
             for (int q = 0; q < kTileA * kTileA / 32; ++q) acc += red[threadIdx.x][q];
-            a.partial[size_t(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = acc;
+            a.partial[size_t(blk.y() * blk.gx() + blk.x()) * 3 + threadIdx.x] = acc;
         }
     }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kTileA * kTileA) k_vjp(VjpArgs<R> a,
+                                                         const __grid_constant__ BoxMaps<9> maps) {
+    vjp_tile<R>(a, maps, SoloBlock{});
 }
 
 // -------------------------------------------------------------------------
@@ -493,14 +499,13 @@ struct BlockArgs {
     int ny, nx;
 };
 
-template <class R, bool TR>
-__global__ void __launch_bounds__(kTile * kTile)
-    k_block_factor(BlockArgs<R> a, const __grid_constant__ BoxMaps<7> maps) {
+template <class R, bool TR, class BLK>
+__device__ __forceinline__ void block_factor_tile(const BlockArgs<R>& a, const BoxMaps<7>& maps, BLK blk) {
     using TileT = StateBoxTile<R>;
     constexpr int NC = TileT::NE;
     __shared__ __align__(128) TileT t;
     __shared__ unsigned long long bar;
-    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int i0 = blk.y() * kTile, j0 = blk.x() * kTile;
     const int ny = a.ny, nx = a.nx;
     if (!stage_state_boxes<R>(t, maps, a.u, a.v, a.H, a.phi, a.bed, a.beta, a.B, i0, j0, &bar, a.err)) return;
     StateBoxView<R> s{t, i0, j0, ny, nx};
@@ -543,14 +548,20 @@ __global__ void __launch_bounds__(kTile * kTile)
     for (int k = 0; k < 25; ++k) f[k * a.plane] = M[k];
 }
 
+template <class R, bool TR>
+__global__ void __launch_bounds__(kTile * kTile)
+    k_block_factor(BlockArgs<R> a, const __grid_constant__ BoxMaps<7> maps) {
+    block_factor_tile<R, TR>(a, maps, SoloBlock{});
+}
+
 // One linear block-smoother sweep with stored factors: x += omega * delta
 // with delta = B^-1 (f - Op x) per cell, face corrections averaged between
 // the two cells of a face (adjoint: lambda -= omega * B^-T r, r = J^T lambda - f).
-template <class R, bool TR>
-__global__ void __launch_bounds__(kSweepThreads) k_block_sweep(BlockArgs<R> a) {
+template <class R, bool TR, class BLK>
+__device__ __forceinline__ void block_sweep_tile(const BlockArgs<R>& a, BLK blk) {
     constexpr int ND = kTile + 1;
     __shared__ R dl[ND][ND][4];
-    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int i0 = blk.y() * kTile, j0 = blk.x() * kTile;
     const int ny = a.ny, nx = a.nx;
     int i, j;
     const int tid = threadIdx.x;
@@ -605,6 +616,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_block_sweep(BlockArgs<R> a) {
     }
 }
 
+template <class R, bool TR>
+__global__ void __launch_bounds__(kSweepThreads) k_block_sweep(BlockArgs<R> a) {
+    block_sweep_tile<R, TR>(a, SoloBlock{});
+}
+
 // -------------------------------------------------------------------------
 // Gradients (grad.cu:2-169, glide/operators.py:589-593), gathered per cell
 // with the reference's index guards.
@@ -629,8 +645,7 @@ struct GView {
 };
 
 template <class R>
-__global__ void k_gradients(GradArgs<R> a) {
-    const int J = blockIdx.x * blockDim.x + threadIdx.x, I = blockIdx.y;
+__device__ __forceinline__ void gradients_at(const GradArgs<R>& a, int I, int J) {
     const int ny = a.ny, nx = a.nx;
     if (J >= nx) return;
     GView<R> g{a, ny, nx};
@@ -668,6 +683,11 @@ __global__ void k_gradients(GradArgs<R> a) {
     }
     if (a.g_Hp.p) a.g_Hp.at(I, J) = -a.lH.at(I, J) / a.dt;
     if (a.g_smb.p) a.g_smb.at(I, J) = -a.lH.at(I, J);
+}
+
+template <class R>
+__global__ void k_gradients(GradArgs<R> a) {
+    gradients_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace glide

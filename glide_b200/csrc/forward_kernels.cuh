@@ -34,91 +34,18 @@ struct ResidualArgs {
 // The tile's state is staged in box layout (TMA on large levels).  Each warp
 // computes a 4 x 8 patch of the 16 x 16 tile; with 24-entry rows the patch's
 // stencil reads are bank-conflict free.
+// The tile (bx, by) of a grid gx tiles wide; the kernel below runs one tile
+// per block, the grouped launches of several hierarchies run the same body.
+template <class R, class BLK>
+__device__ __forceinline__ void residual_tile(const ResidualArgs<R>& a, const BoxMaps<7>& maps, BLK blk) {
+#include "residual_tile.inc"
+}
+
 template <class R>
-__global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a, const __grid_constant__ BoxMaps<7> maps) {
-    using TileT = StateBoxTile<R>;
-    constexpr int NC = TileT::NE;
-    __shared__ __align__(128) TileT t;
-    __shared__ double red[3][8];
-    __shared__ unsigned long long bar;
-    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
-    const int ny = a.ny, nx = a.nx;
-    if (!stage_state_boxes<R>(t, maps, a.u, a.v, a.H, a.phi, a.bed, a.beta, a.B, i0, j0, &bar, a.err)) return;
-    StateBoxView<R> s{t, i0, j0, ny, nx};
-    for (int k = threadIdx.x; k < NC * NC; k += blockDim.x) {
-        int r = k / NC, c = k % NC;
-        int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        t.eta[r][c] = eta_at<R>(s, s.BC(gi, gj), a.p, gi, gj);
-    }
-    __syncthreads();
-    const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    const int i = i0 + 4 * (wp >> 1) + (ln >> 3), j = j0 + 8 * (wp & 1) + (ln & 7);
-    double ssu = 0, ssv = 0, ssh = 0;
-    if (i < ny && j < nx) {
-        const bool f = a.use_forcing != 0;
-        if (a.active_set) {
-            // Newton mode: store the unmasked mass residual, decide the active
-            // set with the smoother's rule H - dt r_H <= gamma, and accumulate
-            // the norm of the masked residual (H - gamma on active cells)
-            R fH = f ? a.f_H.at(i, j) : R(0);
-            R r = mass_residual<R>(s, a.p, i, j, fH);
-            R Hc = s.Hc(i, j), g = a.gamma.at(i, j);
-            const bool act = (Hc - a.p.dt * r) <= g;
-            a.mask.at(i, j) = act ? R(1) : R(0);
-            a.o_H.at(i, j) = r;
-            R rn = act ? Hc - g : r;
-            ssh += double(rn) * double(rn);
-        } else {
-            R fH = f ? a.f_H.at(i, j) : R(0);
-            R r = mass_residual<R>(s, a.p, i, j, fH);
-            R msk = a.use_mask ? a.mask.at(i, j) : R(0);
-            R Hc = s.Hc(i, j);
-            r = (R(1) - msk) * r + msk * (Hc - a.gamma.at(i, j));
-            if (a.s_H.p) r = r - a.s_H.at(i, j);
-            a.o_H.at(i, j) = r;
-            ssh += double(r) * double(r);
-        }
-        {
-            R r = umom_residual<R>(s, a.p, i, j, f ? a.f_u.at(i, j) : R(0));
-            if (a.s_u.p) r = r - a.s_u.at(i, j);
-            a.o_u.at(i, j) = r;
-            ssu += double(r) * double(r);
-            if (j == nx - 1) {
-                R r2 = umom_residual<R>(s, a.p, i, nx, f ? a.f_u.at(i, nx) : R(0));
-                if (a.s_u.p) r2 = r2 - a.s_u.at(i, nx);
-                a.o_u.at(i, nx) = r2;
-                ssu += double(r2) * double(r2);
-            }
-        }
-        {
-            R r = vmom_residual<R>(s, a.p, i, j, f ? a.f_v.at(i, j) : R(0));
-            if (a.s_v.p) r = r - a.s_v.at(i, j);
-            a.o_v.at(i, j) = r;
-            ssv += double(r) * double(r);
-            if (i == ny - 1) {
-                R r2 = vmom_residual<R>(s, a.p, ny, j, f ? a.f_v.at(ny, j) : R(0));
-                if (a.s_v.p) r2 = r2 - a.s_v.at(ny, j);
-                a.o_v.at(ny, j) = r2;
-                ssv += double(r2) * double(r2);
-            }
-        }
-    }
-    if (a.partial) {
-        // fixed-order block reduction: warp shuffles, then warp 0
-        for (int o = 16; o > 0; o >>= 1) {
-            ssu += __shfl_down_sync(0xffffffffu, ssu, o);
-            ssv += __shfl_down_sync(0xffffffffu, ssv, o);
-            ssh += __shfl_down_sync(0xffffffffu, ssh, o);
-        }
-        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        if (l == 0) { red[0][w] = ssu; red[1][w] = ssv; red[2][w] = ssh; }
-        __syncthreads();
-        if (threadIdx.x < 3) {
-            double acc = 0;
-            for (int q = 0; q < 8; ++q) acc += red[threadIdx.x][q];
-            a.partial[size_t(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = acc;
-        }
-    }
+__global__ void __launch_bounds__(256) k_residual(ResidualArgs<R> a,
+                                                  const __grid_constant__ BoxMaps<7> maps) {
+    const SoloBlock blk{};
+#include "residual_tile.inc"
 }
 
 // -------------------------------------------------------------------------
@@ -168,6 +95,33 @@ __global__ void __launch_bounds__(256) k_vanka_dump(ResidualArgs<R> a, R* Jout, 
 
 // Sum the per-block partials in a fixed order and take square roots:
 // out[0..2] = |r_u|, |r_v|, |r_H|; out[3] = sqrt of their squares' sum.
+// One block of kNormThreads.
+constexpr int kNormThreads = 1024;
+__device__ __forceinline__ void finish_norms_block(const double* partial, int nblocks, double* out) {
+    // thread-strided sums, a fixed shuffle tree per warp, then warp 0 over
+    // the 32 warp sums: the same order on every call
+    __shared__ double ws[3][32];
+    const int t = threadIdx.x, l = t & 31, w = t >> 5;
+    double s[3] = {0, 0, 0};
+    for (int b = t; b < nblocks; b += kNormThreads)
+        for (int q = 0; q < 3; ++q) s[q] += partial[size_t(b) * 3 + q];
+    for (int o = 16; o > 0; o >>= 1)
+        for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+    if (l == 0)
+        for (int q = 0; q < 3; ++q) ws[q][w] = s[q];
+    __syncthreads();
+    if (w == 0) {
+        for (int q = 0; q < 3; ++q) s[q] = ws[q][l];
+        for (int o = 16; o > 0; o >>= 1)
+            for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+        if (l == 0) {
+            out[0] = sqrt(s[0]);
+            out[1] = sqrt(s[1]);
+            out[2] = sqrt(s[2]);
+            out[3] = sqrt(s[0] + s[1] + s[2]);
+        }
+    }
+}
 __global__ void k_finish_norms(const double* partial, int nblocks, double* out);
 
 // -------------------------------------------------------------------------
@@ -175,11 +129,23 @@ __global__ void k_finish_norms(const double* partial, int nblocks, double* out);
 // (viscosity.cu:17-36).
 // -------------------------------------------------------------------------
 template <class R>
+struct GroundedArgs {
+    Arr<R> phi, H, bed;
+    R c, relax;
+    int ny, nx;
+};
+
+template <class R>
+__device__ __forceinline__ void grounded_at(const GroundedArgs<R>& a, int i, int j) {
+    if (j >= a.nx) return;
+    R g = grounded_frac(a.H.at(i, j), a.bed.at(i, j), a.c);
+    a.phi.at(i, j) = (R(1) - a.relax) * g + a.relax * a.phi.at(i, j);
+}
+
+template <class R>
 __global__ void k_grounded(Arr<R> phi, Arr<R> H, Arr<R> bed, R c, R relax, int ny, int nx) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (j >= nx) return;
-    R g = grounded_frac(H.at(i, j), bed.at(i, j), c);
-    phi.at(i, j) = (R(1) - relax) * g + relax * phi.at(i, j);
+    const GroundedArgs<R> a{phi, H, bed, c, relax, ny, nx};
+    grounded_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // -------------------------------------------------------------------------
@@ -209,6 +175,7 @@ struct SweepArgs {
     R relax;                     // local Newton step length (the reference fixes 0.5)
     int newton_steps;
     int ny, nx;
+    int gmode;                   // GammaMode of grouped launches (the kernel's template fixes it)
 };
 
 constexpr int kSweepThreads = kTile * kTile + 2 * kTile;
@@ -216,14 +183,14 @@ constexpr int kSweepThreads = kTile * kTile + 2 * kTile;
 // MINB = resident blocks per SM the register allocation is fitted to: 1
 // keeps every value in registers, 2 doubles the warps that hide the FP64
 // dependency latency at the price of some spills; the runtime picks one.
-template <class R, int GMODE, bool PHI_LIVE, int MINB>
-__global__ void __launch_bounds__(kSweepThreads, MINB) k_vanka_sweep(SweepArgs<R> a) {
+template <class R, bool PHI_LIVE, class BLK>
+__device__ __forceinline__ void vanka_sweep_tile(const SweepArgs<R>& a, int gmode, BLK blk) {
     using TileT = Tile<R, kTile, 2, 1>;
     constexpr int NC = TileT::NC;     // 19
     constexpr int ND = kTile + 1;     // deltas for rows/cols [i0-1, i0+16)
     __shared__ TileT t;
     __shared__ R dl[ND][ND][4];
-    const int i0 = blockIdx.y * kTile, j0 = blockIdx.x * kTile;
+    const int i0 = blk.y() * kTile, j0 = blk.x() * kTile;
     const int ny = a.ny, nx = a.nx;
     stage_tile<R, kTile, 2, 1>(t, i0, j0, ny, nx, a.u, a.v, a.H, a.bed, a.beta, PHI_LIVE ? nullptr : &a.phi);
     __syncthreads();
@@ -250,8 +217,8 @@ __global__ void __launch_bounds__(kSweepThreads, MINB) k_vanka_sweep(SweepArgs<R
     if (live) {
         R x[5] = {s.U(i, j), s.U(i, j + 1), s.V(i, j), s.V(i + 1, j), s.Hc(i, j)};
         R thk;
-        if (GMODE == kGammaArray) thk = a.gamma.at(i, j);
-        else if (GMODE == kGammaWChi) thk = a.wH.at(i, j) + a.chi.at(i, j);
+        if (gmode == kGammaArray) thk = a.gamma.at(i, j);
+        else if (gmode == kGammaWChi) thk = a.wH.at(i, j) + a.chi.at(i, j);
         else thk = a.wH.at(i, j) + (-a.chi_c.at(i >> 1, j >> 1) + a.chi.at(i, j));
         masked = tid < kTile * kTile ? a.mask.at(i, j) : R(0);  // halo cells never write it
         R comp[5] = {0, 0, 0, 0, 0};
@@ -318,6 +285,11 @@ __global__ void __launch_bounds__(kSweepThreads, MINB) k_vanka_sweep(SweepArgs<R
         a.mask.at(i, j) = masked;
         if (PHI_LIVE) a.phi.at(i, j) = s.PHI(i, j);
     }
+}
+
+template <class R, int GMODE, bool PHI_LIVE, int MINB>
+__global__ void __launch_bounds__(kSweepThreads, MINB) k_vanka_sweep(SweepArgs<R> a) {
+    vanka_sweep_tile<R, PHI_LIVE>(a, GMODE, SoloBlock{});
 }
 
 }  // namespace glide

@@ -37,4 +37,21 @@ struct Dims {
     int ny, nx;
 };
 
+// Block coordinates of a stencil tile.  A kernel launched for one hierarchy
+// reads them from the launch (SoloBlock); a grouped launch over several
+// hierarchies hands each block the tile it maps to (GroupBlock).
+// Both are unsigned, as blockIdx is: the tile origin arithmetic of the
+// kernels is unsigned.
+struct SoloBlock {
+    __device__ __forceinline__ unsigned x() const { return blockIdx.x; }
+    __device__ __forceinline__ unsigned y() const { return blockIdx.y; }
+    __device__ __forceinline__ unsigned gx() const { return gridDim.x; }
+};
+struct GroupBlock {
+    unsigned bx, by, bz, w;
+    __device__ __forceinline__ unsigned x() const { return bx; }
+    __device__ __forceinline__ unsigned y() const { return by; }
+    __device__ __forceinline__ unsigned gx() const { return w; }
+};
+
 }  // namespace glide

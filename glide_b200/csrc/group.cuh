@@ -1,0 +1,431 @@
+// group.cuh -- grouped launches over several hierarchies.
+//
+// A group runs the same solver cycle on many independent hierarchies (the
+// members of an ensemble, of uneven sizes).  Each member's cycle is recorded
+// as its sequence of launches; launches of one kind from different members
+// are merged into ONE persistent launch over a table of items, one per
+// member: its arguments and its tile grid.  The table is the launch's kernel
+// parameters (__grid_constant__, up to 32 KB, read through the constant
+// bank).  Every block first lists the items whose member still runs this
+// cycle and their tile ranges, then strides over those tiles only, running
+// each with its member's arguments; the grid is one wave of resident blocks,
+// so members that have converged cost nothing.  Stencil tiles are staged with
+// plain loads (tensor maps stay per member).
+//
+// The convergence test of every member runs on the device (k_group_control)
+// and clears the member's run flag, so its state stays that of its last
+// cycle -- the state a solo solve of that member stops at.
+#pragma once
+
+#include "glide_b200.h"
+#include "adjoint_kernels.cuh"
+#include "forward_kernels.cuh"
+#include "tangent_kernels.cuh"
+#include "transfer_kernels.cuh"
+
+namespace glide {
+
+// Launch kinds a hierarchy records for grouped execution.
+enum GroupOpKind {
+    G_SNAPSHOT, G_RESTRICT, G_RESTRICT_BATCH, G_CORRECT_BATCH, G_GROUNDED, G_COPY, G_SET_RHS, G_SWEEP,
+    G_RESIDUAL, G_NORMS, G_VJP, G_BLOCK_FACTOR, G_BLOCK_SWEEP, G_GRADIENTS, G_FILL, G_JVP, G_TANGENT_RHS,
+    G_NEWTON_UPDATE, G_KINDS
+};
+
+template <class R>
+struct JvpOpArgs {
+    VjpArgs<R> a;
+    int mode;
+};
+
+struct NormsArgs {
+    const double* partial;
+    int nblocks;
+    double* out;
+};
+
+template <class R>
+struct RestrictArgs {
+    Arr<R> f, c, copy;
+    int kind, nyc, nxc;
+};
+
+// One item of a grouped launch: the member's grid of `blocks` = gx x gy x gz
+// tiles, as its own launch would have it.
+struct GroupItem {
+    int blocks, gx, gy, member;
+};
+
+constexpr int kGroupParamBytes = 32000;  // below the 32764-byte kernel parameter limit
+constexpr int kGroupMaxItems = 64;        // items of one launch (two per lane of the scanning warp)
+
+template <class A>
+constexpr int group_capacity() {
+    return (kGroupParamBytes - 64) / int(sizeof(A) + sizeof(GroupItem)) < kGroupMaxItems
+               ? (kGroupParamBytes - 64) / int(sizeof(A) + sizeof(GroupItem))
+               : kGroupMaxItems;
+}
+
+template <class A, int N>
+struct GroupParams {
+    const int* flags;  // per-member run flags
+    int n;             // items
+    int when;          // flag bits a member must have for its items to run (0: every member)
+    GroupItem item[N];
+    A args[N];
+};
+
+// Pointwise kernels: 256 threads, x over columns, y over rows, z over jobs.
+template <class R>
+struct GSnapshot {
+    static constexpr int kMinBlocks = 4;
+    using Args = SnapshotArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        snapshot_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GRestrict {
+    static constexpr int kMinBlocks = 4;
+    using Args = RestrictArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        restrict_at(a.f, a.c, a.copy, a.kind, a.nyc, a.nxc, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GRestrictBatch {
+    static constexpr int kMinBlocks = 4;
+    using Args = RestrictJobs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        restrict_at(a.f[b.bz], a.c[b.bz], a.copy[b.bz], a.kind[b.bz], a.nyc, a.nxc, b.by,
+                    b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GCorrectBatch {
+    static constexpr int kMinBlocks = 4;
+    using Args = CorrectJobs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        correct_at(a.j[b.bz], b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GGrounded {
+    static constexpr int kMinBlocks = 4;
+    using Args = GroundedArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        grounded_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GCopy {
+    static constexpr int kMinBlocks = 4;
+    using Args = CopyArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        copy_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GSetRhs {
+    static constexpr int kMinBlocks = 4;
+    using Args = SetRhsArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        set_rhs_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GGradients {
+    static constexpr int kMinBlocks = 4;
+    using Args = GradArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        const int J = b.bx * kThreads + threadIdx.x;
+        if (J < a.nx) gradients_at(a, b.by, J);
+    }
+};
+template <class R>
+struct GFill {
+    static constexpr int kMinBlocks = 4;
+    using Args = FillArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        fill_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GTangentRhs {
+    static constexpr int kMinBlocks = 4;
+    using Args = TangentRhsArgs<R, R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        tangent_rhs_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+template <class R>
+struct GNewtonUpdate {
+    static constexpr int kMinBlocks = 4;
+    using Args = NewtonUpdateArgs<R, R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        newton_update_at(a, b.by, b.bx * kThreads + threadIdx.x);
+    }
+};
+struct GNorms {
+    static constexpr int kMinBlocks = 1;
+    using Args = NormsArgs;
+    static constexpr int kThreads = kNormThreads;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock) {
+        finish_norms_block(a.partial, a.nblocks, a.out);
+    }
+};
+
+// Stencil kernels: the tile bodies of the per-hierarchy kernels, staged with
+// plain loads.
+template <int N>
+__device__ __forceinline__ BoxMaps<N> no_maps() {
+    BoxMaps<N> m;
+    m.use = 0;
+    return m;
+}
+
+// Register budgets: the per-hierarchy kernels' resident blocks per SM.
+template <class R, bool PHI_LIVE, int MINB>
+struct GSweep {
+    static constexpr int kMinBlocks = MINB;
+    using Args = SweepArgs<R>;
+    static constexpr int kThreads = kSweepThreads;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        vanka_sweep_tile<R, PHI_LIVE>(a, a.gmode, b);
+    }
+};
+template <class R>
+struct GResidual {
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 4 : 5;
+    using Args = ResidualArgs<R>;
+    static constexpr int kThreads = 256;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        residual_tile<R>(a, no_maps<7>(), b);
+    }
+};
+template <class R>
+struct GVjp {
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 3;
+    using Args = VjpArgs<R>;
+    static constexpr int kThreads = kTileA * kTileA;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) { vjp_tile<R>(a, no_maps<9>(), b); }
+};
+template <class R>
+struct GJvp {
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 3 : 6;
+    using Args = JvpOpArgs<R>;
+    static constexpr int kThreads = kTileA * kTileA;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        jvp_tile<R>(a.a, a.mode, no_maps<JvpTile<R>::NB>(), b);
+    }
+};
+template <class R, bool TR>
+struct GBlockFactor {
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 4;
+    using Args = BlockArgs<R>;
+    static constexpr int kThreads = kTile * kTile;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+        block_factor_tile<R, TR>(a, no_maps<7>(), b);
+    }
+};
+template <class R, bool TR>
+struct GBlockSweep {
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 4 : 5;
+    using Args = BlockArgs<R>;
+    static constexpr int kThreads = kSweepThreads;
+    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) { block_sweep_tile<R, TR>(a, b); }
+};
+
+// The items of a launch whose member runs this cycle, in order, with their
+// first tile: computed by warp 0 of every block (lane k handles items k and
+// k + 32), read by the whole block.
+template <int N>
+struct GroupScan {
+    int count;
+    int idx[N];
+    int start[N + 1];
+};
+
+template <class A, int N>
+__device__ __forceinline__ void group_scan(const GroupParams<A, N>& P, GroupScan<N>& S) {
+    static_assert(N <= 64, "two items per lane");
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const unsigned lt = (1u << lane) - 1u;
+        int base = 0, placed = 0;
+        for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            const bool act = k < P.n && (P.when == 0 || (P.flags[P.item[k].member] & P.when) != 0);
+            int c = act ? P.item[k].blocks : 0;
+            int incl = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const unsigned ball = __ballot_sync(0xffffffffu, act);
+            if (act) {
+                const int pos = placed + __popc(ball & lt);
+                S.idx[pos] = k;
+                S.start[pos] = base + incl - c;
+            }
+            base += __shfl_sync(0xffffffffu, incl, 31);
+            placed += __popc(ball);
+        }
+        if (lane == 0) {
+            S.count = placed;
+            S.start[placed] = base;
+        }
+    }
+    __syncthreads();
+}
+
+template <class Op, int N>
+__global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks)
+    k_group(const __grid_constant__ GroupParams<typename Op::Args, N> P) {
+    __shared__ GroupScan<N> S;
+    group_scan(P, S);
+    const int total = S.start[S.count];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        int lo = 0, hi = S.count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (S.start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const int k = S.idx[lo];
+        const GroupItem& it = P.item[k];
+        const unsigned gx = unsigned(it.gx), local = unsigned(t - S.start[lo]), per = gx * unsigned(it.gy);
+        const unsigned rest = local % per;
+        Op::run(P.args[k], GroupBlock{rest % gx, rest / gx, local / per, gx});
+        __syncthreads();  // the next tile restages the block's shared memory
+    }
+}
+
+// ------------------------------------------------------------ convergence
+// Per-member solve state on the device, and the per-hierarchy solve loop's
+// decisions taken there (Solver::solve_loop): another cycle while
+// rel > rtol, |r| > atol and cycles < max; on a forward solve with the Newton
+// method, a Newton step once rel <= newton_switch and rel <= gate, preceded
+// by the Newton prologue when the previous cycle was not one, its state saved
+// first and restored if the residual grew (gate then drops tenfold), and
+// Newton switched off after two steps that cut the residual by less than the
+// stall ratio.  A cycle's launches are predicated on the member's flag bits.
+constexpr int kGroupHistory = GLIDE_MAX_HISTORY;
+enum GroupFlag {
+    kGroupRun = 1,     // the member runs this cycle
+    kGroupFas = 2,     // ... a FASCD cycle (or a linear cycle)
+    kGroupNewton = 4,  // ... a Newton step (saved state, tangent solve, update)
+    kGroupPro = 8,     // ... preceded by the Newton prologue
+    kGroupUndo = 16,   // the Newton step is undone
+};
+enum GroupStatus { GS_RUNNING = 0, GS_DONE = 1, GS_NONFINITE = 2 };
+enum GroupPhase { GC_INIT = 0, GC_PRE = 1, GC_MID = 2, GC_POST = 3, GC_END = 4 };
+
+struct GroupMember {
+    const double* norms;  // the member's norm vector |r_u|, |r_v|, |r_H|, |r|
+    double rtol, atol;
+    double newton_switch, stall_ratio;
+    int max_cycles;
+    int newton;           // forward solve with the Newton method
+    int cycles, status;
+    int in_newton, newton_off, stall, rejects;
+    int fas_cycles, prologues;  // cycles that were FASCD (or linear) cycles; Newton prologues run
+    double r0, last, rel, prev, gate;
+    double last_norms[3];
+    double history[kGroupHistory];
+};
+
+constexpr int kGroupControlThreads = 1024;
+
+// One phase of the decisions for every member (one thread each).  Members
+// that stopped are left alone.  running[0] receives the number of members
+// still running after GC_INIT and GC_END.
+__global__ void __launch_bounds__(kGroupControlThreads)
+    k_group_control(GroupMember* m, int* flags, int n, int phase, int* running) {
+    __shared__ int count;
+    if (threadIdx.x == 0) count = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        GroupMember& g = m[k];
+        int f = flags[k];
+        if (phase == GC_INIT) {
+            const double ab = g.norms[3];
+            g.r0 = g.last = g.prev = ab;
+            g.rel = 1.0;
+            g.gate = g.newton_switch;
+            g.cycles = g.fas_cycles = g.prologues = 0;
+            g.in_newton = g.newton_off = g.stall = g.rejects = 0;
+            g.history[0] = ab;
+            for (int q = 0; q < 3; ++q) g.last_norms[q] = g.norms[q];
+            if (!isfinite(ab)) {
+                g.status = GS_NONFINITE;
+                f = 0;
+            } else {
+                const bool run = g.rel > g.rtol && ab > g.atol && g.max_cycles > 0;
+                g.status = run ? GS_RUNNING : GS_DONE;
+                f = run ? kGroupRun : 0;
+            }
+        } else if (!(f & kGroupRun)) {
+            continue;
+        } else if (phase == GC_PRE) {
+            const bool newton_phase = g.newton && g.rel <= g.newton_switch;
+            const bool step = newton_phase && !g.newton_off && g.rel <= g.gate;
+            f = kGroupRun | (step ? kGroupNewton : kGroupFas) | (step && !g.in_newton ? kGroupPro : 0);
+            if (!step) g.in_newton = 0;
+        } else if (phase == GC_MID) {
+            if (f & kGroupPro) {
+                g.prev = g.norms[3];
+                g.in_newton = 1;
+                g.prologues += 1;
+            }
+        } else if (phase == GC_POST) {
+            if ((f & kGroupNewton) && !(g.norms[3] <= g.prev)) f |= kGroupUndo;
+        } else {  // GC_END
+            double ab = g.norms[3];
+            for (int q = 0; q < 3; ++q) g.last_norms[q] = g.norms[q];
+            if (f & kGroupUndo) {
+                ab = g.prev;
+                g.gate = 0.1 * (g.prev / g.r0);
+                g.in_newton = 0;
+                g.stall = 0;
+                g.rejects += 1;
+            }
+            if (!isfinite(ab)) {
+                g.status = GS_NONFINITE;
+                g.last = ab;
+                flags[k] = 0;
+                continue;
+            }
+            g.rel = ab / g.r0;
+            if ((f & kGroupNewton) && g.in_newton) {
+                g.stall = ab > g.stall_ratio * g.prev ? g.stall + 1 : 0;
+                if (g.stall >= 2) g.newton_off = 1;
+            }
+            g.prev = ab;
+            g.last = ab;
+            g.cycles += 1;
+            if (!(f & kGroupNewton)) g.fas_cycles += 1;
+            if (g.cycles < kGroupHistory) g.history[g.cycles] = ab;
+            const bool run = g.rel > g.rtol && ab > g.atol && g.cycles < g.max_cycles;
+            g.status = run ? GS_RUNNING : GS_DONE;
+            f = run ? kGroupRun : 0;
+        }
+        flags[k] = f;
+        if (f & kGroupRun) atomicAdd(&count, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && (phase == GC_INIT || phase == GC_END)) *running = count;
+}
+
+}  // namespace glide

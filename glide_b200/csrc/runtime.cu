@@ -10,7 +10,9 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
+#include <functional>
 #include <mutex>
 #include <cstdio>
 #include <cstring>
@@ -23,11 +25,17 @@
 #include "adjoint_kernels.cuh"
 #include "tangent_kernels.cuh"
 #include "transfer_kernels.cuh"
+#include "group.cuh"
 
 namespace glide {
 
 // ------------------------------------------------------------------ errors
 static thread_local std::string g_err;
+
+// Stream captures of CUDA graphs and the device allocations made while
+// solving take this lock: handles driven from several host threads then never
+// allocate while another thread's capture is open, nor open two at once.
+static std::mutex g_capture_mu;
 
 struct Fail {
     int code;
@@ -50,32 +58,8 @@ static void check_launch(const char* what) {
     if (e != cudaSuccess) fail(GLIDE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-constexpr int kNormThreads = 1024;
-
 __global__ void __launch_bounds__(kNormThreads) k_finish_norms(const double* partial, int nblocks, double* out) {
-    // thread-strided sums, a fixed shuffle tree per warp, then warp 0 over
-    // the 32 warp sums: the same order on every call
-    __shared__ double ws[3][32];
-    const int t = threadIdx.x, l = t & 31, w = t >> 5;
-    double s[3] = {0, 0, 0};
-    for (int b = t; b < nblocks; b += kNormThreads)
-        for (int q = 0; q < 3; ++q) s[q] += partial[size_t(b) * 3 + q];
-    for (int o = 16; o > 0; o >>= 1)
-        for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
-    if (l == 0)
-        for (int q = 0; q < 3; ++q) ws[q][w] = s[q];
-    __syncthreads();
-    if (w == 0) {
-        for (int q = 0; q < 3; ++q) s[q] = ws[q][l];
-        for (int o = 16; o > 0; o >>= 1)
-            for (int q = 0; q < 3; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
-        if (l == 0) {
-            out[0] = sqrt(s[0]);
-            out[1] = sqrt(s[1]);
-            out[2] = sqrt(s[2]);
-            out[3] = sqrt(s[0] + s[1] + s[2]);
-        }
-    }
+    finish_norms_block(partial, nblocks, out);
 }
 
 // ------------------------------------------------------------------ fields
@@ -186,6 +170,19 @@ struct SolverBase {
     double newton_stall_ratio = 0.7;
 };
 
+// A launch recorded instead of issued, for grouped execution: the kind and
+// template variant, the grid the per-hierarchy launch would use, the argument
+// struct's bytes and the launch's algorithmic bytes.
+struct RecOp {
+    int op, variant;
+    int gx, gy, gz;
+    std::vector<unsigned char> args;
+    double bytes;
+};
+
+template <class R>
+struct Solver;
+
 template <class R>
 struct Level {
     int ny = 0, nx = 0;
@@ -238,6 +235,23 @@ struct Solver : SolverBase {
     bool last_not_converged = false;  // the last solve_loop ended short of its tolerances
     double last_relative = 0.0;
     int last_cycles = 0;
+
+    // While set, the launches of the cycle bodies are appended here instead
+    // of issued; launch sites that have no grouped form refuse.
+    std::vector<RecOp>* rec = nullptr;
+
+    template <class A>
+    bool record(int op, int variant, dim3 g, const A& a, double bytes) {
+        if (!rec) return false;
+        RecOp r{op, variant, int(g.x), int(g.y), int(g.z), std::vector<unsigned char>(sizeof(A)), bytes};
+        std::memcpy(r.args.data(), &a, sizeof(A));
+        rec->push_back(std::move(r));
+        return true;
+    }
+
+    void not_recordable(const char* what) const {
+        if (rec) fail(GLIDE_ERR_STATE, std::string(what) + " has no grouped form");
+    }
 
     void counted(const char* what, double bytes) {
         check_launch(what);
@@ -320,11 +334,16 @@ struct Solver : SolverBase {
     static dim3 pw_grid(int rows, int cols) { return dim3((cols + 255) / 256, rows); }
 
     void fill(const Arr<R>& a, R val, cudaStream_t s) {
+        if (record(G_FILL, 0, pw_grid(a.rows, a.cols), FillArgs<R>{a, val}, double(a.rows) * a.cols * sizeof(R)))
+            return;
         k_fill<R><<<pw_grid(a.rows, a.cols), 256, 0, s>>>(a, val, a.rows, a.cols);
         counted("fill", double(a.rows) * a.cols * sizeof(R));
     }
 
     void copy(const Arr<R>& dst, const Arr<R>& src, cudaStream_t s) {
+        if (record(G_COPY, 0, pw_grid(src.rows, src.cols), CopyArgs<R>{dst, src},
+                   2.0 * src.rows * src.cols * sizeof(R)))
+            return;
         GCU(cudaMemcpy2DAsync(dst.p, size_t(dst.pitch) * sizeof(R), src.p, size_t(src.pitch) * sizeof(R),
                               size_t(src.cols) * sizeof(R), src.rows, cudaMemcpyDeviceToDevice, s));
         traffic(2.0 * src.rows * src.cols * sizeof(R));
@@ -343,6 +362,9 @@ struct Solver : SolverBase {
         if (fa.cols == lv[l].nx + 1) kind = kFaceU;
         else if (fa.rows == lv[l].ny + 1) kind = kFaceV;
         else kind = cell_kind >= 0 ? cell_kind : kCellAvg;
+        if (record(G_RESTRICT, 0, pw_grid(C.ny + 1, C.nx + 1), RestrictArgs<R>{fa, ca, copy_to, kind, C.ny, C.nx},
+                   restrict_bytes(l, kind, copy_to.p != nullptr)))
+            return;
         k_restrict<R><<<pw_grid(C.ny + 1, C.nx + 1), 256, 0, s>>>(fa, ca, copy_to, kind, C.ny, C.nx);
         counted("restrict", restrict_bytes(l, kind, copy_to.p != nullptr));
     }
@@ -364,6 +386,11 @@ struct Solver : SolverBase {
 
     void compute_phi(int l, double relax, cudaStream_t s) {
         Level<R>& v = lv[l];
+        if (record(G_GROUNDED, 0, pw_grid(v.ny, v.nx),
+                   GroundedArgs<R>{v.a[GLIDE_PHI], v.a[GLIDE_H], v.a[GLIDE_BED], R(v.phys.flotation_reg_driving),
+                                   R(relax), v.ny, v.nx},
+                   lb(l, 4)))
+            return;
         k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_PHI], v.a[GLIDE_H], v.a[GLIDE_BED],
                                                           R(v.phys.flotation_reg_driving), R(relax), v.ny, v.nx);
         counted("grounded", lb(l, 4));  // H, bed, phi read; phi written
@@ -371,8 +398,9 @@ struct Solver : SolverBase {
 
     void set_rhs(int l, double dt, cudaStream_t s) {
         Level<R>& v = lv[l];
-        k_set_rhs<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_F_H], v.a[GLIDE_H_PREV], v.a[GLIDE_SMB],
-                                                         R(dt), v.ny, v.nx);
+        const SetRhsArgs<R> a{v.a[GLIDE_F_H], v.a[GLIDE_H_PREV], v.a[GLIDE_SMB], R(dt), v.ny, v.nx};
+        if (record(G_SET_RHS, 0, pw_grid(v.ny, v.nx), a, lb(l, 3))) return;
+        k_set_rhs<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(a);
         counted("set_rhs", lb(l, 3));
     }
 
@@ -396,14 +424,22 @@ struct Solver : SolverBase {
         a.use_forcing = use_forcing; a.use_mask = use_mask;
         a.active_set = active_set ? 1 : 0;
         dim3 g(v.blocks_x(), v.blocks_y());
-        k_residual<R><<<g, 256, 0, s>>>(a, box_maps(l, kStateBoxes));
         // u, v, H, phi, mask, bed, B, beta, gamma; forcing; subtrahend; 3 rows
         // written (and the active set)
-        counted("residual", lb(l, 9 + (use_forcing ? 3 : 0) + (sub ? 3 : 0) + 3 + (active_set ? 1 : 0)));
-        if (norms) {
-            k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
-            counted("finish_norms", 24.0 * g.x * g.y + 32.0);
+        const double bytes = lb(l, 9 + (use_forcing ? 3 : 0) + (sub ? 3 : 0) + 3 + (active_set ? 1 : 0));
+        if (!record(G_RESIDUAL, 0, g, a, bytes)) {
+            k_residual<R><<<g, 256, 0, s>>>(a, box_maps(l, kStateBoxes));
+            counted("residual", bytes);
         }
+        if (norms) finish_norms(int(g.x * g.y), s);
+    }
+
+    // the norm vector of the per-block partials of the last stencil pass
+    void finish_norms(int nblocks, cudaStream_t s) {
+        const double bytes = 24.0 * nblocks + 32.0;
+        if (record(G_NORMS, 0, dim3(1), NormsArgs{partial, nblocks, norms_dev}, bytes)) return;
+        k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, nblocks, norms_dev);
+        counted("finish_norms", bytes);
     }
 
     void vanka_dump(int l, double dt, R* J, R* r, cudaStream_t s) {
@@ -418,12 +454,14 @@ struct Solver : SolverBase {
         a.p = physr(l, dt, false);
         a.ny = v.ny; a.nx = v.nx;
         a.use_forcing = 1; a.use_mask = 0; a.active_set = 0;
+        not_recordable("vanka_dump");
         k_vanka_dump<R><<<dim3(v.blocks_x(), v.blocks_y()), 256, 0, s>>>(a, J, r);
         counted("vanka_dump", lb(l, 11 + 30));
     }
 
     // the norm vector and, in the same copy, the error word behind it
     void read_norms(double out[4], cudaStream_t s) {
+        not_recordable("read_norms");
         GCU(cudaMemcpyAsync(norms_host, norms_dev, 4 * sizeof(double) + sizeof(int), cudaMemcpyDeviceToHost, s));
         GCU(cudaStreamSynchronize(s));
         for (int q = 0; q < 4; ++q) out[q] = norms_host[q];
@@ -514,10 +552,13 @@ struct Solver : SolverBase {
             a.uo = v.a[ou]; a.vo = v.a[ov]; a.Ho = v.a[oh];
             a.iters = (k == n - 1) ? iters : nullptr;
             if (!freeze_phi && !phi_live) {
-                k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(v.a[GLIDE_PHI], v.a[ih], v.a[GLIDE_BED],
-                                                                  R(v.phys.flotation_reg_driving), R(c.relax_phi),
-                                                                  v.ny, v.nx);
-                counted("grounded", lb(l, 4));
+                const GroundedArgs<R> ga{v.a[GLIDE_PHI], v.a[ih], v.a[GLIDE_BED], R(v.phys.flotation_reg_driving),
+                                         R(c.relax_phi), v.ny, v.nx};
+                if (!record(G_GROUNDED, 0, pw_grid(v.ny, v.nx), ga, lb(l, 4))) {
+                    k_grounded<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(ga.phi, ga.H, ga.bed, ga.c, ga.relax, v.ny,
+                                                                      v.nx);
+                    counted("grounded", lb(l, 4));
+                }
             }
             launch_sweep(a, gmode, phi_live, g, s, lb(l, 15));
         }
@@ -535,6 +576,12 @@ struct Solver : SolverBase {
     // one fused sweep: u, v, H, f_u, f_v, f_H, bed, B, beta, gamma, phi read;
     // u, v, H, mask written (15 N s)
     void launch_sweep(const SweepArgs<R>& a, int gmode, bool phi_live, dim3 g, cudaStream_t s, double bytes) {
+        if (rec) {
+            SweepArgs<R> ga = a;
+            ga.gmode = gmode;
+            record(G_SWEEP, (phi_live ? 1 : 0) | (sweep_blocks_per_sm >= 2 ? 2 : 0), g, ga, bytes);
+            return;
+        }
         if (sweep_blocks_per_sm >= 2) launch_sweep_occ<2>(a, gmode, phi_live, g, s);
         else launch_sweep_occ<1>(a, gmode, phi_live, g, s);
         counted("vanka_sweep", bytes);
@@ -562,9 +609,10 @@ struct Solver : SolverBase {
         b.nyc = C.ny; b.nxc = C.nx;
         dim3 g = pw_grid(C.ny + 1, C.nx + 1);
         g.z = n;
-        k_restrict_batch<R><<<g, 256, 0, s>>>(b);
         double bytes = 0;
         for (int q = 0; q < n; ++q) bytes += restrict_bytes(l, b.kind[q], jobs[q].copy_to >= 0);
+        if (record(G_RESTRICT_BATCH, 0, g, b, bytes)) return;
+        k_restrict_batch<R><<<g, 256, 0, s>>>(b);
         counted("restrict_batch", bytes);
     }
 
@@ -580,9 +628,11 @@ struct Solver : SolverBase {
         }
         dim3 g = pw_grid(F.ny + 1, F.nx + 1);
         g.z = 3;
-        k_correct_batch<R><<<g, 256, 0, s>>>(b);
         // per field: fine x and w read, x written; coarse x and w read
-        counted("correct_batch", 3 * (lb(l, 3) + lb(l + 1, 2)));
+        const double bytes = 3 * (lb(l, 3) + lb(l + 1, 2));
+        if (record(G_CORRECT_BATCH, 0, g, b, bytes)) return;
+        k_correct_batch<R><<<g, 256, 0, s>>>(b);
+        counted("correct_batch", bytes);
     }
 
 
@@ -594,10 +644,13 @@ struct Solver : SolverBase {
         const bool fcal = coarse && c.freeze_coarse_calving, fphi = coarse && c.freeze_coarse_phi;
         Level<R>& v = lv[l];
         if (finest) {
-            k_snapshot<R><<<pw_grid(v.ny + 1, v.nx + 1), 256, 0, s>>>(
-                v.a[GLIDE_U], v.a[GLIDE_V], v.a[GLIDE_H], v.a[F_W_U], v.a[F_W_V], v.a[F_W_H], v.a[F_CHI],
-                R(v.phys.thklim), v.ny, v.nx);
-            counted("snapshot", lb(l, 7));  // u, v, H read; w_u, w_v, w_H, chi written
+            const SnapshotArgs<R> sa{v.a[GLIDE_U], v.a[GLIDE_V], v.a[GLIDE_H], v.a[F_W_U], v.a[F_W_V],
+                                     v.a[F_W_H], v.a[F_CHI], R(v.phys.thklim), v.ny, v.nx};
+            // u, v, H read; w_u, w_v, w_H, chi written
+            if (!record(G_SNAPSHOT, 0, pw_grid(v.ny + 1, v.nx + 1), sa, lb(l, 7))) {
+                k_snapshot<R><<<pw_grid(v.ny + 1, v.nx + 1), 256, 0, s>>>(sa);
+                counted("snapshot", lb(l, 7));
+            }
         }
         if (l == n_levels - 1) {
             sweeps(l, dt, c.coarsest_steps, kGammaWChi, fcal, fphi, nullptr, s);
@@ -663,6 +716,7 @@ struct Solver : SolverBase {
         CachedGraph& cg = graphs[kind];
         if (!cg.exec || cg.version != version || cg.dt != dt || cg.start != start) {
             if (cg.exec) { cudaGraphExecDestroy(cg.exec); cg.exec = nullptr; }
+            std::lock_guard<std::mutex> lock(g_capture_mu);
             cudaGraph_t g;
             const long long before = launches;
             const double bytes_before = alg_bytes;
@@ -704,6 +758,7 @@ struct Solver : SolverBase {
 
     template <class D, class Src>
     void convert(const Arr<D>& d, const Arr<Src>& src, double scale, cudaStream_t s) {
+        not_recordable("convert");
         k_convert<D, Src><<<pw_grid(src.rows, src.cols), 256, 0, s>>>(d, src, scale, src.rows, src.cols);
         counted("convert", double(src.rows) * src.cols * (sizeof(D) + sizeof(Src)));
     }
@@ -741,6 +796,7 @@ struct Solver : SolverBase {
         Solver<float>& f = *lo;
         Level<R>& D = lv[l];
         Level<float>& F = f.lv[l];
+        not_recordable("mixed_cycle");
         push_to_shadow(l, {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_MASK, GLIDE_PHI}, false, s);
         residual(l, dt, true, false, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, false, s);
         push_to_shadow(l, {GLIDE_R_U, GLIDE_R_V, GLIDE_R_H}, false, s);
@@ -774,6 +830,7 @@ struct Solver : SolverBase {
 
     template <class Src>
     void convert_add(const Arr<R>& d, const Arr<Src>& src, cudaStream_t s) {
+        not_recordable("convert_add");
         k_add_converted<R, Src><<<pw_grid(src.rows, src.cols), 256, 0, s>>>(d, src, src.rows, src.cols);
         counted("add_converted", double(src.rows) * src.cols * (2 * sizeof(R) + sizeof(Src)));
     }
@@ -957,19 +1014,20 @@ struct Solver : SolverBase {
         if (L.tr) {
             const int fl[AdjTile<R>::NB] = {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_BED, GLIDE_BETA,
                                             GLIDE_B, L.x[0], L.x[1]};
-            k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a, box_maps(l, fl, AdjTile<R>::BH));
-            counted("vjp", lin_bytes);
+            if (!record(G_VJP, 0, g, a, lin_bytes)) {
+                k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a, box_maps(l, fl, AdjTile<R>::BH));
+                counted("vjp", lin_bytes);
+            }
         } else {
             const int fl[JvpTile<R>::NB] = {GLIDE_U, GLIDE_V, L.x[0], L.x[1], GLIDE_H, GLIDE_PHI, GLIDE_BED,
                                             GLIDE_BETA, GLIDE_B, L.x[2]};
             const int mode = (ref_rows ? 1 : 0) | ((jvp_flags & GLIDE_USE_MASK) ? 0 : 2);
-            k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, mode, box_maps(l, fl));
-            counted("jvp", lin_bytes);
+            if (!record(G_JVP, 0, g, JvpOpArgs<R>{a, mode}, lin_bytes)) {
+                k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, mode, box_maps(l, fl));
+                counted("jvp", lin_bytes);
+            }
         }
-        if (norms) {
-            k_finish_norms<<<1, kNormThreads, 0, s>>>(partial, g.x * g.y, norms_dev);
-            counted("finish_norms", 24.0 * g.x * g.y + 32.0);
-        }
+        if (norms) finish_norms(int(g.x * g.y), s);
     }
 
     void vjp_into(int l, double dt, bool use_forcing, int ou, int ov, int oh, cudaStream_t s) {
@@ -989,6 +1047,7 @@ struct Solver : SolverBase {
     // allocated on first use, before any stream capture begins
     void ensure_blocks() {
         if (!blk.empty()) return;
+        std::lock_guard<std::mutex> lock(g_capture_mu);
         blk.assign(n_levels, nullptr);
         for (int l = 0; l < n_levels; ++l)
             GCU(cudaMalloc(&blk[l], size_t(25) * lv[l].ny * lv[l].pc * sizeof(R)));
@@ -1017,10 +1076,12 @@ struct Solver : SolverBase {
     void block_factor(int l, double dt, const Lin& L, cudaStream_t s) {
         BlockArgs<R> a = block_args(l, dt, L);
         dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
+        const double bytes = lb(l, 9 + 25);  // state read, 25 factor planes written
+        if (record(G_BLOCK_FACTOR, L.tr ? 1 : 0, g, a, bytes)) return;
         const BoxMaps<7> m = box_maps(l, kStateBoxes);
         if (L.tr) k_block_factor<R, true><<<g, kTile * kTile, 0, s>>>(a, m);
         else k_block_factor<R, false><<<g, kTile * kTile, 0, s>>>(a, m);
-        counted("block_factor", lb(l, 9 + 25));  // state read, 25 factor planes written
+        counted("block_factor", bytes);
     }
 
     // n linear smoother sweeps (residual, then block solve and update); the
@@ -1032,10 +1093,16 @@ struct Solver : SolverBase {
         dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
         for (int k = 0; k < n; ++k) {
             lin_residual(l, dt, L, false, s);
-            if (L.tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
-            else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
-            counted("linear_sweep", lb(l, 34));  // 25 factors, r, x read; x written
+            block_sweep(l, a, L.tr, g, s);
         }
+    }
+
+    // 25 factors, r, x read; x written
+    void block_sweep(int l, const BlockArgs<R>& a, bool tr, dim3 g, cudaStream_t s) {
+        if (record(G_BLOCK_SWEEP, tr ? 1 : 0, g, a, lb(l, 34))) return;
+        if (tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
+        else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
+        counted("linear_sweep", lb(l, 34));
     }
 
     void adj_sweeps(int l, double dt, int n, cudaStream_t s) { lin_sweeps(l, dt, n, adj_sys(), s); }
@@ -1050,10 +1117,7 @@ struct Solver : SolverBase {
             return;
         }
         BlockArgs<R> a = block_args(l, dt, L);
-        dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
-        if (L.tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
-        else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
-        counted("linear_sweep", lb(l, 34));
+        block_sweep(l, a, L.tr, dim3(lv[l].blocks_x(), lv[l].blocks_y()), s);
     }
 
     // glide/multigrid.py:905-973 (linear FAS)
@@ -1106,18 +1170,25 @@ struct Solver : SolverBase {
         Level<R>& D = lv[l];
         Level<T>& F = ts.lv[l];
         if constexpr (!std::is_same<T, R>::value) {
+            not_recordable("a mixed-precision Newton step");
             push_to_shadow(l, {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_MASK}, false, s);
         }
-        k_tangent_rhs<T, R><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
-            F.a[F_TF_U], F.a[F_TF_V], F.a[F_TF_H], D.a[GLIDE_R_U], D.a[GLIDE_R_V], D.a[GLIDE_R_H], D.a[GLIDE_H],
-            D.a[GLIDE_GAMMA], D.a[GLIDE_MASK], D.ny, D.nx);
-        counted("tangent_rhs", double(D.ny) * D.nx * (6 * sizeof(R) + 3 * sizeof(T)));
+        const TangentRhsArgs<T, R> ta{F.a[F_TF_U], F.a[F_TF_V], F.a[F_TF_H], D.a[GLIDE_R_U], D.a[GLIDE_R_V],
+                                      D.a[GLIDE_R_H], D.a[GLIDE_H], D.a[GLIDE_GAMMA], D.a[GLIDE_MASK], D.ny, D.nx};
+        const double ta_bytes = double(D.ny) * D.nx * (6 * sizeof(R) + 3 * sizeof(T));
+        if (!record(G_TANGENT_RHS, 0, pw_grid(D.ny + 1, D.nx + 1), ta, ta_bytes)) {
+            k_tangent_rhs<T, R><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(ta);
+            counted("tangent_rhs", ta_bytes);
+        }
         for (int fld : {F_E_U, F_E_V, F_E_H}) ts.fill(F.a[fld], T(0), s);
         for (int k = 0; k < tangent_vcycles; ++k) ts.lin_vcycle(l, true, dt, Solver<T>::tan_sys(), s);
-        k_newton_update<R, T><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(
-            D.a[GLIDE_U], D.a[GLIDE_V], D.a[GLIDE_H], D.a[GLIDE_GAMMA], F.a[F_E_U], F.a[F_E_V], F.a[F_E_H],
-            D.ny, D.nx);
-        counted("newton_update", double(D.ny) * D.nx * (7 * sizeof(R) + 3 * sizeof(T)));
+        const NewtonUpdateArgs<R, T> na{D.a[GLIDE_U], D.a[GLIDE_V], D.a[GLIDE_H], D.a[GLIDE_GAMMA],
+                                        F.a[F_E_U], F.a[F_E_V], F.a[F_E_H], D.ny, D.nx};
+        const double na_bytes = double(D.ny) * D.nx * (7 * sizeof(R) + 3 * sizeof(T));
+        if (!record(G_NEWTON_UPDATE, 0, pw_grid(D.ny + 1, D.nx + 1), na, na_bytes)) {
+            k_newton_update<R, T><<<pw_grid(D.ny + 1, D.nx + 1), 256, 0, s>>>(na);
+            counted("newton_update", na_bytes);
+        }
         residual(l, dt, true, false, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s, true);
     }
 
@@ -1164,8 +1235,431 @@ struct Solver : SolverBase {
         a.p = physr(l, dt, false);
         a.dt = R(dt);
         a.ny = v.ny; a.nx = v.nx;
+        const double bytes = lb(l, 9 + __builtin_popcount(unsigned(mask) & 15u));
+        if (record(G_GRADIENTS, 0, pw_grid(v.ny, v.nx), a, bytes)) return;
         k_gradients<R><<<pw_grid(v.ny, v.nx), 256, 0, s>>>(a);
-        counted("gradients", lb(l, 9 + __builtin_popcount(unsigned(mask) & 15u)));
+        counted("gradients", bytes);
+    }
+};
+
+// ================================================================== groups
+// One solver cycle run over several hierarchies of one value type in grouped
+// launches (group.cuh).  A plan is every member's cycle as its own Solver
+// code issues it, recorded instead of launched, then merged: the member with
+// the most launches left sets the next kind, and every member whose next
+// launch is of that kind joins it.  Each member's launches keep their order,
+// so a member computes exactly what its own solve computes.  A plan is
+// captured once as a CUDA graph and replayed; the graph of a cycle ends in
+// the device-side convergence test.
+struct GroupBase {
+    virtual ~GroupBase() {}
+    int dtype = GLIDE_F64;
+    long long launches = 0;  // grouped launches issued (graph replays included)
+    int shape[4] = {0, 0, 0, 0};  // last forward / adjoint cycle: grouped launches, member launches
+    virtual void forward(double dt, int start, glide_stats* st, cudaStream_t s) = 0;
+    virtual void backward(double dt, int start, int grad_mask, glide_stats* st, cudaStream_t s) = 0;
+};
+
+template <class R>
+struct GroupRun : GroupBase {
+    std::vector<Solver<R>*> members;
+    GroupMember* dev = nullptr;   // device solve state, one per member
+    int* flags = nullptr;         // device run flags; flags[n] counts the running members
+    int* running_host = nullptr;  // pinned copy of that count
+    std::vector<GroupMember> host;
+    cudaStream_t own_stream = nullptr;
+
+    struct Launch {
+        int op, variant, when;
+        std::vector<std::pair<int, const RecOp*>> items;  // (member, its recorded launch)
+    };
+    // A plan is a list of sections: grouped launches predicated on a flag bit,
+    // or one phase of the device-side decisions.
+    struct Section {
+        int control;  // a GroupPhase, or -1
+        int when;     // flag bits of the members whose launches run (0: every member)
+        std::function<void(Solver<R>&, int)> body;  // records member k's launches
+    };
+    struct Plan {
+        std::vector<int> control;                      // per section
+        std::vector<std::vector<std::vector<RecOp>>> rec;  // [section][member]
+        std::vector<std::vector<Launch>> launches;     // [section]
+        std::vector<std::vector<double>> bytes;        // [section][member]: algorithmic bytes
+        cudaGraphExec_t exec = nullptr;
+        long long nodes = 0;
+        std::vector<unsigned> versions;
+        double dt = 0;
+        int start = -1, extra = 0;
+        bool valid = false;
+    };
+    enum { P_FWD_PRO, P_FWD_CYCLE, P_ADJ_PRO, P_ADJ_CYCLE, P_GRAD, P_COUNT };
+    Plan plans[P_COUNT];
+    // the forward cycle's sections, in order (byte accounting reads them)
+    enum { S_PRE, S_PRO, S_MID, S_BACKUP, S_FAS, S_NEWTON, S_POST, S_UNDO, S_END };
+
+    explicit GroupRun(std::vector<Solver<R>*> m) : members(std::move(m)) {
+        dtype = sizeof(R) == 8 ? GLIDE_F64 : GLIDE_F32;
+        const int n = int(members.size());
+        host.resize(n);
+        GCU(cudaMalloc(&dev, sizeof(GroupMember) * n));
+        GCU(cudaMalloc(&flags, sizeof(int) * (n + 1)));
+        GCU(cudaMemset(flags, 0, sizeof(int) * (n + 1)));
+        GCU(cudaMallocHost(&running_host, sizeof(int)));
+        GCU(cudaDeviceSynchronize());
+    }
+
+    ~GroupRun() override {
+        for (Plan& p : plans)
+            if (p.exec) cudaGraphExecDestroy(p.exec);
+        if (own_stream) cudaStreamDestroy(own_stream);
+        if (running_host) cudaFreeHost(running_host);
+        if (flags) cudaFree(flags);
+        if (dev) cudaFree(dev);
+    }
+
+    // Record every member's sections into P (unless P is current) and merge
+    // each section's launches across members: the member with the most
+    // launches left sets the next kind, every member whose next launch is of
+    // that kind joins it.
+    void build(Plan& P, double dt, int start, int extra, const std::vector<Section>& secs) {
+        std::vector<unsigned> v;
+        for (auto* m : members) v.push_back(m->version);
+        if (P.valid && P.dt == dt && P.start == start && P.extra == extra && P.versions == v) return;
+        if (P.exec) {
+            cudaGraphExecDestroy(P.exec);
+            P.exec = nullptr;
+        }
+        P.valid = false;
+        const int n = int(members.size());
+        const size_t ns = secs.size();
+        P.control.assign(ns, -1);
+        P.rec.assign(ns, std::vector<std::vector<RecOp>>(n));
+        P.launches.assign(ns, {});
+        P.bytes.assign(ns, std::vector<double>(n, 0.0));
+        for (size_t q = 0; q < ns; ++q) {
+            P.control[q] = secs[q].control;
+            if (secs[q].control >= 0) continue;
+            for (int k = 0; k < n; ++k) {
+                Solver<R>& m = *members[k];
+                m.rec = &P.rec[q][k];
+                try {
+                    secs[q].body(m, k);
+                } catch (...) {
+                    m.rec = nullptr;
+                    throw;
+                }
+                m.rec = nullptr;
+                for (const RecOp& r : P.rec[q][k]) P.bytes[q][k] += r.bytes;
+            }
+            std::vector<size_t> pos(n, 0);
+            for (;;) {
+                int pick = -1;
+                size_t most = 0;
+                for (int k = 0; k < n; ++k)
+                    if (P.rec[q][k].size() - pos[k] > most) {
+                        most = P.rec[q][k].size() - pos[k];
+                        pick = k;
+                    }
+                if (pick < 0) break;
+                const RecOp& h = P.rec[q][pick][pos[pick]];
+                Launch L{h.op, h.variant, secs[q].when, {}};
+                for (int k = 0; k < n; ++k) {
+                    if (pos[k] == P.rec[q][k].size()) continue;
+                    const RecOp& r = P.rec[q][k][pos[k]];
+                    if (r.op == h.op && r.variant == h.variant) {
+                        L.items.push_back({k, &r});
+                        ++pos[k];
+                    }
+                }
+                P.launches[q].push_back(std::move(L));
+            }
+        }
+        P.versions = v;
+        P.dt = dt;
+        P.start = start;
+        P.extra = extra;
+        P.valid = true;
+    }
+
+    // One persistent launch per N items of L (N: what fits the parameter
+    // space): at most one wave of resident blocks, striding over the tiles
+    // of the items whose member runs.
+    template <class Op>
+    long long issue_op(const Launch& L, cudaStream_t s) {
+        using A = typename Op::Args;
+        constexpr int N = group_capacity<A>();
+        static_assert(sizeof(GroupParams<A, N>) <= 32764, "kernel parameters over the limit");
+        static const long long wave = [] {
+            int dev = 0, sms = 0, per_sm = 0;
+            GCU(cudaGetDevice(&dev));
+            GCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            GCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_group<Op, N>, Op::kThreads, 0));
+            return (long long)sms * std::max(per_sm, 1);
+        }();
+        long long issued = 0;
+        for (size_t base = 0; base < L.items.size(); base += N) {
+            auto P = std::make_unique<GroupParams<A, N>>();
+            P->flags = flags;
+            P->when = L.when;
+            long long nb = 0;
+            int k = 0;
+            for (size_t q = base; q < L.items.size() && k < N; ++q, ++k) {
+                const RecOp& r = *L.items[q].second;
+                if (r.args.size() != sizeof(A)) fail(GLIDE_ERR_STATE, "recorded arguments of the wrong size");
+                const long long blocks = (long long)r.gx * r.gy * r.gz;
+                if (blocks > 0x7fffffffLL) fail(GLIDE_ERR_SHAPE, "grouped launch over 2^31 tiles");
+                P->item[k] = GroupItem{int(blocks), r.gx, r.gy, L.items[q].first};
+                std::memcpy(static_cast<void*>(&P->args[k]), r.args.data(), sizeof(A));
+                nb += blocks;
+            }
+            if (nb > 0x7fffffffLL) fail(GLIDE_ERR_SHAPE, "grouped launch over 2^31 tiles");
+            P->n = k;
+            k_group<Op, N><<<unsigned(std::min(nb, wave)), Op::kThreads, 0, s>>>(*P);
+            check_launch("grouped launch");
+            ++issued;
+        }
+        return issued;
+    }
+
+    long long issue(const Launch& L, cudaStream_t s) {
+        const int v = L.variant;
+        switch (L.op) {
+            case G_SNAPSHOT: return issue_op<GSnapshot<R>>(L, s);
+            case G_RESTRICT: return issue_op<GRestrict<R>>(L, s);
+            case G_RESTRICT_BATCH: return issue_op<GRestrictBatch<R>>(L, s);
+            case G_CORRECT_BATCH: return issue_op<GCorrectBatch<R>>(L, s);
+            case G_GROUNDED: return issue_op<GGrounded<R>>(L, s);
+            case G_COPY: return issue_op<GCopy<R>>(L, s);
+            case G_FILL: return issue_op<GFill<R>>(L, s);
+            case G_SET_RHS: return issue_op<GSetRhs<R>>(L, s);
+            case G_TANGENT_RHS: return issue_op<GTangentRhs<R>>(L, s);
+            case G_NEWTON_UPDATE: return issue_op<GNewtonUpdate<R>>(L, s);
+            case G_GRADIENTS: return issue_op<GGradients<R>>(L, s);
+            case G_NORMS: return issue_op<GNorms>(L, s);
+            case G_RESIDUAL: return issue_op<GResidual<R>>(L, s);
+            case G_VJP: return issue_op<GVjp<R>>(L, s);
+            case G_JVP: return issue_op<GJvp<R>>(L, s);
+            case G_SWEEP:
+                if (v & 2) return (v & 1) ? issue_op<GSweep<R, true, 2>>(L, s) : issue_op<GSweep<R, false, 2>>(L, s);
+                return (v & 1) ? issue_op<GSweep<R, true, 1>>(L, s) : issue_op<GSweep<R, false, 1>>(L, s);
+            case G_BLOCK_FACTOR:
+                return v ? issue_op<GBlockFactor<R, true>>(L, s) : issue_op<GBlockFactor<R, false>>(L, s);
+            case G_BLOCK_SWEEP:
+                return v ? issue_op<GBlockSweep<R, true>>(L, s) : issue_op<GBlockSweep<R, false>>(L, s);
+            default: fail(GLIDE_ERR_STATE, "unknown grouped launch kind");
+        }
+        return 0;
+    }
+
+    // replay P's graph, capturing it first
+    void run_plan(Plan& P, cudaStream_t s) {
+        const int n = int(members.size());
+        if (!P.exec) {
+            std::lock_guard<std::mutex> lock(g_capture_mu);
+            cudaGraph_t g = nullptr;
+            long long nodes = 0;
+            GCU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                for (size_t q = 0; q < P.control.size(); ++q) {
+                    if (P.control[q] >= 0) {
+                        k_group_control<<<1, kGroupControlThreads, 0, s>>>(dev, flags, n, P.control[q], flags + n);
+                        check_launch("group_control");
+                        ++nodes;
+                    } else {
+                        for (const Launch& L : P.launches[q]) nodes += issue(L, s);
+                    }
+                }
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            GCU(cudaStreamEndCapture(s, &g));
+            const cudaError_t e = cudaGraphInstantiate(&P.exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) fail(GLIDE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            P.nodes = nodes;
+        }
+        GCU(cudaGraphLaunch(P.exec, s));
+        launches += P.nodes;
+    }
+
+    cudaStream_t stream_for(cudaStream_t s) {
+        // the legacy default stream cannot be captured (see Solver::cycle_and_check)
+        if (s) return s;
+        if (!own_stream) GCU(cudaStreamCreate(&own_stream));
+        return own_stream;
+    }
+
+    void check_members(int start) {
+        for (auto* m : members) {
+            m->check_level(start);
+            m->check_quirks();
+            if constexpr (sizeof(R) == 8) {
+                if (m->lo) fail(GLIDE_ERR_STATE, "mixed-precision hierarchies have no grouped form");
+            }
+        }
+    }
+
+    static Section launches_of(int when, std::function<void(Solver<R>&, int)> body) {
+        return Section{-1, when, std::move(body)};
+    }
+    static Section control(int phase) { return Section{phase, 0, nullptr}; }
+
+    // the prologue plan, then cycles until no member runs; returns the
+    // members' final device state in `host`
+    void solve(Plan& pro, Plan& cyc, int cfg, bool forward, cudaStream_t s) {
+        const int n = int(members.size());
+        int max_cycles = 0;
+        for (int k = 0; k < n; ++k) {
+            Solver<R>& m = *members[k];
+            const glide_fas_config& c = m.fas[cfg];
+            GroupMember& g = host[k];
+            std::memset(static_cast<void*>(&g), 0, sizeof(g));
+            g.norms = m.norms_dev;
+            g.rtol = c.relative_tolerance;
+            g.atol = c.absolute_tolerance;
+            g.max_cycles = c.maximum_vcycles;
+            g.newton = forward && m.forward_method == 1;
+            g.newton_switch = m.newton_switch;
+            g.stall_ratio = m.newton_stall_ratio;
+            max_cycles = std::max(max_cycles, c.maximum_vcycles);
+        }
+        GCU(cudaMemcpyAsync(dev, host.data(), sizeof(GroupMember) * n, cudaMemcpyHostToDevice, s));
+        run_plan(pro, s);  // ends with the GC_INIT phase
+        for (int it = 0;; ++it) {
+            GCU(cudaMemcpyAsync(running_host, flags + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+            GCU(cudaStreamSynchronize(s));
+            if (*running_host == 0 || it >= max_cycles) break;
+            run_plan(cyc, s);  // ends with the GC_END phase
+        }
+        GCU(cudaMemcpyAsync(host.data(), dev, sizeof(GroupMember) * n, cudaMemcpyDeviceToHost, s));
+        GCU(cudaStreamSynchronize(s));
+    }
+
+    // statistics and the members' own records of the solve
+    void finish(const Plan& pro, int cfg, glide_stats* st, const std::function<double(int)>& bytes) {
+        int bad = -1;
+        for (size_t k = 0; k < members.size(); ++k) {
+            const GroupMember& g = host[k];
+            Solver<R>& m = *members[k];
+            if (st) {
+                glide_stats& o = st[k];
+                std::memset(&o, 0, sizeof(o));
+                o.vcycles = g.cycles;
+                o.initial_norm = g.r0;
+                o.final_norm = g.last;
+                for (int q = 0; q < 3; ++q) o.norms[q] = g.last_norms[q];
+                for (int q = 0; q <= g.cycles && q < GLIDE_MAX_HISTORY; ++q) o.history[q] = g.history[q];
+            }
+            double b = bytes(int(k));
+            for (const auto& sec : pro.bytes) b += sec[k];
+            m.traffic(b);
+            m.newton_rejects += g.rejects;
+            const double rel = g.r0 > 0 ? g.last / g.r0 : 0.0;
+            const glide_fas_config& c = m.fas[cfg];
+            m.last_not_converged = !(rel <= c.relative_tolerance || g.last <= c.absolute_tolerance);
+            m.last_relative = rel;
+            m.last_cycles = g.cycles;
+            if (g.status == GS_NONFINITE && bad < 0) bad = int(k);
+        }
+        if (bad >= 0) fail(GLIDE_ERR_NONFINITE, "member " + std::to_string(bad) + ": residual norm is not finite");
+    }
+
+    void note_shape(const Plan& P, int slot) {
+        int grouped = 0;
+        long long total = 0;
+        for (size_t q = 0; q < P.control.size(); ++q) {
+            grouped += int(P.launches[q].size());
+            for (const auto& r : P.rec[q]) total += (long long)r.size();
+        }
+        shape[slot] = grouped;
+        shape[slot + 1] = int(total);
+    }
+
+    void forward(double dt, int start, glide_stats* st, cudaStream_t s) override {
+        s = stream_for(s);
+        check_members(start);
+        bool any_newton = false;
+        for (auto* m : members)
+            if (m->forward_method == 1) {
+                m->ensure_blocks();
+                any_newton = true;
+            }
+        auto is_newton = [&](int k) { return members[k]->forward_method == 1; };
+        build(plans[P_FWD_PRO], dt, start, 0,
+              {launches_of(0, [&](Solver<R>& m, int) {
+                   m.set_rhs(start, dt, s);
+                   m.residual(start, dt, true, true, false, false, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true,
+                              s);
+               }),
+               control(GC_INIT)});
+        auto fas = [&](Solver<R>& m, int) {
+            m.vcycle(start, true, dt, s);
+            m.residual(start, dt, true, true, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
+        };
+        auto save = [&](Solver<R>& m, int k, bool undo) {
+            if (!is_newton(k)) return;
+            Level<R>& L0 = m.lv[start];
+            const int x[4] = {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_MASK}, b[4] = {F_BK_U, F_BK_V, F_BK_H, F_BK_MASK};
+            for (int q = 0; q < 4; ++q) {
+                if (undo) m.copy(L0.a[x[q]], L0.a[b[q]], s);
+                else m.copy(L0.a[b[q]], L0.a[x[q]], s);
+            }
+        };
+        std::vector<Section> cycle;
+        if (any_newton) {
+            // the per-hierarchy solve loop's sequence for the Newton method
+            cycle = {control(GC_PRE),
+                     launches_of(kGroupPro, [&](Solver<R>& m, int k) {
+                         if (is_newton(k)) m.newton_prologue(start, dt, true, s);
+                     }),
+                     control(GC_MID),
+                     launches_of(kGroupNewton, [&](Solver<R>& m, int k) { save(m, k, false); }),
+                     launches_of(kGroupFas, fas),
+                     launches_of(kGroupNewton, [&](Solver<R>& m, int k) {
+                         if (is_newton(k)) m.newton_cycle(start, dt, s);
+                     }),
+                     control(GC_POST),
+                     launches_of(kGroupUndo, [&](Solver<R>& m, int k) { save(m, k, true); }),
+                     control(GC_END)};
+        } else {
+            cycle = {launches_of(kGroupRun, fas), control(GC_END)};
+        }
+        Plan& C = plans[P_FWD_CYCLE];
+        build(C, dt, start, any_newton ? 1 : 0, cycle);
+        note_shape(C, 0);
+        solve(plans[P_FWD_PRO], C, 0, true, s);
+        finish(plans[P_FWD_PRO], 0, st, [&](int k) {
+            const GroupMember& g = host[k];
+            if (!any_newton) return g.cycles * C.bytes[0][k];
+            // FASCD cycles, Newton steps (state saved), prologues and undone steps
+            const int steps = g.cycles - g.fas_cycles;
+            return g.fas_cycles * C.bytes[S_FAS][k] + steps * (C.bytes[S_BACKUP][k] + C.bytes[S_NEWTON][k]) +
+                   g.prologues * C.bytes[S_PRO][k] + g.rejects * C.bytes[S_UNDO][k];
+        });
+    }
+
+    void backward(double dt, int start, int grad_mask, glide_stats* st, cudaStream_t s) override {
+        s = stream_for(s);
+        check_members(start);
+        for (auto* m : members) m->ensure_blocks();
+        build(plans[P_ADJ_PRO], dt, start, 0,
+              {launches_of(0, [&](Solver<R>& m, int) { m.adj_residual(start, dt, true, s); }), control(GC_INIT)});
+        Plan& C = plans[P_ADJ_CYCLE];
+        build(C, dt, start, 0,
+              {launches_of(kGroupRun,
+                           [&](Solver<R>& m, int) {
+                               m.adj_vcycle(start, true, dt, s);
+                               m.adj_residual(start, dt, true, s);
+                           }),
+               control(GC_END)});
+        build(plans[P_GRAD], dt, start, grad_mask,
+              {launches_of(0, [&](Solver<R>& m, int) { m.gradients(start, dt, grad_mask, s); })});
+        note_shape(C, 2);
+        solve(plans[P_ADJ_PRO], C, 1, false, s);
+        run_plan(plans[P_GRAD], s);
+        finish(plans[P_ADJ_PRO], 1, st, [&](int k) { return host[k].cycles * C.bytes[0][k] + plans[P_GRAD].bytes[0][k]; });
     }
 };
 
@@ -1176,6 +1670,10 @@ using namespace glide;
 
 struct glide_solver {
     std::unique_ptr<SolverBase> impl;
+};
+
+struct glide_group_s {
+    std::unique_ptr<GroupBase> impl;
 };
 
 namespace {
@@ -1659,6 +2157,65 @@ int glide_transfer(int op, int dtype, int ny_fine, int nx_fine, const void* src,
         };
         if (dtype == GLIDE_F64) run(static_cast<const double*>(src));
         else run(static_cast<const float*>(src));
+    });
+}
+
+int glide_group_create(const glide_handle* members, int n, glide_group* out) {
+    return guarded([&] {
+        if (!out) fail(GLIDE_ERR_ARG, "out is null");
+        *out = nullptr;
+        if (!members || n <= 0) fail(GLIDE_ERR_ARG, "a group needs at least one member");
+        if (n > kGroupControlThreads) fail(GLIDE_ERR_ARG, "too many members");
+        for (int k = 0; k < n; ++k) {
+            if (!members[k] || !members[k]->impl) fail(GLIDE_ERR_ARG, "null member handle");
+            for (int q = 0; q < k; ++q)
+                if (members[q] == members[k]) fail(GLIDE_ERR_ARG, "a handle appears twice in the group");
+            if (members[k]->impl->dtype != members[0]->impl->dtype)
+                fail(GLIDE_ERR_ARG, "group members must share one dtype");
+        }
+        auto g = std::make_unique<glide_group_s>();
+        if (members[0]->impl->dtype == GLIDE_F64) {
+            std::vector<Solver<double>*> v;
+            for (int k = 0; k < n; ++k) {
+                auto* m = static_cast<Solver<double>*>(members[k]->impl.get());
+                if (m->lo) fail(GLIDE_ERR_STATE, "mixed-precision hierarchies have no grouped form");
+                v.push_back(m);
+            }
+            g->impl = std::make_unique<GroupRun<double>>(std::move(v));
+        } else {
+            std::vector<Solver<float>*> v;
+            for (int k = 0; k < n; ++k) v.push_back(static_cast<Solver<float>*>(members[k]->impl.get()));
+            g->impl = std::make_unique<GroupRun<float>>(std::move(v));
+        }
+        *out = g.release();
+    });
+}
+
+int glide_group_destroy(glide_group g) {
+    return guarded([&] { delete g; });
+}
+
+int glide_group_forward(glide_group g, double dt, int start_level, glide_stats* stats, void* stream) {
+    return guarded([&] {
+        if (!g || !g->impl) fail(GLIDE_ERR_ARG, "null group");
+        g->impl->forward(dt, start_level, stats, S(stream));
+    });
+}
+
+int glide_group_backward(glide_group g, double dt, int start_level, int grad_mask, glide_stats* stats,
+                         void* stream) {
+    return guarded([&] {
+        if (!g || !g->impl) fail(GLIDE_ERR_ARG, "null group");
+        g->impl->backward(dt, start_level, grad_mask, stats, S(stream));
+    });
+}
+
+int glide_group_counters(glide_group g, long long* launches, int* shape) {
+    return guarded([&] {
+        if (!g || !g->impl) fail(GLIDE_ERR_ARG, "null group");
+        if (launches) *launches = g->impl->launches;
+        if (shape)
+            for (int q = 0; q < 4; ++q) shape[q] = g->impl->shape[q];
     });
 }
 

@@ -190,9 +190,9 @@ __device__ __forceinline__ void eta_and_dot(const S& s, R Bc, const PhysR<R>& p,
 // warp computes a 4 x 8 patch of the 16 x 16 tile.
 // The arrays k_jvp stages, in the order of its BoxMaps: u, v, e_u, e_v, H,
 // phi, bed, beta, B, e_H.
-template <class R>
-__global__ void __launch_bounds__(kTileA * kTileA)
-    k_jvp(VjpArgs<R> a, int mode, const __grid_constant__ BoxMaps<JvpTile<R>::NB> maps) {
+template <class R, class BLK>
+__device__ __forceinline__ void jvp_tile(const VjpArgs<R>& a, int mode, const BoxMaps<JvpTile<R>::NB>& maps,
+                                         BLK blk) {
     // mode bit 0: the reference's row conventions; bit 1: mask ignored
     // (the reference's use_mask = False, which reads the mask as 0)
     const bool ref_rows = (mode & 1) != 0, use_mask = (mode & 2) == 0;
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kTileA * kTileA)
     __shared__ __align__(128) TT T;
     __shared__ double red[3][kTileA * kTileA / 32];
     __shared__ unsigned long long bar;
-    const int i0 = blockIdx.y * kTileA, j0 = blockIdx.x * kTileA;
+    const int i0 = blk.y() * kTileA, j0 = blk.x() * kTileA;
     const int ny = a.ny, nx = a.nx;
     {
         Box<R>* const dst[TT::NB] = {&T.u, &T.v, &T.eu, &T.ev, &T.H, &T.phi, &T.bed, &T.beta, &T.B, &T.eH};
@@ -256,9 +256,15 @@ __global__ void __launch_bounds__(kTileA * kTileA)
         if (threadIdx.x < 3) {
             double acc = 0;
             for (int q = 0; q < kTileA * kTileA / 32; ++q) acc += red[threadIdx.x][q];
-            a.partial[size_t(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = acc;
+            a.partial[size_t(blk.y() * blk.gx() + blk.x()) * 3 + threadIdx.x] = acc;
         }
     }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kTileA * kTileA)
+    k_jvp(VjpArgs<R> a, int mode, const __grid_constant__ BoxMaps<JvpTile<R>::NB> maps) {
+    jvp_tile<R>(a, mode, maps, SoloBlock{});
 }
 
 }  // namespace glide

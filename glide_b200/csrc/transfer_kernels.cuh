@@ -159,23 +159,55 @@ __global__ void k_correct_batch(CorrectJobs<R> b) {
 // Finest-level snapshot at the top of a V-cycle (multigrid.py:552-556):
 // w = x, chi = thklim - H.
 template <class R>
-__global__ void k_snapshot(Arr<R> u, Arr<R> v, Arr<R> H, Arr<R> wu, Arr<R> wv, Arr<R> wH, Arr<R> chi,
-                           R thklim, int ny, int nx) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (i < ny && j <= nx) wu.at(i, j) = u.at(i, j);
-    if (i <= ny && j < nx) wv.at(i, j) = v.at(i, j);
-    if (i < ny && j < nx) {
-        R h = H.at(i, j);
-        wH.at(i, j) = h;
-        if (chi.p) chi.at(i, j) = thklim - h;
+struct SnapshotArgs {
+    Arr<R> u, v, H, wu, wv, wH, chi;
+    R thklim;
+    int ny, nx;
+};
+
+template <class R>
+__device__ __forceinline__ void snapshot_at(const SnapshotArgs<R>& a, int i, int j) {
+    if (i < a.ny && j <= a.nx) a.wu.at(i, j) = a.u.at(i, j);
+    if (i <= a.ny && j < a.nx) a.wv.at(i, j) = a.v.at(i, j);
+    if (i < a.ny && j < a.nx) {
+        R h = a.H.at(i, j);
+        a.wH.at(i, j) = h;
+        if (a.chi.p) a.chi.at(i, j) = a.thklim - h;
     }
+}
+
+template <class R>
+__global__ void k_snapshot(SnapshotArgs<R> a) {
+    snapshot_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // f = H_prev / dt + smb (glide/operators.py:275-276)
 template <class R>
-__global__ void k_set_rhs(Arr<R> fH, Arr<R> Hp, Arr<R> smb, R dt, int ny, int nx) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (i < ny && j < nx) fH.at(i, j) = Hp.at(i, j) / dt + smb.at(i, j);
+struct SetRhsArgs {
+    Arr<R> fH, Hp, smb;
+    R dt;
+    int ny, nx;
+};
+
+template <class R>
+__device__ __forceinline__ void set_rhs_at(const SetRhsArgs<R>& a, int i, int j) {
+    if (i < a.ny && j < a.nx) a.fH.at(i, j) = a.Hp.at(i, j) / a.dt + a.smb.at(i, j);
+}
+
+template <class R>
+__global__ void k_set_rhs(SetRhsArgs<R> a) {
+    set_rhs_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Copy of one pitched array (the grouped form of a device-to-device copy).
+template <class R>
+struct CopyArgs {
+    Arr<R> dst, src;
+};
+
+template <class R>
+__device__ __forceinline__ void copy_at(const CopyArgs<R>& a, int i, int j) {
+    if (i < a.src.rows && j < a.src.cols) a.dst.at(i, j) = a.src.at(i, j);
 }
 
 // a = s * b + c over a pitched array (c may alias a)
@@ -228,23 +260,54 @@ __global__ void k_defect_update(Arr<D> u, Arr<D> v, Arr<D> H, Arr<D> mask, Arr<D
 // Right-hand side of the Newton correction, -r, in the tangent system's
 // precision; active cells take -(H - gamma) so that H + e_H = gamma.
 template <class T, class R>
-__global__ void k_tangent_rhs(Arr<T> fu, Arr<T> fv, Arr<T> fH, Arr<R> ru, Arr<R> rv, Arr<R> rH, Arr<R> H,
-                              Arr<R> gamma, Arr<R> mask, int ny, int nx) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (i < ny && j <= nx) fu.at(i, j) = T(-ru.at(i, j));
-    if (i <= ny && j < nx) fv.at(i, j) = T(-rv.at(i, j));
-    if (i < ny && j < nx)
-        fH.at(i, j) = T(mask.at(i, j) > R(0.5) ? -(H.at(i, j) - gamma.at(i, j)) : -rH.at(i, j));
+struct TangentRhsArgs {
+    Arr<T> fu, fv, fH;
+    Arr<R> ru, rv, rH, H, gamma, mask;
+    int ny, nx;
+};
+
+template <class T, class R>
+__device__ __forceinline__ void tangent_rhs_at(const TangentRhsArgs<T, R>& a, int i, int j) {
+    if (i < a.ny && j <= a.nx) a.fu.at(i, j) = T(-a.ru.at(i, j));
+    if (i <= a.ny && j < a.nx) a.fv.at(i, j) = T(-a.rv.at(i, j));
+    if (i < a.ny && j < a.nx)
+        a.fH.at(i, j) = T(a.mask.at(i, j) > R(0.5) ? -(a.H.at(i, j) - a.gamma.at(i, j)) : -a.rH.at(i, j));
+}
+
+template <class T, class R>
+__global__ void k_tangent_rhs(TangentRhsArgs<T, R> a) {
+    tangent_rhs_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Newton update x += e (e possibly in lower precision), thickness floored at gamma.
 template <class D, class S>
-__global__ void k_newton_update(Arr<D> u, Arr<D> v, Arr<D> H, Arr<D> gamma, Arr<S> eu, Arr<S> ev, Arr<S> eH,
-                                int ny, int nx) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (i < ny && j <= nx) u.at(i, j) = u.at(i, j) + D(eu.at(i, j));
-    if (i <= ny && j < nx) v.at(i, j) = v.at(i, j) + D(ev.at(i, j));
-    if (i < ny && j < nx) H.at(i, j) = fmax(H.at(i, j) + D(eH.at(i, j)), gamma.at(i, j));
+struct NewtonUpdateArgs {
+    Arr<D> u, v, H, gamma;
+    Arr<S> eu, ev, eH;
+    int ny, nx;
+};
+
+template <class D, class S>
+__device__ __forceinline__ void newton_update_at(const NewtonUpdateArgs<D, S>& a, int i, int j) {
+    if (i < a.ny && j <= a.nx) a.u.at(i, j) = a.u.at(i, j) + D(a.eu.at(i, j));
+    if (i <= a.ny && j < a.nx) a.v.at(i, j) = a.v.at(i, j) + D(a.ev.at(i, j));
+    if (i < a.ny && j < a.nx) a.H.at(i, j) = fmax(a.H.at(i, j) + D(a.eH.at(i, j)), a.gamma.at(i, j));
+}
+
+template <class D, class S>
+__global__ void k_newton_update(NewtonUpdateArgs<D, S> a) {
+    newton_update_at(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+template <class R>
+struct FillArgs {
+    Arr<R> a;
+    R val;
+};
+
+template <class R>
+__device__ __forceinline__ void fill_at(const FillArgs<R>& f, int i, int j) {
+    if (i < f.a.rows && j < f.a.cols) f.a.at(i, j) = f.val;
 }
 
 template <class R>

@@ -13,6 +13,13 @@ timing a step of the class's first member from a warm state: the member is
 first advanced one step, trials run from that state, and the member's
 original state is restored afterwards.
 
+With `grouped=True` the members' cycles run in grouped launches
+(glide_b200.group): one forward solve and one adjoint solve cover the group
+members -- each kind of launch of a cycle issued once for all of them, the
+cycle one CUDA graph, each member's convergence test and Newton decisions on
+the device -- while members above `group_max_cells` solve on the worker
+streams meanwhile.  Members run the same cycles either way.
+
 No counterpart in the reference (its models run one grid at a time); the
 members themselves are the reference-compatible `IceDynamics`.
 """
@@ -25,6 +32,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
+from .group import HierarchyGroup
 from .model import IceDynamics
 
 STATE = ("u", "v", "H", "H_prev", "phi", "mask")
@@ -105,7 +113,8 @@ def apply_schedule(model: IceDynamics, cfg: dict):
 class Ensemble:
     """Concurrent driver of independent members (see the module text)."""
 
-    def __init__(self, members: list[IceDynamics], workers: int | None = None):
+    def __init__(self, members: list[IceDynamics], workers: int | None = None, grouped: bool = False,
+                 group_max_cells: int | None = None):
         self.members = list(members)
         n = len(self.members)
         self.workers = max(1, min(workers or min(n, 16), n))
@@ -118,14 +127,33 @@ class Ensemble:
         self._streams = [None] * self.workers
         self.schedules: dict[int, str] = {}
         self.retries = 0  # forward solves repeated under another schedule
+        # autotune trials per size class: name -> {"ms": warm step, "vcycles", "converged",
+        # "history": the residual norms relative to the first}
+        self.trials: dict[int, dict[str, dict]] = {}
+        self.grouped = grouped
+        # grouped mode: members of at most this many cells join the groups (None: every member)
+        self.group_max_cells = group_max_cells
+        self._fwd_group: HierarchyGroup | None = None
+        self._fwd_keys: tuple[int, ...] = ()
+        self._adj_group: HierarchyGroup | None = None
+        self._adj_keys: tuple[int, ...] = ()
+        self._side = ThreadPoolExecutor(max_workers=1) if grouped else None
+        self._side_stream = None
 
     def close(self):
         self._pool.shutdown(wait=True)
+        if self._side is not None:
+            self._side.shutdown(wait=True)
+        for g in (self._fwd_group, self._adj_group):
+            if g is not None:
+                g.close()
 
-    def _run(self, fn):
-        """fn(k, model) for every member, each worker on its own stream;
-        returns the results in member order."""
+    def _run(self, fn, keys=None, side=None):
+        """fn(k, model) for the members `keys` (every member by default), each
+        worker on its own stream; `side()`, when given, runs meanwhile on a
+        stream of its own.  Returns the results in member order and side's."""
         res = [None] * len(self.members)
+        keys = set(range(len(self.members))) if keys is None else set(keys)
         caller = torch.cuda.current_stream()
         start = torch.cuda.Event()
         start.record(caller)
@@ -137,15 +165,53 @@ class Ensemble:
             s.wait_event(start)
             with torch.cuda.stream(s):
                 for k in self._groups[w]:
-                    res[k] = fn(k, self.members[k])
+                    if k in keys:
+                        res[k] = fn(k, self.members[k])
             done = torch.cuda.Event()
             done.record(s)
             return done
 
+        def side_job():
+            if self._side_stream is None:
+                self._side_stream = torch.cuda.Stream()
+            s = self._side_stream
+            s.wait_event(start)
+            with torch.cuda.stream(s):
+                out = side()
+            done = torch.cuda.Event()
+            done.record(s)
+            return out, done
+
+        fut = self._side.submit(side_job) if side is not None else None
         events = list(self._pool.map(work, range(self.workers)))
+        side_out = None
+        if fut is not None:
+            side_out, e = fut.result()
+            events.append(e)
         for e in events:
             caller.wait_event(e)
-        return res
+        return res, side_out
+
+    def _in_groups(self, k: int) -> bool:
+        """Member k joins the grouped solves: binary64 or binary32, solved
+        from its top level, within the size limit."""
+        m = self.members[k]
+        ny, nx, _ = m.mg.hierarchy.shapes[0]
+        return (m.mg.hierarchy.precision != "mixed" and m.top_level == 0
+                and (self.group_max_cells is None or ny * nx <= self.group_max_cells))
+
+    def _groupable(self, k: int) -> bool:
+        """Member k's forward solve runs in the grouped solve: a group member
+        with a schedule (FASCD or guarded Newton)."""
+        return self._in_groups(k) and self.schedules.get(k) in CANDIDATES
+
+    def _forward_group(self, keys: tuple[int, ...]) -> HierarchyGroup:
+        if self._fwd_group is None or self._fwd_keys != keys:
+            if self._fwd_group is not None:
+                self._fwd_group.close()
+            self._fwd_group = HierarchyGroup([self.members[k].mg.hierarchy for k in keys])
+            self._fwd_keys = keys
+        return self._fwd_group
 
     def forward(self, t: float, dt: float, update_geometry: bool = True, retry: bool = True):
         """One forward step of every member.  With `retry`, a member whose
@@ -156,8 +222,11 @@ class Ensemble:
         there becomes that member's schedule.  The returned statistics span
         all attempts.  The geometry update and post-forward hooks run once,
         after the last solve."""
-        def one(k, m):
-            st = m.forward_solver.solve(dt, start_level=m.top_level, report_norms=False)
+        def one(k, m, st=None):
+            if st is None:
+                st = m.forward_solver.solve(dt, start_level=m.top_level, report_norms=False)
+            else:  # the grouped solve's result, recorded as the member's own solve records it
+                m.forward_solver.dt, m.forward_solver.last_stats = float(dt), st
             if retry and not _converged(m, st):
                 c = m.forward_solver._fas_config
                 rtol, atol = c.relative_tolerance, c.absolute_tolerance
@@ -188,14 +257,52 @@ class Ensemble:
             for hook in m._post_forward_hooks:
                 hook(t + dt)
             return st
-        return self._run(one)
+        if not self.grouped:
+            return self._run(one)[0]
+        n = len(self.members)
+        gk = tuple(k for k in range(n) if self._groupable(k))
+        solo = [k for k in range(n) if k not in gk]
+        if not gk:
+            return self._run(one)[0]
+        group = self._forward_group(gk)
+        res, gst = self._run(one, keys=solo, side=lambda: group.forward(dt))
+        # retries, geometry update and hooks of the grouped members, on the workers
+        first = dict(zip(gk, gst))
+        done, _ = self._run(lambda k, m: one(k, m, first[k]), keys=gk)
+        for k in gk:
+            res[k] = done[k]
+        return res
 
     def backward(self, t: float, dt: float, dJ):
-        """dJ(k, model) -> (dJdu, dJdv, dJdH) per member; returns the adjoint stats."""
+        """dJ(k, model) -> (dJdu, dJdv, dJdH) per member; returns the adjoint
+        stats.  Grouped: the group members' adjoint solves in one grouped
+        solve, the others on the worker streams meanwhile."""
         def one(k, m):
             du, dv, dH = dJ(k, m)
             return m.backward(t, dt, dJdu=du, dJdv=dv, dJdH=dH)
-        return self._run(one)
+        gk = tuple(k for k in range(len(self.members)) if self.grouped and self._in_groups(k))
+        if not gk:
+            return self._run(one)[0]
+        masks = set()
+        for k in gk:
+            m = self.members[k]
+            du, dv, dH = dJ(k, m)
+            masks.add(m.prepare_backward(dJdu=du, dJdv=dv, dJdH=dH))
+        if len(masks) != 1:
+            raise ValueError("grouped adjoint solves need one gradient mask for every member")
+        mask = masks.pop()
+        if self._adj_group is None or self._adj_keys != gk:
+            if self._adj_group is not None:
+                self._adj_group.close()
+            self._adj_group = HierarchyGroup([self.members[k].mg.hierarchy for k in gk])
+            self._adj_keys = gk
+        group = self._adj_group
+        solo = [k for k in range(len(self.members)) if k not in gk]
+        res, gst = self._run(one, keys=solo, side=lambda: group.backward(dt, mask=mask))
+        for k, s in zip(gk, gst):
+            self.members[k].adjoint_solver.dt, self.members[k].adjoint_solver.last_stats = float(dt), s
+            res[k] = s
+        return res
 
     def autotune(self, dt: float, candidates: dict | None = None, warm: bool = True) -> dict[int, str]:
         """Per size class: time one forward step of the class's first member
@@ -238,6 +345,10 @@ class Ensemble:
                     el = time.perf_counter() - t0
                 ok = st["final_norm"] <= max(h.get_fas(False)["relative_tolerance"] * st["initial_norm"],
                                              h.get_fas(False)["absolute_tolerance"])
+                h0 = st["history"][0] if st["history"] and st["history"][0] > 0 else 1.0
+                self.trials.setdefault(n, {})[name] = {
+                    "ms": el * 1e3, "vcycles": int(st["vcycles"]), "converged": bool(ok),
+                    "history": [float(f"{x / h0:.2e}") for x in st["history"][:12]]}
                 if ok and el < best_t:
                     best, best_t = name, el
             best = best or FALLBACK

@@ -68,6 +68,16 @@ class IceDynamics:
         which solve ran before it.  Reference mode keeps that; native mode
         (reference_quirks=False) starts every solve from lambda = 0, which
         makes each gradient a function of this step's inputs alone."""
+        mask = self.prepare_backward(dJdu, dJdv, dJdH, compute_beta_grad, compute_bed_grad, compute_H_prev_grad,
+                                     compute_smb_grad)
+        return self.adjoint_solver.solve(dt, start_level=self.top_level, grad_mask=mask)
+
+    def prepare_backward(self, dJdu=None, dJdv=None, dJdH=None, compute_beta_grad=True, compute_bed_grad=True,
+                         compute_H_prev_grad=True, compute_smb_grad=True) -> int:
+        """The adjoint solve's inputs as `backward` sets them (right-hand side
+        -dJ/dx, lambda = 0 in native mode); returns the gradient mask.  For
+        grouped solves (glide_b200.group), which then solve many members at
+        once."""
         h = self.mg.hierarchy
         top = self.top_level
         if not getattr(h, "reference_quirks", True):
@@ -78,9 +88,8 @@ class IceDynamics:
                 h.set(name, top, 0.0)
             else:
                 h.set(name, top, -torch.as_tensor(g, device="cuda", dtype=h.dtype))
-        mask = ((_lib.GRAD_BETA if compute_beta_grad else 0) | (_lib.GRAD_BED if compute_bed_grad else 0) |
+        return ((_lib.GRAD_BETA if compute_beta_grad else 0) | (_lib.GRAD_BED if compute_bed_grad else 0) |
                 (_lib.GRAD_H_PREV if compute_H_prev_grad else 0) | (_lib.GRAD_SMB if compute_smb_grad else 0))
-        return self.adjoint_solver.solve(dt, start_level=top, grad_mask=mask)
 
 
 class ThermalModel:

@@ -298,6 +298,41 @@ const char* glide_noalloc_last_error(void);
 int glide_transfer(int op, int dtype, int ny_fine, int nx_fine, const void* src, int ld_src, void* dst, int ld_dst,
                    void* stream);
 
+/* Groups: one solve of many handles in grouped launches.  No counterpart in
+ * the reference, whose models solve one grid at a time (IceDynamics.forward /
+ * backward, glide/model.py:62-94); each member is an ordinary handle and
+ * keeps that API.  A group solve runs every member's cycle -- the same
+ * launches, in the same order, with the same arguments as glide_forward /
+ * glide_backward on that member -- but issues each kind of launch once for
+ * all members: blocks map to (member, tile) through a table in the launch's
+ * parameters.  The cycle of all members is one CUDA graph, and each member's
+ * convergence test (its own tolerances and cycle cap) runs on the device, so
+ * a converged member's launches are skipped from the next cycle on.  Results
+ * equal the members' own solves.
+ *
+ * Members: handles of one dtype, GLIDE_F64 or GLIDE_F32 (mixed-precision
+ * handles: GLIDE_ERR_STATE), each at most once; they must outlive the group
+ * and must not be used from another thread while a group call runs.  Each
+ * member solves with its own schedule, tolerances and forward method: the
+ * guarded Newton steps' decisions (when to step, undoing a step whose
+ * residual grew, falling back to FASCD) are taken on the device as
+ * glide_forward takes them on the host.  stats: n entries, one per member
+ * (may be NULL).  A
+ * member whose residual becomes non-finite returns GLIDE_ERR_NONFINITE after
+ * the others finish.  Plans (the merged launch lists and their graphs) are
+ * rebuilt when dt, start_level, grad_mask or any member's configuration
+ * changes. */
+typedef struct glide_group_s* glide_group;
+int glide_group_create(const glide_handle* members, int n, glide_group* out);
+int glide_group_destroy(glide_group g);
+int glide_group_forward(glide_group g, double dt, int start_level, glide_stats* stats, void* stream);
+int glide_group_backward(glide_group g, double dt, int start_level, int grad_mask, glide_stats* stats,
+                         void* stream);
+/* launches: grouped launches issued so far.  shape (4 ints, may be NULL): the
+ * last forward cycle's grouped launches and the members' launches they
+ * carry, then the same for the adjoint cycle. */
+int glide_group_counters(glide_group g, long long* launches, int* shape);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,3 +97,48 @@ def test_forward_retries_other_schedules_when_a_solve_stops_short():
     assert np.isfinite(st["final_norm"])
     H = m.mg.hierarchy.get("H", 0)
     assert bool(torch.equal(m.mg.hierarchy.get("H_prev", 0), H))
+
+
+@pytest.mark.gpu
+def test_grouped_ensemble_matches_solo_runs():
+    """Grouped mode: the members of at most 96^2 cells solve in one grouped
+    forward solve (FASCD and guarded Newton schedules) and one grouped
+    adjoint solve while the 128^2 member solves on a worker stream; each
+    member runs the cycles of its own solo solves and its fields agree with
+    them to rounding (the grouped kernels are separate compilations of the
+    same tile bodies)."""
+    from util import rel_err
+    from glide_b200.ensemble import CANDIDATES, Ensemble, apply_schedule
+    sizes = [64, 96, 128, 64, 96]
+    names = ["fast", "classic", "fast", "fascd/1", "newton/classic"]
+
+    def build():
+        members = [_member(n, seed=40 + k) for k, n in enumerate(sizes)]
+        for m, name in zip(members, names):
+            apply_schedule(m, CANDIDATES[name])
+            m.forward_solver.fas_options.set(maximum_vcycles=30, relative_tolerance=1e-8)
+            m.adjoint_solver.fas_options.set(maximum_vcycles=30, relative_tolerance=1e-8)
+        return members
+
+    dJ = lambda k, m: (0.05 * m.mg.levels[0].state.u.data, 0.05 * m.mg.levels[0].state.v.data, None)
+    a, b = build(), build()
+    ens = Ensemble(a, workers=2, grouped=True, group_max_cells=96 * 96)
+    for k, name in enumerate(names):
+        ens.schedules[k] = name
+    fa = [ens.forward(step * 10.0, 10.0, retry=False) for step in range(2)]
+    ba = ens.backward(20.0, 10.0, dJ)
+    torch.cuda.synchronize()
+    assert ens._fwd_keys == (0, 1, 3, 4) and ens._adj_keys == (0, 1, 3, 4)
+    ens.close()
+    fb = [[m.forward(step * 10.0, 10.0) for m in b] for step in range(2)]
+    bb = []
+    for k, m in enumerate(b):
+        du, dv, _ = dJ(k, m)
+        bb.append(m.backward(20.0, 10.0, dJdu=du, dJdv=dv))
+    torch.cuda.synchronize()
+    assert [[s["vcycles"] for s in f] for f in fa] == [[s["vcycles"] for s in f] for f in fb]
+    assert [s["vcycles"] for s in ba] == [s["vcycles"] for s in bb]
+    for ma, mb in zip(a, b):
+        for k in ("u", "v", "H", "H_prev", "lambda_u", "lambda_H", "grad_beta", "grad_bed"):
+            x, y = ma.mg.hierarchy.get(k, 0).cpu().numpy(), mb.mg.hierarchy.get(k, 0).cpu().numpy()
+            assert rel_err(x, y) <= 1e-10, (k, rel_err(x, y))
