@@ -90,6 +90,12 @@ def parse(argv=None):
                     help="ensemble: every member solves on its own (no grouped launches)")
     ap.add_argument("--ens-group-max-n", type=int, default=0,
                     help="ensemble: only members of at most n x n cells join the grouped solves (0: all)")
+    ap.add_argument("--ens-group-size", type=int, default=0,
+                    help="ensemble: at most this many members per group (0: no limit)")
+    ap.add_argument("--ens-sizes", default="128,192,256,384,512,768",
+                    help="ensemble: grid sizes the members are drawn from")
+    ap.add_argument("--ens-group-by", default="class", choices=["class", "all"],
+                    help="ensemble: one group per grid size (each on its own stream) or one group")
     ap.add_argument("--ens-adjoint", default="fast", choices=["fast", "reference"],
                     help="ensemble adjoint: 4/4/0/50 cycles with omega 0.8, or the reference's 10/20/50/200")
     ap.add_argument("--enth-point-blocks", type=int, default=None, help="enthalpy residual/layer blocks per SM")
@@ -750,7 +756,8 @@ def run_ensemble(a):
     from cases import dome
     from glide_b200.ensemble import Ensemble, member_specs
     from glide_b200.model import IceDynamics
-    specs = member_specs(a.members, seed=0)
+    sizes = tuple(int(x) for x in a.ens_sizes.split(","))
+    specs = member_specs(a.members, seed=0, sizes=sizes)
     max_cycles = max(a.max_vcycles, 100)  # small steep domes need up to ~60 classic cycles
     members = []
     for sp in specs:
@@ -771,7 +778,8 @@ def run_ensemble(a):
             m.adjoint_solver.vanka_options.set(omega=0.8)
         members.append(m)
     ens = Ensemble(members, workers=a.ens_workers, grouped=not a.ens_solo,
-                   group_max_cells=a.ens_group_max_n ** 2 if a.ens_group_max_n else None)
+                   group_max_cells=a.ens_group_max_n ** 2 if a.ens_group_max_n else None,
+                   group_by=a.ens_group_by, group_size=a.ens_group_size or None)
     t0 = time.perf_counter()
     chosen = ens.autotune(a.dt, warm=not a.ens_cold_tune)
     tune_s = time.perf_counter() - t0
@@ -788,9 +796,10 @@ def run_ensemble(a):
     ms = event_time(lambda: stats.append(step(0.0)), a.ens_steps, stream)
     group_cycles = None
     if ens.grouped:
-        group_cycles = {"forward": ens._fwd_group.counters()["forward_cycle"] if ens._fwd_group else None,
-                        "adjoint": ens._adj_group.counters()["adjoint_cycle"] if ens._adj_group else None,
-                        "what": "grouped launches of one cycle, and the members' launches they carry"}
+        size = lambda keys: f"{specs[keys[0]].n}x{len(keys)}@{keys[0]}"
+        group_cycles = {"forward": {size(k): g.counters()["forward_cycle"] for k, g in ens.groups("fwd")},
+                        "adjoint": {size(k): g.counters()["adjoint_cycle"] for k, g in ens.groups("adj")},
+                        "what": "per group: grouped launches of one cycle, and the members' launches they carry"}
     ens.close()
     cells = sum(sp.n * sp.n for sp in specs)
     # the members' forward steps one after another, each at its class's tuned warm-step time
@@ -813,6 +822,8 @@ def run_ensemble(a):
             "grouped_forward_members": len(ens._fwd_keys),
             "grouped_adjoint_members": len(ens._adj_keys),
             "group_max_n": a.ens_group_max_n or None,
+            "group_by": a.ens_group_by,
+            "group_size": a.ens_group_size or None,
             "group_cycles": group_cycles,
             "autotune_trials": {str(n): {k: dict(v, ms=round(v["ms"], 2)) for k, v in t.items()}
                                 for n, t in ens.trials.items()},

@@ -330,7 +330,7 @@ enum GroupFlag {
     kGroupUndo = 16,   // the Newton step is undone
 };
 enum GroupStatus { GS_RUNNING = 0, GS_DONE = 1, GS_NONFINITE = 2 };
-enum GroupPhase { GC_INIT = 0, GC_PRE = 1, GC_MID = 2, GC_POST = 3, GC_END = 4 };
+enum GroupPhase { GC_INIT = 0, GC_MID = 1, GC_POST = 2, GC_END = 3 };
 
 struct GroupMember {
     const double* norms;  // the member's norm vector |r_u|, |r_v|, |r_H|, |r|
@@ -348,13 +348,23 @@ struct GroupMember {
 
 constexpr int kGroupControlThreads = 1024;
 
-// One phase of the decisions for every member (one thread each).  Members
-// that stopped are left alone.  running[0] receives the number of members
-// still running after GC_INIT and GC_END.
+// The next cycle of a running member: a Newton step or a FASCD cycle, with
+// the Newton prologue when the previous cycle was not a Newton step.
+__device__ __forceinline__ int group_decide(GroupMember& g) {
+    const bool newton_phase = g.newton && g.rel <= g.newton_switch;
+    const bool step = newton_phase && !g.newton_off && g.rel <= g.gate;
+    if (!step) g.in_newton = 0;
+    return kGroupRun | (step ? kGroupNewton : kGroupFas) | (step && !g.in_newton ? kGroupPro : 0);
+}
+
+// One phase of the decisions for every member (one thread each); GC_INIT and
+// GC_END also decide every running member's next cycle.  Members that stopped
+// are left alone.  After GC_INIT and GC_END, out[0] is the number of members
+// still running and out[1] the union of their next cycle's section bits.
 __global__ void __launch_bounds__(kGroupControlThreads)
-    k_group_control(GroupMember* m, int* flags, int n, int phase, int* running) {
-    __shared__ int count;
-    if (threadIdx.x == 0) count = 0;
+    k_group_control(GroupMember* m, int* flags, int n, int phase, int* out) {
+    __shared__ int count, sections;
+    if (threadIdx.x == 0) count = sections = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         GroupMember& g = m[k];
@@ -374,15 +384,10 @@ __global__ void __launch_bounds__(kGroupControlThreads)
             } else {
                 const bool run = g.rel > g.rtol && ab > g.atol && g.max_cycles > 0;
                 g.status = run ? GS_RUNNING : GS_DONE;
-                f = run ? kGroupRun : 0;
+                f = run ? group_decide(g) : 0;
             }
         } else if (!(f & kGroupRun)) {
             continue;
-        } else if (phase == GC_PRE) {
-            const bool newton_phase = g.newton && g.rel <= g.newton_switch;
-            const bool step = newton_phase && !g.newton_off && g.rel <= g.gate;
-            f = kGroupRun | (step ? kGroupNewton : kGroupFas) | (step && !g.in_newton ? kGroupPro : 0);
-            if (!step) g.in_newton = 0;
         } else if (phase == GC_MID) {
             if (f & kGroupPro) {
                 g.prev = g.norms[3];
@@ -419,13 +424,19 @@ __global__ void __launch_bounds__(kGroupControlThreads)
             if (g.cycles < kGroupHistory) g.history[g.cycles] = ab;
             const bool run = g.rel > g.rtol && ab > g.atol && g.cycles < g.max_cycles;
             g.status = run ? GS_RUNNING : GS_DONE;
-            f = run ? kGroupRun : 0;
+            f = run ? group_decide(g) : 0;
         }
         flags[k] = f;
-        if (f & kGroupRun) atomicAdd(&count, 1);
+        if (f & kGroupRun) {
+            atomicAdd(&count, 1);
+            atomicOr(&sections, f);
+        }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && (phase == GC_INIT || phase == GC_END)) *running = count;
+    if (threadIdx.x == 0 && (phase == GC_INIT || phase == GC_END)) {
+        out[0] = count;
+        out[1] = sections;
+    }
 }
 
 }  // namespace glide

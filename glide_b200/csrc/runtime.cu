@@ -1264,8 +1264,8 @@ template <class R>
 struct GroupRun : GroupBase {
     std::vector<Solver<R>*> members;
     GroupMember* dev = nullptr;   // device solve state, one per member
-    int* flags = nullptr;         // device run flags; flags[n] counts the running members
-    int* running_host = nullptr;  // pinned copy of that count
+    int* flags = nullptr;         // device run flags; flags[n], flags[n + 1]: running members, their sections
+    int* running_host = nullptr;  // pinned copy of those two words
     std::vector<GroupMember> host;
     cudaStream_t own_stream = nullptr;
 
@@ -1279,7 +1279,11 @@ struct GroupRun : GroupBase {
         int control;  // a GroupPhase, or -1
         int when;     // flag bits of the members whose launches run (0: every member)
         std::function<void(Solver<R>&, int)> body;  // records member k's launches
+        int tag = -1;  // byte accounting: one of the T_* kinds below
     };
+    // forward cycle sections whose algorithmic bytes are accounted per use
+    enum { T_PRO, T_BACKUP, T_FAS, T_NEWTON, T_UNDO, T_COUNT };
+    std::vector<double> sec_bytes[T_COUNT];  // per member, one pass
     struct Plan {
         std::vector<int> control;                      // per section
         std::vector<std::vector<std::vector<RecOp>>> rec;  // [section][member]
@@ -1292,24 +1296,28 @@ struct GroupRun : GroupBase {
         int start = -1, extra = 0;
         bool valid = false;
     };
-    enum { P_FWD_PRO, P_FWD_CYCLE, P_ADJ_PRO, P_ADJ_CYCLE, P_GRAD, P_COUNT };
+    enum { P_FWD_PRO, P_ADJ_PRO, P_ADJ_CYCLE, P_GRAD, P_COUNT };
     Plan plans[P_COUNT];
-    // the forward cycle's sections, in order (byte accounting reads them)
-    enum { S_PRE, S_PRO, S_MID, S_BACKUP, S_FAS, S_NEWTON, S_POST, S_UNDO, S_END };
+    // forward cycles by the sections they hold (bits: FASCD, Newton, prologue):
+    // each cycle replays the variant holding just what the running members need
+    Plan fwd_cycles[8];
 
     explicit GroupRun(std::vector<Solver<R>*> m) : members(std::move(m)) {
         dtype = sizeof(R) == 8 ? GLIDE_F64 : GLIDE_F32;
         const int n = int(members.size());
         host.resize(n);
         GCU(cudaMalloc(&dev, sizeof(GroupMember) * n));
-        GCU(cudaMalloc(&flags, sizeof(int) * (n + 1)));
-        GCU(cudaMemset(flags, 0, sizeof(int) * (n + 1)));
-        GCU(cudaMallocHost(&running_host, sizeof(int)));
+        GCU(cudaMalloc(&flags, sizeof(int) * (n + 2)));
+        GCU(cudaMemset(flags, 0, sizeof(int) * (n + 2)));
+        GCU(cudaMallocHost(&running_host, 2 * sizeof(int)));
+        for (auto& b : sec_bytes) b.assign(n, 0.0);
         GCU(cudaDeviceSynchronize());
     }
 
     ~GroupRun() override {
         for (Plan& p : plans)
+            if (p.exec) cudaGraphExecDestroy(p.exec);
+        for (Plan& p : fwd_cycles)
             if (p.exec) cudaGraphExecDestroy(p.exec);
         if (own_stream) cudaStreamDestroy(own_stream);
         if (running_host) cudaFreeHost(running_host);
@@ -1350,6 +1358,7 @@ struct GroupRun : GroupBase {
                 }
                 m.rec = nullptr;
                 for (const RecOp& r : P.rec[q][k]) P.bytes[q][k] += r.bytes;
+                if (secs[q].tag >= 0) sec_bytes[secs[q].tag][k] = P.bytes[q][k];
             }
             std::vector<size_t> pos(n, 0);
             for (;;) {
@@ -1462,7 +1471,8 @@ struct GroupRun : GroupBase {
             try {
                 for (size_t q = 0; q < P.control.size(); ++q) {
                     if (P.control[q] >= 0) {
-                        k_group_control<<<1, kGroupControlThreads, 0, s>>>(dev, flags, n, P.control[q], flags + n);
+                        k_group_control<<<1, kGroupControlThreads, 0, s>>>(dev, flags, n, P.control[q],
+                                                                            flags + n);
                         check_launch("group_control");
                         ++nodes;
                     } else {
@@ -1501,14 +1511,15 @@ struct GroupRun : GroupBase {
         }
     }
 
-    static Section launches_of(int when, std::function<void(Solver<R>&, int)> body) {
-        return Section{-1, when, std::move(body)};
+    static Section launches_of(int when, std::function<void(Solver<R>&, int)> body, int tag = -1) {
+        return Section{-1, when, std::move(body), tag};
     }
     static Section control(int phase) { return Section{phase, 0, nullptr}; }
 
-    // the prologue plan, then cycles until no member runs; returns the
-    // members' final device state in `host`
-    void solve(Plan& pro, Plan& cyc, int cfg, bool forward, cudaStream_t s) {
+    // the prologue plan, then cycles -- cycle(sections) picks the plan for the
+    // section bits the running members need -- until no member runs; the
+    // members' final device state is left in `host`
+    void solve(Plan& pro, const std::function<Plan&(int)>& cycle, int cfg, bool forward, cudaStream_t s) {
         const int n = int(members.size());
         int max_cycles = 0;
         for (int k = 0; k < n; ++k) {
@@ -1528,10 +1539,10 @@ struct GroupRun : GroupBase {
         GCU(cudaMemcpyAsync(dev, host.data(), sizeof(GroupMember) * n, cudaMemcpyHostToDevice, s));
         run_plan(pro, s);  // ends with the GC_INIT phase
         for (int it = 0;; ++it) {
-            GCU(cudaMemcpyAsync(running_host, flags + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+            GCU(cudaMemcpyAsync(running_host, flags + n, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
             GCU(cudaStreamSynchronize(s));
-            if (*running_host == 0 || it >= max_cycles) break;
-            run_plan(cyc, s);  // ends with the GC_END phase
+            if (running_host[0] == 0 || it >= max_cycles) break;
+            run_plan(cycle(running_host[1]), s);  // ends with the GC_END phase
         }
         GCU(cudaMemcpyAsync(host.data(), dev, sizeof(GroupMember) * n, cudaMemcpyDeviceToHost, s));
         GCU(cudaStreamSynchronize(s));
@@ -1580,12 +1591,8 @@ struct GroupRun : GroupBase {
     void forward(double dt, int start, glide_stats* st, cudaStream_t s) override {
         s = stream_for(s);
         check_members(start);
-        bool any_newton = false;
         for (auto* m : members)
-            if (m->forward_method == 1) {
-                m->ensure_blocks();
-                any_newton = true;
-            }
+            if (m->forward_method == 1) m->ensure_blocks();
         auto is_newton = [&](int k) { return members[k]->forward_method == 1; };
         build(plans[P_FWD_PRO], dt, start, 0,
               {launches_of(0, [&](Solver<R>& m, int) {
@@ -1594,10 +1601,6 @@ struct GroupRun : GroupBase {
                               s);
                }),
                control(GC_INIT)});
-        auto fas = [&](Solver<R>& m, int) {
-            m.vcycle(start, true, dt, s);
-            m.residual(start, dt, true, true, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
-        };
         auto save = [&](Solver<R>& m, int k, bool undo) {
             if (!is_newton(k)) return;
             Level<R>& L0 = m.lv[start];
@@ -1607,36 +1610,49 @@ struct GroupRun : GroupBase {
                 else m.copy(L0.a[b[q]], L0.a[x[q]], s);
             }
         };
-        std::vector<Section> cycle;
-        if (any_newton) {
-            // the per-hierarchy solve loop's sequence for the Newton method
-            cycle = {control(GC_PRE),
-                     launches_of(kGroupPro, [&](Solver<R>& m, int k) {
-                         if (is_newton(k)) m.newton_prologue(start, dt, true, s);
-                     }),
-                     control(GC_MID),
-                     launches_of(kGroupNewton, [&](Solver<R>& m, int k) { save(m, k, false); }),
-                     launches_of(kGroupFas, fas),
-                     launches_of(kGroupNewton, [&](Solver<R>& m, int k) {
-                         if (is_newton(k)) m.newton_cycle(start, dt, s);
-                     }),
-                     control(GC_POST),
-                     launches_of(kGroupUndo, [&](Solver<R>& m, int k) { save(m, k, true); }),
-                     control(GC_END)};
-        } else {
-            cycle = {launches_of(kGroupRun, fas), control(GC_END)};
-        }
-        Plan& C = plans[P_FWD_CYCLE];
-        build(C, dt, start, any_newton ? 1 : 0, cycle);
-        note_shape(C, 0);
-        solve(plans[P_FWD_PRO], C, 0, true, s);
+        // The per-hierarchy solve loop's sequence: the Newton prologue, the
+        // state saved, a FASCD cycle or a Newton step, the step undone if its
+        // residual grew, the convergence test and the next cycle's decision.
+        int used[8] = {0};
+        auto cycle = [&](int bits) -> Plan& {
+            const int fas = bits & kGroupFas, newton = bits & kGroupNewton, pro = bits & kGroupPro;
+            const int v = (fas ? 1 : 0) | (newton ? 2 : 0) | (pro ? 4 : 0);
+            std::vector<Section> secs;
+            if (pro) {
+                secs.push_back(launches_of(kGroupPro, [&](Solver<R>& m, int k) {
+                    if (is_newton(k)) m.newton_prologue(start, dt, true, s);
+                }, T_PRO));
+                secs.push_back(control(GC_MID));
+            }
+            if (newton) secs.push_back(launches_of(kGroupNewton, [&](Solver<R>& m, int k) { save(m, k, false); }, T_BACKUP));
+            if (fas)
+                secs.push_back(launches_of(kGroupFas, [&](Solver<R>& m, int) {
+                    m.vcycle(start, true, dt, s);
+                    m.residual(start, dt, true, true, false, true, GLIDE_R_U, GLIDE_R_V, GLIDE_R_H, nullptr, true, s);
+                }, T_FAS));
+            if (newton) {
+                secs.push_back(launches_of(kGroupNewton, [&](Solver<R>& m, int k) {
+                    if (is_newton(k)) m.newton_cycle(start, dt, s);
+                }, T_NEWTON));
+                secs.push_back(control(GC_POST));
+                secs.push_back(launches_of(kGroupUndo, [&](Solver<R>& m, int k) { save(m, k, true); }, T_UNDO));
+            }
+            secs.push_back(control(GC_END));
+            build(fwd_cycles[v], dt, start, 0, secs);
+            ++used[v];
+            return fwd_cycles[v];
+        };
+        solve(plans[P_FWD_PRO], cycle, 0, true, s);
+        int most = 0;
+        for (int v = 1; v < 8; ++v)
+            if (used[v] > used[most]) most = v;
+        if (used[most]) note_shape(fwd_cycles[most], 0);
         finish(plans[P_FWD_PRO], 0, st, [&](int k) {
-            const GroupMember& g = host[k];
-            if (!any_newton) return g.cycles * C.bytes[0][k];
             // FASCD cycles, Newton steps (state saved), prologues and undone steps
+            const GroupMember& g = host[k];
             const int steps = g.cycles - g.fas_cycles;
-            return g.fas_cycles * C.bytes[S_FAS][k] + steps * (C.bytes[S_BACKUP][k] + C.bytes[S_NEWTON][k]) +
-                   g.prologues * C.bytes[S_PRO][k] + g.rejects * C.bytes[S_UNDO][k];
+            return g.fas_cycles * sec_bytes[T_FAS][k] + steps * (sec_bytes[T_BACKUP][k] + sec_bytes[T_NEWTON][k]) +
+                   g.prologues * sec_bytes[T_PRO][k] + g.rejects * sec_bytes[T_UNDO][k];
         });
     }
 
@@ -1657,7 +1673,7 @@ struct GroupRun : GroupBase {
         build(plans[P_GRAD], dt, start, grad_mask,
               {launches_of(0, [&](Solver<R>& m, int) { m.gradients(start, dt, grad_mask, s); })});
         note_shape(C, 2);
-        solve(plans[P_ADJ_PRO], C, 1, false, s);
+        solve(plans[P_ADJ_PRO], [&](int) -> Plan& { return C; }, 1, false, s);
         run_plan(plans[P_GRAD], s);
         finish(plans[P_ADJ_PRO], 1, st, [&](int k) { return host[k].cycles * C.bytes[0][k] + plans[P_GRAD].bytes[0][k]; });
     }

@@ -38,6 +38,33 @@ from .model import IceDynamics
 STATE = ("u", "v", "H", "H_prev", "phi", "mask")
 
 
+class _Streams:
+    """CUDA streams of the ensemble's own, one per host worker and grouped
+    job.  torch.cuda.Stream() hands out streams round-robin from a fixed pool
+    (32 per priority), so many workers would share some -- and a stream that
+    one thread drives while another captures a graph on it breaks the
+    capture.  Created non-blocking, destroyed by close()."""
+
+    def __init__(self):
+        self._raw = []
+
+    def new(self) -> torch.cuda.Stream:
+        from cuda.bindings import runtime as rt
+        err, s = rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking)
+        if err != rt.cudaError_t.cudaSuccess:
+            raise RuntimeError(f"cudaStreamCreateWithFlags: {err}")
+        self._raw.append(s)
+        return torch.cuda.ExternalStream(int(s))
+
+    def close(self):
+        from cuda.bindings import runtime as rt
+        if self._raw:
+            torch.cuda.synchronize()
+        for s in self._raw:
+            rt.cudaStreamDestroy(s)
+        self._raw = []
+
+
 def levels_for(n: int, min_coarse: int = 16, max_levels: int = 8) -> int:
     """Most levels such that n halves exactly down to a coarsest grid of at
     least `min_coarse` cells."""
@@ -114,7 +141,7 @@ class Ensemble:
     """Concurrent driver of independent members (see the module text)."""
 
     def __init__(self, members: list[IceDynamics], workers: int | None = None, grouped: bool = False,
-                 group_max_cells: int | None = None):
+                 group_max_cells: int | None = None, group_by: str = "class", group_size: int | None = None):
         self.members = list(members)
         n = len(self.members)
         self.workers = max(1, min(workers or min(n, 16), n))
@@ -124,6 +151,7 @@ class Ensemble:
         for r, k in enumerate(order):
             self._groups[r % self.workers].append(k)
         self._pool = ThreadPoolExecutor(max_workers=self.workers)
+        self._own = _Streams()
         self._streams = [None] * self.workers
         self.schedules: dict[int, str] = {}
         self.retries = 0  # forward solves repeated under another schedule
@@ -131,27 +159,65 @@ class Ensemble:
         # "history": the residual norms relative to the first}
         self.trials: dict[int, dict[str, dict]] = {}
         self.grouped = grouped
-        # grouped mode: members of at most this many cells join the groups (None: every member)
+        # grouped mode: members of at most this many cells join the groups (None: every member);
+        # group_by "class": one group per grid size, each on its own stream; "all": one group
         self.group_max_cells = group_max_cells
-        self._fwd_group: HierarchyGroup | None = None
+        if group_by not in ("class", "all"):
+            raise ValueError("group_by must be 'class' or 'all'")
+        self.group_by = group_by
+        self.group_size = group_size  # at most this many members per group (None: no limit)
+        self._groups_of: dict[tuple[str, tuple[int, ...]], HierarchyGroup] = {}
         self._fwd_keys: tuple[int, ...] = ()
-        self._adj_group: HierarchyGroup | None = None
         self._adj_keys: tuple[int, ...] = ()
-        self._side = ThreadPoolExecutor(max_workers=1) if grouped else None
-        self._side_stream = None
+        self._side = ThreadPoolExecutor(max_workers=max(self.workers, 8)) if grouped else None
+        self._side_streams: list = []
+        self._parts_now: list[tuple[int, ...]] = []
 
     def close(self):
         self._pool.shutdown(wait=True)
         if self._side is not None:
             self._side.shutdown(wait=True)
-        for g in (self._fwd_group, self._adj_group):
-            if g is not None:
-                g.close()
+        for g in self._groups_of.values():
+            g.close()
+        self._groups_of = {}
+        self._own.close()
 
-    def _run(self, fn, keys=None, side=None):
+    def groups(self, kind: str) -> list[tuple[tuple[int, ...], HierarchyGroup]]:
+        """The current groups of the forward ("fwd") or adjoint ("adj") solves
+        and their members."""
+        return [(keys, g) for (kd, keys), g in self._groups_of.items() if kd == kind]
+
+    def _parts(self, keys: tuple[int, ...]) -> list[tuple[int, ...]]:
+        if self.group_by == "all":
+            parts = [list(keys)] if keys else []
+        else:
+            by: dict[int, list[int]] = {}
+            for k in keys:
+                by.setdefault(self.members[k].mg.hierarchy.shapes[0][0], []).append(k)
+            parts = [v for _, v in sorted(by.items())]
+        q = self.group_size or max(len(keys), 1)
+        return [tuple(p[i:i + q]) for p in parts for i in range(0, len(p), q)]
+
+    def _group(self, kind: str, keys: tuple[int, ...]) -> HierarchyGroup:
+        """The group of these members for `kind`; groups of that kind over
+        other member sets are closed."""
+        for key in [q for q in self._groups_of if q[0] == kind and q[1] not in self._parts_now]:
+            self._groups_of.pop(key).close()
+        g = self._groups_of.get((kind, keys))
+        if g is None:
+            g = self._groups_of[(kind, keys)] = HierarchyGroup([self.members[k].mg.hierarchy for k in keys])
+        return g
+
+    def _grouped_jobs(self, kind: str, keys: tuple[int, ...], call):
+        """One side job per group of `keys`: call(group) on its own stream."""
+        self._parts_now = self._parts(keys)
+        return [(part, (lambda g=self._group(kind, part): call(g))) for part in self._parts_now]
+
+    def _run(self, fn, keys=None, sides=()):
         """fn(k, model) for the members `keys` (every member by default), each
-        worker on its own stream; `side()`, when given, runs meanwhile on a
-        stream of its own.  Returns the results in member order and side's."""
+        worker on its own stream; every callable in `sides` runs meanwhile on
+        a stream of its own.  Returns the results in member order and the
+        sides' results."""
         res = [None] * len(self.members)
         keys = set(range(len(self.members))) if keys is None else set(keys)
         caller = torch.cuda.current_stream()
@@ -160,7 +226,7 @@ class Ensemble:
 
         def work(w):
             if self._streams[w] is None:
-                self._streams[w] = torch.cuda.Stream()
+                self._streams[w] = self._own.new()
             s = self._streams[w]
             s.wait_event(start)
             with torch.cuda.stream(s):
@@ -171,22 +237,24 @@ class Ensemble:
             done.record(s)
             return done
 
-        def side_job():
-            if self._side_stream is None:
-                self._side_stream = torch.cuda.Stream()
-            s = self._side_stream
+        while len(self._side_streams) < len(sides):
+            self._side_streams.append(self._own.new())
+
+        def side_job(q):
+            s = self._side_streams[q]
             s.wait_event(start)
             with torch.cuda.stream(s):
-                out = side()
+                out = sides[q]()
             done = torch.cuda.Event()
             done.record(s)
             return out, done
 
-        fut = self._side.submit(side_job) if side is not None else None
+        futs = [self._side.submit(side_job, q) for q in range(len(sides))]
         events = list(self._pool.map(work, range(self.workers)))
-        side_out = None
-        if fut is not None:
-            side_out, e = fut.result()
+        side_out = []
+        for f in futs:
+            out, e = f.result()
+            side_out.append(out)
             events.append(e)
         for e in events:
             caller.wait_event(e)
@@ -204,14 +272,6 @@ class Ensemble:
         """Member k's forward solve runs in the grouped solve: a group member
         with a schedule (FASCD or guarded Newton)."""
         return self._in_groups(k) and self.schedules.get(k) in CANDIDATES
-
-    def _forward_group(self, keys: tuple[int, ...]) -> HierarchyGroup:
-        if self._fwd_group is None or self._fwd_keys != keys:
-            if self._fwd_group is not None:
-                self._fwd_group.close()
-            self._fwd_group = HierarchyGroup([self.members[k].mg.hierarchy for k in keys])
-            self._fwd_keys = keys
-        return self._fwd_group
 
     def forward(self, t: float, dt: float, update_geometry: bool = True, retry: bool = True):
         """One forward step of every member.  With `retry`, a member whose
@@ -264,10 +324,11 @@ class Ensemble:
         solo = [k for k in range(n) if k not in gk]
         if not gk:
             return self._run(one)[0]
-        group = self._forward_group(gk)
-        res, gst = self._run(one, keys=solo, side=lambda: group.forward(dt))
+        jobs = self._grouped_jobs("fwd", gk, lambda g: g.forward(dt))
+        self._fwd_keys = gk
+        res, outs = self._run(one, keys=solo, sides=[job for _, job in jobs])
         # retries, geometry update and hooks of the grouped members, on the workers
-        first = dict(zip(gk, gst))
+        first = {k: st for (part, _), gst in zip(jobs, outs) for k, st in zip(part, gst)}
         done, _ = self._run(lambda k, m: one(k, m, first[k]), keys=gk)
         for k in gk:
             res[k] = done[k]
@@ -291,17 +352,14 @@ class Ensemble:
         if len(masks) != 1:
             raise ValueError("grouped adjoint solves need one gradient mask for every member")
         mask = masks.pop()
-        if self._adj_group is None or self._adj_keys != gk:
-            if self._adj_group is not None:
-                self._adj_group.close()
-            self._adj_group = HierarchyGroup([self.members[k].mg.hierarchy for k in gk])
-            self._adj_keys = gk
-        group = self._adj_group
+        jobs = self._grouped_jobs("adj", gk, lambda g: g.backward(dt, mask=mask))
+        self._adj_keys = gk
         solo = [k for k in range(len(self.members)) if k not in gk]
-        res, gst = self._run(one, keys=solo, side=lambda: group.backward(dt, mask=mask))
-        for k, s in zip(gk, gst):
-            self.members[k].adjoint_solver.dt, self.members[k].adjoint_solver.last_stats = float(dt), s
-            res[k] = s
+        res, outs = self._run(one, keys=solo, sides=[job for _, job in jobs])
+        for (part, _), gst in zip(jobs, outs):
+            for k, s in zip(part, gst):
+                self.members[k].adjoint_solver.dt, self.members[k].adjoint_solver.last_stats = float(dt), s
+                res[k] = s
         return res
 
     def autotune(self, dt: float, candidates: dict | None = None, warm: bool = True) -> dict[int, str]:

@@ -3,8 +3,8 @@ kind of launch of a V-cycle once for all members, and every member computes
 what its own solve computes: the same cycles, the same launches and
 arguments.  The grouped kernels are separate compilations of the same tile
 bodies, so the results agree to rounding (measured ~1e-12 relative after a
-solve; asserted at the 1e-10 binary64 parity bar, 1e-4 in binary32) and the
-cycle counts are identical.
+solve; asserted at the 1e-10 binary64 parity bar, in binary32 at ten times
+the solve tolerance of 1e-4) and the cycle counts are identical.
 
 - forward solves to a relative tolerance -- FASCD and guarded Newton with
   its undo and fallback decisions taken on the device -- members stopping at
@@ -94,7 +94,7 @@ def test_group_matches_solo_solves(precision):
     assert solo_stats == group_stats
     # the two forward steps stop after different cycle counts per member
     assert len(set(solo_stats[0])) > 1
-    tol = 1e-10 if precision == "fp64" else 1e-4
+    tol = 1e-10 if precision == "fp64" else 1e-3
     for a, b in zip(solo, grouped):
         for k in FIELDS:
             x = a.mg.hierarchy.get(k, 0).double().cpu().numpy()
