@@ -86,8 +86,8 @@ def parse(argv=None):
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
     ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
     ap.add_argument("--ens-cold-tune", action="store_true", help="ensemble: autotune on the cold first step")
-    ap.add_argument("--ens-solo", action="store_true",
-                    help="ensemble: every member solves on its own (no grouped launches)")
+    ap.add_argument("--ens-grouped", action="store_true",
+                    help="ensemble: grouped launches (glide_b200.group) instead of per-stream member solves")
     ap.add_argument("--ens-group-max-n", type=int, default=0,
                     help="ensemble: only members of at most n x n cells join the grouped solves (0: all)")
     ap.add_argument("--ens-group-size", type=int, default=0,
@@ -102,7 +102,8 @@ def parse(argv=None):
     ap.add_argument("--enth-column-blocks", type=int, default=None, help="enthalpy column kernel blocks per SM")
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
     ap.add_argument("--mode", default="step",
-                    choices=["step", "sweeps", "kernels", "thermal", "columns", "ensemble", "vti", "coupled"],
+                    choices=["step", "sweeps", "kernels", "thermal", "columns", "ensemble", "group", "vti",
+                             "coupled"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -744,6 +745,66 @@ def run_columns(a):
     print(json.dumps({"mode": "columns", "size": a.size, "nz": a.nz}), flush=True)
 
 
+def run_group_case(a):
+    """Profiling case for grouped solves: 8 members of 192^2 (4 levels, dx
+    1500 m, short FASCD schedule), 3 forward and 3 adjoint cycles each (no
+    tolerance test), solved as one group and then one member after another
+    on one stream, from the same states.  A profiler's launch list of this
+    command sets each grouped kernel's time beside the per-member kernels it
+    replaces."""
+    import torch
+    from cases import dome
+    from glide_b200.ensemble import CANDIDATES, apply_schedule
+    from glide_b200.group import HierarchyGroup
+    from glide_b200.model import IceDynamics
+
+    def members():
+        out = []
+        for k in range(8):
+            f = dome(192, 1500.0, 0.4 * 192 * 1500.0, seed=10 + k)
+            m = IceDynamics(n_levels=4, ny=192, nx=192, dx=1500.0, reference_quirks=False)
+            mg = m.mg
+            for key, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
+                getattr(grp, key).set(torch.as_tensor(f[key]))
+            mg.state.H.set(torch.as_tensor(f["H"]))
+            mg.state.H_prev.set(torch.as_tensor(f["H_prev"]))
+            apply_schedule(m, CANDIDATES["fascd"])
+            for solver in (m.forward_solver, m.adjoint_solver):
+                solver.fas_options.set(maximum_vcycles=3, relative_tolerance=0.0, absolute_tolerance=0.0,
+                                       report_norms=False)
+            out.append(m)
+        return out
+
+    def dJ(m):
+        return 0.05 * m.mg.hierarchy.get("u", 0)
+
+    stream = torch.cuda.current_stream()
+    grouped, solo = members(), members()
+    g = HierarchyGroup([m.mg.hierarchy for m in grouped])
+
+    def run_group():
+        g.forward(a.dt, 0)
+        for m in grouped:
+            m.prepare_backward(dJdu=dJ(m))
+        g.backward(a.dt, 0)
+
+    def run_solo():
+        for m in solo:
+            m.mg.hierarchy.forward(a.dt, 0)
+            m.prepare_backward(dJdu=dJ(m))
+            m.mg.hierarchy.backward(a.dt, 0)
+
+    run_group()  # plans and graphs are built on the first call
+    run_solo()
+    ms_group = event_time(run_group, 3, stream)
+    ms_solo = event_time(run_solo, 3, stream)
+    c = g.counters()
+    g.close()
+    return {"members": 8, "grid": 192, "cycles": "3 forward + 3 adjoint per member", "ms_grouped": ms_group,
+            "ms_one_after_another": ms_solo, "forward_cycle": c["forward_cycle"], "adjoint_cycle": c["adjoint_cycle"],
+            "what": "one group solve, then the members' own solves one after another on one stream"}
+
+
 def run_ensemble(a):
     """The batched-ensemble workload: `--members` independent domes of uneven
     sizes drawn from {128, 192, 256, 384, 512, 768}^2 (dx 1500 m, levels down to
@@ -777,7 +838,7 @@ def run_ensemble(a):
             m.adjoint_solver.fas_options.set(pre_steps=4, post_steps=4, finest_steps=0, coarsest_steps=50)
             m.adjoint_solver.vanka_options.set(omega=0.8)
         members.append(m)
-    ens = Ensemble(members, workers=a.ens_workers, grouped=not a.ens_solo,
+    ens = Ensemble(members, workers=a.ens_workers, grouped=a.ens_grouped,
                    group_max_cells=a.ens_group_max_n ** 2 if a.ens_group_max_n else None,
                    group_by=a.ens_group_by, group_size=a.ens_group_size or None)
     t0 = time.perf_counter()
@@ -1357,6 +1418,9 @@ def main():
         return 0
     if a.mode == "ensemble":
         print(json.dumps({"mode": "ensemble", **run_ensemble(a)}), flush=True)
+        return 0
+    if a.mode == "group":
+        print(json.dumps({"mode": "group", **run_group_case(a)}), flush=True)
         return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
