@@ -142,3 +142,28 @@ def test_grouped_ensemble_matches_solo_runs():
         for k in ("u", "v", "H", "H_prev", "lambda_u", "lambda_H", "grad_beta", "grad_bed"):
             x, y = ma.mg.hierarchy.get(k, 0).cpu().numpy(), mb.mg.hierarchy.get(k, 0).cpu().numpy()
             assert rel_err(x, y) <= 1e-10, (k, rel_err(x, y))
+
+
+def test_grouping_partitions_members_by_size_and_count():
+    """Grouped mode's partition of the group members: one group per grid size
+    (members in order), split into groups of at most `group_size`; "all"
+    puts every member in one group before the split."""
+    from types import SimpleNamespace
+    from glide_b200.ensemble import Ensemble
+
+    def fake(n):
+        h = SimpleNamespace(shapes=[(n, n, 1500.0)], precision="fp64")
+        return SimpleNamespace(mg=SimpleNamespace(hierarchy=h), top_level=0)
+
+    sizes = [128, 256, 128, 768, 256, 128, 128]
+    ens = Ensemble([fake(n) for n in sizes], workers=2, grouped=True)
+    keys = tuple(range(len(sizes)))
+    assert ens._parts(keys) == [(0, 2, 5, 6), (1, 4), (3,)]
+    ens.group_size = 3
+    assert ens._parts(keys) == [(0, 2, 5), (6,), (1, 4), (3,)]
+    ens.group_by, ens.group_size = "all", 4
+    assert ens._parts(keys) == [(0, 1, 2, 3), (4, 5, 6)]
+    assert ens._parts(()) == []
+    ens.group_max_cells = 256 * 256
+    assert [k for k in keys if ens._in_groups(k)] == [0, 1, 2, 4, 5, 6]
+    ens.close()

@@ -119,3 +119,30 @@ def test_group_refuses_mixed_members():
         HierarchyGroup([b.mg.hierarchy, c.mg.hierarchy])  # two precisions
     with pytest.raises(_lib.GlideError):
         HierarchyGroup([b.mg.hierarchy, b.mg.hierarchy])  # a handle twice
+
+
+def test_group_reports_a_nonfinite_member_and_solves_the_others():
+    """A member whose residual is not finite makes the group call return
+    GLIDE_ERR_NONFINITE after the others finish; the others' solves are
+    complete (they equal their solo solves), and the group stays usable."""
+    from glide_b200 import _lib
+    from glide_b200.group import HierarchyGroup
+    solo, grouped = _members("fp64")[:3], _members("fp64")[:3]
+    H = grouped[1].mg.hierarchy.get("H", 0).clone()
+    H[5, 5] = float("nan")
+    grouped[1].mg.hierarchy.set("H", 0, H, restrict_down=True)
+    g = HierarchyGroup([m.mg.hierarchy for m in grouped])
+    with pytest.raises(_lib.GlideError) as err:
+        g.forward(DT)
+    assert err.value.code == _lib.GLIDE_ERR_NONFINITE
+    for k in (0, 2):
+        solo[k].forward(0.0, DT, update_geometry=False)
+        for f in ("u", "v", "H"):
+            x = solo[k].mg.hierarchy.get(f, 0).cpu().numpy()
+            y = grouped[k].mg.hierarchy.get(f, 0).cpu().numpy()
+            assert rel_err(y, x) <= 1e-10, (k, f)
+    # the non-finite member restored, the same group solves all three
+    grouped[1].mg.hierarchy.set("H", 0, solo[1].mg.hierarchy.get("H", 0), restrict_down=True)
+    st = g.forward(DT)
+    assert all(np.isfinite(s["final_norm"]) for s in st)
+    g.close()
