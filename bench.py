@@ -93,6 +93,8 @@ def parse(argv=None):
                     help="ensemble: grouped launches (glide_b200.group) instead of per-stream member solves")
     ap.add_argument("--ens-group-max-n", type=int, default=0,
                     help="ensemble: only members of at most n x n cells join the grouped solves (0: all)")
+    ap.add_argument("--ens-group-waves", type=int, default=None,
+                    help="ensemble: grouped launches of this many waves of resident blocks (0: a block per tile)")
     ap.add_argument("--ens-group-size", type=int, default=0,
                     help="ensemble: at most this many members per group (0: no limit)")
     ap.add_argument("--ens-sizes", default="128,192,256,384,512,768",
@@ -856,7 +858,7 @@ def run_ensemble(a):
         members.append(m)
     ens = Ensemble(members, workers=a.ens_workers, grouped=a.ens_grouped,
                    group_max_cells=a.ens_group_max_n ** 2 if a.ens_group_max_n else None,
-                   group_by=a.ens_group_by, group_size=a.ens_group_size or None)
+                   group_by=a.ens_group_by, group_size=a.ens_group_size or None, group_waves=a.ens_group_waves)
     t0 = time.perf_counter()
     chosen = ens.autotune(a.dt, warm=not a.ens_cold_tune)
     tune_s = time.perf_counter() - t0
@@ -901,6 +903,7 @@ def run_ensemble(a):
             "group_max_n": a.ens_group_max_n or None,
             "group_by": a.ens_group_by,
             "group_size": a.ens_group_size or None,
+            "group_waves": a.ens_group_waves,
             "group_cycles": group_cycles,
             "autotune_trials": {str(n): {k: dict(v, ms=round(v["ms"], 2)) for k, v in t.items()}
                                 for n, t in ens.trials.items()},

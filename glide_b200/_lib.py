@@ -158,6 +158,7 @@ SIGNATURES = {
     "glide_group_forward": ([_H, _D, _I, ctypes.POINTER(Stats), _P], _I),
     "glide_group_backward": ([_H, _D, _I, _I, ctypes.POINTER(Stats), _P], _I),
     "glide_group_counters": ([_H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I)], _I),
+    "glide_group_set_tuning": ([_H, _I, _I], _I),
 }
 
 class EnthalpyConfig(ctypes.Structure):

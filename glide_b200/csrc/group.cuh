@@ -9,13 +9,16 @@
 // bank).  Every block first lists the items whose member still runs this
 // cycle and their tile ranges, then strides over those tiles only, running
 // each with its member's arguments; the grid is one wave of resident blocks,
-// so members that have converged cost nothing.  Stencil tiles are staged with
-// plain loads (tensor maps stay per member).
+// so members that have converged cost nothing.  Stencil tiles are staged by
+// TMA from the member's own tensor maps, kept in a device array per grouped
+// launch (the parameter space holds a pointer to it).
 //
 // The convergence test of every member runs on the device (k_group_control)
 // and clears the member's run flag, so its state stays that of its last
 // cycle -- the state a solo solve of that member stops at.
 #pragma once
+
+#include <type_traits>
 
 #include "glide_b200.h"
 #include "adjoint_kernels.cuh"
@@ -68,12 +71,28 @@ constexpr int group_capacity() {
 
 template <class A, int N>
 struct GroupParams {
-    const int* flags;  // per-member run flags
-    int n;             // items
-    int when;          // flag bits a member must have for its items to run (0: every member)
+    const int* flags;            // per-member run flags
+    const unsigned char* maps;   // the items' staging maps (BoxMaps), maps_stride apart, or null
+    unsigned maps_stride;
+    int n;                       // items
+    int when;                    // flag bits a member must have for its items to run (0: every member)
     GroupItem item[N];
     A args[N];
 };
+
+// The staging maps of one item, in global memory: the acquire fence orders
+// the TMA unit's reads of them after their upload (thread 0 issues the
+// copies, so thread 0 fences).
+template <int N>
+__device__ __forceinline__ const BoxMaps<N>& item_maps(const unsigned char* mp) {
+    const BoxMaps<N>& m = *reinterpret_cast<const BoxMaps<N>*>(mp);
+    if (threadIdx.x == 0 && m.use) {
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&m.m[q]) : "memory");
+    }
+    return m;
+}
 
 // Pointwise kernels: 256 threads, x over columns, y over rows, z over jobs.
 template <class R>
@@ -81,7 +100,7 @@ struct GSnapshot {
     static constexpr int kMinBlocks = 4;
     using Args = SnapshotArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         snapshot_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -90,7 +109,7 @@ struct GRestrict {
     static constexpr int kMinBlocks = 4;
     using Args = RestrictArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         restrict_at(a.f, a.c, a.copy, a.kind, a.nyc, a.nxc, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -99,7 +118,7 @@ struct GRestrictBatch {
     static constexpr int kMinBlocks = 4;
     using Args = RestrictJobs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         restrict_at(a.f[b.bz], a.c[b.bz], a.copy[b.bz], a.kind[b.bz], a.nyc, a.nxc, b.by,
                     b.bx * kThreads + threadIdx.x);
     }
@@ -109,7 +128,7 @@ struct GCorrectBatch {
     static constexpr int kMinBlocks = 4;
     using Args = CorrectJobs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         correct_at(a.j[b.bz], b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -118,7 +137,7 @@ struct GGrounded {
     static constexpr int kMinBlocks = 4;
     using Args = GroundedArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         grounded_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -127,7 +146,7 @@ struct GCopy {
     static constexpr int kMinBlocks = 4;
     using Args = CopyArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         copy_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -136,7 +155,7 @@ struct GSetRhs {
     static constexpr int kMinBlocks = 4;
     using Args = SetRhsArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         set_rhs_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -145,7 +164,7 @@ struct GGradients {
     static constexpr int kMinBlocks = 4;
     using Args = GradArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         const int J = b.bx * kThreads + threadIdx.x;
         if (J < a.nx) gradients_at(a, b.by, J);
     }
@@ -155,7 +174,7 @@ struct GFill {
     static constexpr int kMinBlocks = 4;
     using Args = FillArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         fill_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -164,7 +183,7 @@ struct GTangentRhs {
     static constexpr int kMinBlocks = 4;
     using Args = TangentRhsArgs<R, R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         tangent_rhs_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -173,7 +192,7 @@ struct GNewtonUpdate {
     static constexpr int kMinBlocks = 4;
     using Args = NewtonUpdateArgs<R, R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         newton_update_at(a, b.by, b.bx * kThreads + threadIdx.x);
     }
 };
@@ -181,19 +200,23 @@ struct GNorms {
     static constexpr int kMinBlocks = 1;
     using Args = NormsArgs;
     static constexpr int kThreads = kNormThreads;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock) {
         finish_norms_block(a.partial, a.nblocks, a.out);
     }
 };
 
-// Stencil kernels: the tile bodies of the per-hierarchy kernels, staged with
-// plain loads.
-template <int N>
-__device__ __forceinline__ BoxMaps<N> no_maps() {
-    BoxMaps<N> m;
-    m.use = 0;
-    return m;
-}
+// Stencil kernels: the tile bodies of the per-hierarchy kernels, staged from
+// the item's maps (kMaps of them).  A block re-initialises the staging
+// mbarrier for every tile it runs; the tiles are separated by a block-wide
+// barrier, so no thread still waits on the previous phase.
+template <class Op, class = void>
+struct OpMaps {
+    static constexpr int n = 0;
+};
+template <class Op>
+struct OpMaps<Op, std::void_t<decltype(Op::kMaps)>> {
+    static constexpr int n = Op::kMaps;
+};
 
 // Register budgets: the per-hierarchy kernels' resident blocks per SM.
 template <class R, bool PHI_LIVE, int MINB>
@@ -201,42 +224,48 @@ struct GSweep {
     static constexpr int kMinBlocks = MINB;
     using Args = SweepArgs<R>;
     static constexpr int kThreads = kSweepThreads;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
         vanka_sweep_tile<R, PHI_LIVE>(a, a.gmode, b);
     }
 };
 template <class R>
 struct GResidual {
+    static constexpr int kMaps = 7;
     static constexpr int kMinBlocks = sizeof(R) == 8 ? 4 : 5;
     using Args = ResidualArgs<R>;
     static constexpr int kThreads = 256;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
-        residual_tile<R>(a, no_maps<7>(), b);
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char* mp, GroupBlock b) {
+        residual_tile<R>(a, item_maps<7>(mp), b);
     }
 };
 template <class R>
 struct GVjp {
+    static constexpr int kMaps = 9;
     static constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 3;
     using Args = VjpArgs<R>;
     static constexpr int kThreads = kTileA * kTileA;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) { vjp_tile<R>(a, no_maps<9>(), b); }
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char* mp, GroupBlock b) {
+        vjp_tile<R>(a, item_maps<9>(mp), b);
+    }
 };
 template <class R>
 struct GJvp {
+    static constexpr int kMaps = JvpTile<R>::NB;
     static constexpr int kMinBlocks = sizeof(R) == 8 ? 3 : 6;
     using Args = JvpOpArgs<R>;
     static constexpr int kThreads = kTileA * kTileA;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
-        jvp_tile<R>(a.a, a.mode, no_maps<JvpTile<R>::NB>(), b);
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char* mp, GroupBlock b) {
+        jvp_tile<R>(a.a, a.mode, item_maps<JvpTile<R>::NB>(mp), b);
     }
 };
 template <class R, bool TR>
 struct GBlockFactor {
+    static constexpr int kMaps = 7;
     static constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 4;
     using Args = BlockArgs<R>;
     static constexpr int kThreads = kTile * kTile;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) {
-        block_factor_tile<R, TR>(a, no_maps<7>(), b);
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char* mp, GroupBlock b) {
+        block_factor_tile<R, TR>(a, item_maps<7>(mp), b);
     }
 };
 template <class R, bool TR>
@@ -244,7 +273,9 @@ struct GBlockSweep {
     static constexpr int kMinBlocks = sizeof(R) == 8 ? 4 : 5;
     using Args = BlockArgs<R>;
     static constexpr int kThreads = kSweepThreads;
-    static __device__ __forceinline__ void run(const Args& a, GroupBlock b) { block_sweep_tile<R, TR>(a, b); }
+    static __device__ __forceinline__ void run(const Args& a, const unsigned char*, GroupBlock b) {
+        block_sweep_tile<R, TR>(a, b);
+    }
 };
 
 // The items of a launch whose member runs this cycle, in order, with their
@@ -307,7 +338,7 @@ __global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks)
         const GroupItem& it = P.item[k];
         const unsigned gx = unsigned(it.gx), local = unsigned(t - S.start[lo]), per = gx * unsigned(it.gy);
         const unsigned rest = local % per;
-        Op::run(P.args[k], GroupBlock{rest % gx, rest / gx, local / per, gx});
+        Op::run(P.args[k], P.maps + size_t(k) * P.maps_stride, GroupBlock{rest % gx, rest / gx, local / per, gx});
         __syncthreads();  // the next tile restages the block's shared memory
     }
 }
@@ -329,11 +360,12 @@ enum GroupFlag {
     kGroupPro = 8,     // ... preceded by the Newton prologue
     kGroupUndo = 16,   // the Newton step is undone
 };
-enum GroupStatus { GS_RUNNING = 0, GS_DONE = 1, GS_NONFINITE = 2 };
+enum GroupStatus { GS_RUNNING = 0, GS_DONE = 1, GS_NONFINITE = 2, GS_TIMEOUT = 3 };
 enum GroupPhase { GC_INIT = 0, GC_MID = 1, GC_POST = 2, GC_END = 3 };
 
 struct GroupMember {
     const double* norms;  // the member's norm vector |r_u|, |r_v|, |r_H|, |r|
+    const int* err;       // the member's error word (a staged tile's bounded wait gave up)
     double rtol, atol;
     double newton_switch, stall_ratio;
     int max_cycles;
@@ -397,6 +429,11 @@ __global__ void __launch_bounds__(kGroupControlThreads)
         } else if (phase == GC_POST) {
             if ((f & kGroupNewton) && !(g.norms[3] <= g.prev)) f |= kGroupUndo;
         } else {  // GC_END
+            if (*(volatile const int*)g.err) {
+                g.status = GS_TIMEOUT;
+                flags[k] = 0;
+                continue;
+            }
             double ab = g.norms[3];
             for (int q = 0; q < 3; ++q) g.last_norms[q] = g.norms[q];
             if (f & kGroupUndo) {

@@ -178,6 +178,7 @@ struct RecOp {
     int gx, gy, gz;
     std::vector<unsigned char> args;
     double bytes;
+    std::vector<unsigned char> maps;  // the staging maps of a stencil launch (BoxMaps)
 };
 
 template <class R>
@@ -247,6 +248,13 @@ struct Solver : SolverBase {
         std::memcpy(r.args.data(), &a, sizeof(A));
         rec->push_back(std::move(r));
         return true;
+    }
+
+    // the staging maps of the launch just recorded
+    template <int N>
+    void attach_maps(const BoxMaps<N>& m) {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&m);
+        rec->back().maps.assign(p, p + sizeof(m));
     }
 
     void not_recordable(const char* what) const {
@@ -427,7 +435,9 @@ struct Solver : SolverBase {
         // u, v, H, phi, mask, bed, B, beta, gamma; forcing; subtrahend; 3 rows
         // written (and the active set)
         const double bytes = lb(l, 9 + (use_forcing ? 3 : 0) + (sub ? 3 : 0) + 3 + (active_set ? 1 : 0));
-        if (!record(G_RESIDUAL, 0, g, a, bytes)) {
+        if (record(G_RESIDUAL, 0, g, a, bytes)) {
+            attach_maps(box_maps(l, kStateBoxes));
+        } else {
             k_residual<R><<<g, 256, 0, s>>>(a, box_maps(l, kStateBoxes));
             counted("residual", bytes);
         }
@@ -1014,7 +1024,9 @@ struct Solver : SolverBase {
         if (L.tr) {
             const int fl[AdjTile<R>::NB] = {GLIDE_U, GLIDE_V, GLIDE_H, GLIDE_PHI, GLIDE_BED, GLIDE_BETA,
                                             GLIDE_B, L.x[0], L.x[1]};
-            if (!record(G_VJP, 0, g, a, lin_bytes)) {
+            if (record(G_VJP, 0, g, a, lin_bytes)) {
+                attach_maps(box_maps(l, fl, AdjTile<R>::BH));
+            } else {
                 k_vjp<R><<<g, kTileA * kTileA, 0, s>>>(a, box_maps(l, fl, AdjTile<R>::BH));
                 counted("vjp", lin_bytes);
             }
@@ -1022,7 +1034,9 @@ struct Solver : SolverBase {
             const int fl[JvpTile<R>::NB] = {GLIDE_U, GLIDE_V, L.x[0], L.x[1], GLIDE_H, GLIDE_PHI, GLIDE_BED,
                                             GLIDE_BETA, GLIDE_B, L.x[2]};
             const int mode = (ref_rows ? 1 : 0) | ((jvp_flags & GLIDE_USE_MASK) ? 0 : 2);
-            if (!record(G_JVP, 0, g, JvpOpArgs<R>{a, mode}, lin_bytes)) {
+            if (record(G_JVP, 0, g, JvpOpArgs<R>{a, mode}, lin_bytes)) {
+                attach_maps(box_maps(l, fl));
+            } else {
                 k_jvp<R><<<g, kTileA * kTileA, 0, s>>>(a, mode, box_maps(l, fl));
                 counted("jvp", lin_bytes);
             }
@@ -1077,7 +1091,10 @@ struct Solver : SolverBase {
         BlockArgs<R> a = block_args(l, dt, L);
         dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
         const double bytes = lb(l, 9 + 25);  // state read, 25 factor planes written
-        if (record(G_BLOCK_FACTOR, L.tr ? 1 : 0, g, a, bytes)) return;
+        if (record(G_BLOCK_FACTOR, L.tr ? 1 : 0, g, a, bytes)) {
+            attach_maps(box_maps(l, kStateBoxes));
+            return;
+        }
         const BoxMaps<7> m = box_maps(l, kStateBoxes);
         if (L.tr) k_block_factor<R, true><<<g, kTile * kTile, 0, s>>>(a, m);
         else k_block_factor<R, false><<<g, kTile * kTile, 0, s>>>(a, m);
@@ -1253,7 +1270,9 @@ struct Solver : SolverBase {
 // the device-side convergence test.
 struct GroupBase {
     virtual ~GroupBase() {}
+    virtual void invalidate() = 0;  // rebuild every plan on the next call
     int dtype = GLIDE_F64;
+    int waves = 1;  // grid of a grouped launch: waves x resident blocks (0: one block per tile)
     long long launches = 0;  // grouped launches issued (graph replays included)
     int shape[4] = {0, 0, 0, 0};  // last forward / adjoint cycle: grouped launches, member launches
     virtual void forward(double dt, int start, glide_stats* st, cudaStream_t s) = 0;
@@ -1272,6 +1291,7 @@ struct GroupRun : GroupBase {
     struct Launch {
         int op, variant, when;
         std::vector<std::pair<int, const RecOp*>> items;  // (member, its recorded launch)
+        const unsigned char* dev_maps = nullptr;           // the items' staging maps on the device
     };
     // A plan is a list of sections: grouped launches predicated on a flag bit,
     // or one phase of the device-side decisions.
@@ -1291,6 +1311,7 @@ struct GroupRun : GroupBase {
         std::vector<std::vector<double>> bytes;        // [section][member]: algorithmic bytes
         cudaGraphExec_t exec = nullptr;
         long long nodes = 0;
+        std::vector<void*> buffers;  // the launches' staging maps on the device
         std::vector<unsigned> versions;
         double dt = 0;
         int start = -1, extra = 0;
@@ -1315,14 +1336,61 @@ struct GroupRun : GroupBase {
     }
 
     ~GroupRun() override {
-        for (Plan& p : plans)
+        for (Plan& p : plans) {
             if (p.exec) cudaGraphExecDestroy(p.exec);
-        for (Plan& p : fwd_cycles)
+            for (void* b : p.buffers) cudaFree(b);
+        }
+        for (Plan& p : fwd_cycles) {
             if (p.exec) cudaGraphExecDestroy(p.exec);
+            for (void* b : p.buffers) cudaFree(b);
+        }
         if (own_stream) cudaStreamDestroy(own_stream);
         if (running_host) cudaFreeHost(running_host);
         if (flags) cudaFree(flags);
         if (dev) cudaFree(dev);
+    }
+
+    void invalidate() override {
+        for (Plan& p : plans) p.valid = false;
+        for (Plan& p : fwd_cycles) p.valid = false;
+    }
+
+    // the plan's device copies of staging maps (its graph is gone or idle)
+    void release(Plan& P) {
+        for (void* b : P.buffers) cudaFree(b);
+        P.buffers.clear();
+    }
+
+    // Bytes of the staging maps an op kind records (0: none).
+    static size_t maps_bytes(int op) {
+        switch (op) {
+            case G_RESIDUAL: return sizeof(BoxMaps<OpMaps<GResidual<R>>::n>);
+            case G_VJP: return sizeof(BoxMaps<OpMaps<GVjp<R>>::n>);
+            case G_JVP: return sizeof(BoxMaps<OpMaps<GJvp<R>>::n>);
+            case G_BLOCK_FACTOR: return sizeof(BoxMaps<OpMaps<GBlockFactor<R, false>>::n>);
+            default: return 0;
+        }
+    }
+
+    // Copy each stencil launch's staging maps into one device array (before
+    // a capture: no allocation may happen inside it).
+    void upload_maps(Plan& P) {
+        for (auto& sec : P.launches)
+            for (Launch& L : sec) {
+                const size_t b = maps_bytes(L.op);
+                if (!b || L.dev_maps) continue;
+                std::vector<unsigned char> host(b * L.items.size());
+                for (size_t q = 0; q < L.items.size(); ++q) {
+                    const RecOp& r = *L.items[q].second;
+                    if (r.maps.size() != b) fail(GLIDE_ERR_STATE, "a stencil launch was recorded without its maps");
+                    std::memcpy(host.data() + q * b, r.maps.data(), b);
+                }
+                void* d = nullptr;
+                GCU(cudaMalloc(&d, host.size()));
+                P.buffers.push_back(d);
+                GCU(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+                L.dev_maps = static_cast<const unsigned char*>(d);
+            }
     }
 
     // Record every member's sections into P (unless P is current) and merge
@@ -1337,6 +1405,7 @@ struct GroupRun : GroupBase {
             cudaGraphExecDestroy(P.exec);
             P.exec = nullptr;
         }
+        release(P);
         P.valid = false;
         const int n = int(members.size());
         const size_t ns = secs.size();
@@ -1410,6 +1479,10 @@ struct GroupRun : GroupBase {
             auto P = std::make_unique<GroupParams<A, N>>();
             P->flags = flags;
             P->when = L.when;
+            constexpr size_t mb = OpMaps<Op>::n ? sizeof(BoxMaps<OpMaps<Op>::n ? OpMaps<Op>::n : 1>) : 0;
+            if (mb && !L.dev_maps) fail(GLIDE_ERR_STATE, "staging maps not on the device");
+            P->maps = mb ? L.dev_maps + base * mb : nullptr;
+            P->maps_stride = unsigned(mb);
             long long nb = 0;
             int k = 0;
             for (size_t q = base; q < L.items.size() && k < N; ++q, ++k) {
@@ -1423,7 +1496,8 @@ struct GroupRun : GroupBase {
             }
             if (nb > 0x7fffffffLL) fail(GLIDE_ERR_SHAPE, "grouped launch over 2^31 tiles");
             P->n = k;
-            k_group<Op, N><<<unsigned(std::min(nb, wave)), Op::kThreads, 0, s>>>(*P);
+            const long long grid = waves > 0 ? std::min(nb, waves * wave) : nb;
+            k_group<Op, N><<<unsigned(std::max(grid, 1LL)), Op::kThreads, 0, s>>>(*P);
             check_launch("grouped launch");
             ++issued;
         }
@@ -1465,6 +1539,7 @@ struct GroupRun : GroupBase {
         const int n = int(members.size());
         if (!P.exec) {
             std::lock_guard<std::mutex> lock(g_capture_mu);
+            upload_maps(P);
             cudaGraph_t g = nullptr;
             long long nodes = 0;
             GCU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1528,6 +1603,7 @@ struct GroupRun : GroupBase {
             GroupMember& g = host[k];
             std::memset(static_cast<void*>(&g), 0, sizeof(g));
             g.norms = m.norms_dev;
+            g.err = m.err_dev;
             g.rtol = c.relative_tolerance;
             g.atol = c.absolute_tolerance;
             g.max_cycles = c.maximum_vcycles;
@@ -1550,10 +1626,15 @@ struct GroupRun : GroupBase {
 
     // statistics and the members' own records of the solve
     void finish(const Plan& pro, int cfg, glide_stats* st, const std::function<double(int)>& bytes) {
-        int bad = -1;
+        int bad = -1, late = -1;
         for (size_t k = 0; k < members.size(); ++k) {
             const GroupMember& g = host[k];
             Solver<R>& m = *members[k];
+            if (g.status == GS_TIMEOUT) {
+                // clear the word, so the member's next solve starts clean
+                GCU(cudaMemset(m.err_dev, 0, sizeof(int)));
+                if (late < 0) late = int(k);
+            }
             if (st) {
                 glide_stats& o = st[k];
                 std::memset(&o, 0, sizeof(o));
@@ -1574,6 +1655,8 @@ struct GroupRun : GroupBase {
             m.last_cycles = g.cycles;
             if (g.status == GS_NONFINITE && bad < 0) bad = int(k);
         }
+        if (late >= 0)
+            fail(GLIDE_ERR_TIMEOUT, "member " + std::to_string(late) + ": a bounded wait for staged tiles gave up");
         if (bad >= 0) fail(GLIDE_ERR_NONFINITE, "member " + std::to_string(bad) + ": residual norm is not finite");
     }
 
@@ -2223,6 +2306,19 @@ int glide_group_backward(glide_group g, double dt, int start_level, int grad_mas
     return guarded([&] {
         if (!g || !g->impl) fail(GLIDE_ERR_ARG, "null group");
         g->impl->backward(dt, start_level, grad_mask, stats, S(stream));
+    });
+}
+
+int glide_group_set_tuning(glide_group g, int key, int value) {
+    return guarded([&] {
+        if (!g || !g->impl) fail(GLIDE_ERR_ARG, "null group");
+        if (key == GLIDE_GROUP_TUNE_WAVES) {
+            if (value < 0 || value > 64) fail(GLIDE_ERR_ARG, "waves must lie in [0, 64]");
+            g->impl->waves = value;
+            g->impl->invalidate();
+        } else {
+            fail(GLIDE_ERR_ARG, "unknown group tuning key");
+        }
     });
 }
 

@@ -141,7 +141,8 @@ class Ensemble:
     """Concurrent driver of independent members (see the module text)."""
 
     def __init__(self, members: list[IceDynamics], workers: int | None = None, grouped: bool = False,
-                 group_max_cells: int | None = None, group_by: str = "class", group_size: int | None = None):
+                 group_max_cells: int | None = None, group_by: str = "class", group_size: int | None = None,
+                 group_waves: int | None = None):
         self.members = list(members)
         n = len(self.members)
         self.workers = max(1, min(workers or min(n, 16), n))
@@ -166,6 +167,7 @@ class Ensemble:
             raise ValueError("group_by must be 'class' or 'all'")
         self.group_by = group_by
         self.group_size = group_size  # at most this many members per group (None: no limit)
+        self.group_waves = group_waves  # launch shape of the grouped launches (None: the default)
         self._groups_of: dict[tuple[str, tuple[int, ...]], HierarchyGroup] = {}
         self._fwd_keys: tuple[int, ...] = ()
         self._adj_keys: tuple[int, ...] = ()
@@ -206,6 +208,7 @@ class Ensemble:
         g = self._groups_of.get((kind, keys))
         if g is None:
             g = self._groups_of[(kind, keys)] = HierarchyGroup([self.members[k].mg.hierarchy for k in keys])
+            g.set_tuning(waves=self.group_waves)
         return g
 
     def _grouped_jobs(self, kind: str, keys: tuple[int, ...], call):

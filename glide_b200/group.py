@@ -66,6 +66,13 @@ class HierarchyGroup:
                                                     _stream_ptr()))
         return [s.to_dict() for s in st]
 
+    def set_tuning(self, waves: int | None = None):
+        """Launch shape of the grouped launches: `waves` x the GPU's resident
+        blocks per launch, each block striding over the running members'
+        tiles (default 1); 0 launches one block per tile."""
+        if waves is not None:
+            _lib.check(_lib.load().glide_group_set_tuning(self._g, 1, int(waves)))
+
     def counters(self) -> dict:
         """Grouped launches issued so far, and the shape of the last forward
         and adjoint cycles: grouped launches and the members' launches they

@@ -328,6 +328,13 @@ int glide_group_destroy(glide_group g);
 int glide_group_forward(glide_group g, double dt, int start_level, glide_stats* stats, void* stream);
 int glide_group_backward(glide_group g, double dt, int start_level, int grad_mask, glide_stats* stats,
                          void* stream);
+/* Launch shape of the grouped launches (no counterpart in the reference).
+ * GLIDE_GROUP_TUNE_WAVES: the grid is value x the resident blocks of the
+ * GPU, every block striding over the tiles of the running members (default
+ * 1); 0 launches one block per tile of every member instead.  Plans are
+ * recaptured on the next call. */
+#define GLIDE_GROUP_TUNE_WAVES 1
+int glide_group_set_tuning(glide_group g, int key, int value);
 /* launches: grouped launches issued so far.  shape (4 ints, may be NULL): the
  * last forward cycle's grouped launches and the members' launches they
  * carry, then the same for the adjoint cycle. */
