@@ -6,10 +6,12 @@
 // are merged into ONE persistent launch over a table of items, one per
 // member: its arguments and its tile grid.  The table is the launch's kernel
 // parameters (__grid_constant__, up to 32 KB, read through the constant
-// bank).  Every block first lists the items whose member still runs this
-// cycle and their tile ranges, then strides over those tiles only, running
-// each with its member's arguments; the grid is one wave of resident blocks,
-// so members that have converged cost nothing.  Stencil tiles are staged by
+// bank).  A block finds its tile's item by a binary search over the table
+// from its tile index alone, so the compiler sees the item as uniform over
+// the block and reads its arguments as uniform values; a tile whose member
+// no longer runs exits at the cost of that search.  By default there is one
+// block per tile (k_group); k_group_waves instead runs a fixed number of
+// waves of resident blocks that stride over the tiles.  Stencil tiles are staged by
 // TMA from the member's own tensor maps, kept in a device array per grouped
 // launch (the parameter space holds a pointer to it).
 //
@@ -53,10 +55,10 @@ struct RestrictArgs {
     int kind, nyc, nxc;
 };
 
-// One item of a grouped launch: the member's grid of `blocks` = gx x gy x gz
-// tiles, as its own launch would have it.
+// One item of a grouped launch: the member's grid of gx x gy x gz tiles, as
+// its own launch would have it, starting at tile `first` of the launch.
 struct GroupItem {
-    int blocks, gx, gy, member;
+    int first, gx, gy, member;
 };
 
 constexpr int kGroupParamBytes = 32000;  // below the 32764-byte kernel parameter limit
@@ -80,16 +82,18 @@ struct GroupParams {
     A args[N];
 };
 
-// The staging maps of one item, in global memory: the acquire fence orders
-// the TMA unit's reads of them after their upload (thread 0 issues the
-// copies, so thread 0 fences).
+// The staging maps of one item, in global memory, written by a host copy:
+// the acquire fence, at system scope since the writer is the host, orders
+// the TMA unit's reads of them after that copy -- an address freed and
+// allocated again may still be cached with the maps it held before (thread
+// 0 issues the copies, so thread 0 fences).
 template <int N>
 __device__ __forceinline__ const BoxMaps<N>& item_maps(const unsigned char* mp) {
     const BoxMaps<N>& m = *reinterpret_cast<const BoxMaps<N>*>(mp);
     if (threadIdx.x == 0 && m.use) {
 #pragma unroll
         for (int q = 0; q < N; ++q)
-            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&m.m[q]) : "memory");
+            asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(&m.m[q]) : "memory");
     }
     return m;
 }
@@ -278,65 +282,41 @@ struct GBlockSweep {
     }
 };
 
-// The items of a launch whose member runs this cycle, in order, with their
-// first tile: computed by warp 0 of every block (lane k handles items k and
-// k + 32), read by the whole block.
-template <int N>
-struct GroupScan {
-    int count;
-    int idx[N];
-    int start[N + 1];
-};
-
+// The item holding tile t: the last item whose range starts at or before t.
 template <class A, int N>
-__device__ __forceinline__ void group_scan(const GroupParams<A, N>& P, GroupScan<N>& S) {
-    static_assert(N <= 64, "two items per lane");
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        const unsigned lt = (1u << lane) - 1u;
-        int base = 0, placed = 0;
-        for (int h = 0; h < 2; ++h) {
-            const int k = lane + 32 * h;
-            const bool act = k < P.n && (P.when == 0 || (P.flags[P.item[k].member] & P.when) != 0);
-            int c = act ? P.item[k].blocks : 0;
-            int incl = c;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const unsigned ball = __ballot_sync(0xffffffffu, act);
-            if (act) {
-                const int pos = placed + __popc(ball & lt);
-                S.idx[pos] = k;
-                S.start[pos] = base + incl - c;
-            }
-            base += __shfl_sync(0xffffffffu, incl, 31);
-            placed += __popc(ball);
-        }
-        if (lane == 0) {
-            S.count = placed;
-            S.start[placed] = base;
-        }
+__device__ __forceinline__ int group_item_of(const GroupParams<A, N>& P, int t) {
+    int lo = 0, hi = P.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.item[mid].first <= t) lo = mid;
+        else hi = mid - 1;
     }
-    __syncthreads();
+    return lo;
 }
 
+// One block per tile of all items.
 template <class Op, int N>
 __global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks)
     k_group(const __grid_constant__ GroupParams<typename Op::Args, N> P) {
-    __shared__ GroupScan<N> S;
-    group_scan(P, S);
-    const int total = S.start[S.count];
+    const int t = int(blockIdx.x);
+    const int k = group_item_of(P, t);
+    const GroupItem& it = P.item[k];
+    if (P.when && (P.flags[it.member] & P.when) == 0) return;  // uniform over the block
+    const unsigned gx = unsigned(it.gx), local = unsigned(t - it.first), per = gx * unsigned(it.gy);
+    const unsigned rest = local % per;
+    Op::run(P.args[k], P.maps + size_t(k) * P.maps_stride, GroupBlock{rest % gx, rest / gx, local / per, gx});
+}
+
+// `total` tiles of all items, strided over by a fixed grid; the loop and the
+// item search depend only on blockIdx and the parameters.
+template <class Op, int N>
+__global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks)
+    k_group_waves(const __grid_constant__ GroupParams<typename Op::Args, N> P, int total) {
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        int lo = 0, hi = S.count - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (S.start[mid] <= t) lo = mid;
-            else hi = mid - 1;
-        }
-        const int k = S.idx[lo];
+        const int k = group_item_of(P, t);
         const GroupItem& it = P.item[k];
-        const unsigned gx = unsigned(it.gx), local = unsigned(t - S.start[lo]), per = gx * unsigned(it.gy);
+        if (P.when && (P.flags[it.member] & P.when) == 0) continue;  // uniform over the block
+        const unsigned gx = unsigned(it.gx), local = unsigned(t - it.first), per = gx * unsigned(it.gy);
         const unsigned rest = local % per;
         Op::run(P.args[k], P.maps + size_t(k) * P.maps_stride, GroupBlock{rest % gx, rest / gx, local / per, gx});
         __syncthreads();  // the next tile restages the block's shared memory
@@ -360,12 +340,13 @@ enum GroupFlag {
     kGroupPro = 8,     // ... preceded by the Newton prologue
     kGroupUndo = 16,   // the Newton step is undone
 };
-enum GroupStatus { GS_RUNNING = 0, GS_DONE = 1, GS_NONFINITE = 2, GS_TIMEOUT = 3 };
+enum GroupStatus { GS_RUNNING = 0, GS_DONE = 1, GS_NONFINITE = 2, GS_STAGING = 3 };
 enum GroupPhase { GC_INIT = 0, GC_MID = 1, GC_POST = 2, GC_END = 3 };
 
 struct GroupMember {
     const double* norms;  // the member's norm vector |r_u|, |r_v|, |r_H|, |r|
-    const int* err;       // the member's error word (a staged tile's bounded wait gave up)
+    const int* err;       // the member's error word (kStage* bits of a staging block)
+    int err_word;         // its value when the member stopped on it
     double rtol, atol;
     double newton_switch, stall_ratio;
     int max_cycles;
@@ -410,7 +391,11 @@ __global__ void __launch_bounds__(kGroupControlThreads)
             g.in_newton = g.newton_off = g.stall = g.rejects = 0;
             g.history[0] = ab;
             for (int q = 0; q < 3; ++q) g.last_norms[q] = g.norms[q];
-            if (!isfinite(ab)) {
+            if (const int e = *(volatile const int*)g.err) {  // the norms are not this residual's
+                g.status = GS_STAGING;
+                g.err_word = e;
+                f = 0;
+            } else if (!isfinite(ab)) {
                 g.status = GS_NONFINITE;
                 f = 0;
             } else {
@@ -429,8 +414,9 @@ __global__ void __launch_bounds__(kGroupControlThreads)
         } else if (phase == GC_POST) {
             if ((f & kGroupNewton) && !(g.norms[3] <= g.prev)) f |= kGroupUndo;
         } else {  // GC_END
-            if (*(volatile const int*)g.err) {
-                g.status = GS_TIMEOUT;
+            if (const int e = *(volatile const int*)g.err) {
+                g.status = GS_STAGING;
+                g.err_word = e;
                 flags[k] = 0;
                 continue;
             }

@@ -203,7 +203,7 @@ struct Solver : SolverBase {
     double* partial = nullptr;
     double* norms_dev = nullptr;
     double* norms_host = nullptr;
-    int* err_dev = nullptr;  // set by a kernel whose bounded wait gave up
+    int* err_dev = nullptr;  // kStage* bits set by a staging block (its wait gave up, or its maps failed their check)
     // TMA tensor maps of every (level, field), encoded on first use
     // slot per box height (kTmaHeights)
     static constexpr int kTmaHeights[3] = {kBoxH, 22, 24};
@@ -481,6 +481,7 @@ struct Solver : SolverBase {
             // clear the word, so the next call on this handle starts clean
             GCU(cudaMemsetAsync(err_dev, 0, sizeof(int), s));
             GCU(cudaStreamSynchronize(s));
+            if (e & kStageBadMaps) fail(GLIDE_ERR_STATE, "a kernel's staging maps failed their check");
             fail(GLIDE_ERR_TIMEOUT, "a kernel's bounded wait for its tile copies gave up");
         }
     }
@@ -1272,7 +1273,8 @@ struct GroupBase {
     virtual ~GroupBase() {}
     virtual void invalidate() = 0;  // rebuild every plan on the next call
     int dtype = GLIDE_F64;
-    int waves = 1;  // grid of a grouped launch: waves x resident blocks (0: one block per tile)
+    int waves = 0;  // grid of a grouped launch: waves x resident blocks (0: one block per tile)
+    int spoil_maps = 0;  // GLIDE_GROUP_TUNE_SPOIL_MAPS: upload the staging maps without their tag
     long long launches = 0;  // grouped launches issued (graph replays included)
     int shape[4] = {0, 0, 0, 0};  // last forward / adjoint cycle: grouped launches, member launches
     virtual void forward(double dt, int start, glide_stats* st, cudaStream_t s) = 0;
@@ -1372,9 +1374,31 @@ struct GroupRun : GroupBase {
         }
     }
 
+    // Clear the tag of the staging maps at p (op's kind of maps).
+    template <int N>
+    static void untag(unsigned char* p) {
+        BoxMaps<N> m;
+        std::memcpy(static_cast<void*>(&m), p, sizeof(m));
+        m.tag = 0;
+        std::memcpy(p, static_cast<const void*>(&m), sizeof(m));
+    }
+    static void untag(int op, unsigned char* p) {
+        switch (op) {
+            case G_RESIDUAL: return untag<OpMaps<GResidual<R>>::n>(p);
+            case G_VJP: return untag<OpMaps<GVjp<R>>::n>(p);
+            case G_JVP: return untag<OpMaps<GJvp<R>>::n>(p);
+            case G_BLOCK_FACTOR: return untag<OpMaps<GBlockFactor<R, false>>::n>(p);
+            default: return;
+        }
+    }
+
     // Copy each stencil launch's staging maps into one device array (before
-    // a capture: no allocation may happen inside it).
-    void upload_maps(Plan& P) {
+    // a capture: no allocation may happen inside it).  The copies run on the
+    // stream the plan's graph will run on, and the call waits for them: a
+    // copy on the legacy stream would not be ordered before the kernels on a
+    // non-blocking stream, which could then read the array before it holds
+    // the maps.
+    void upload_maps(Plan& P, cudaStream_t s) {
         for (auto& sec : P.launches)
             for (Launch& L : sec) {
                 const size_t b = maps_bytes(L.op);
@@ -1384,11 +1408,13 @@ struct GroupRun : GroupBase {
                     const RecOp& r = *L.items[q].second;
                     if (r.maps.size() != b) fail(GLIDE_ERR_STATE, "a stencil launch was recorded without its maps");
                     std::memcpy(host.data() + q * b, r.maps.data(), b);
+                    if (spoil_maps) untag(L.op, host.data() + q * b);
                 }
                 void* d = nullptr;
                 GCU(cudaMalloc(&d, host.size()));
                 P.buffers.push_back(d);
-                GCU(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+                GCU(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
+                GCU(cudaStreamSynchronize(s));
                 L.dev_maps = static_cast<const unsigned char*>(d);
             }
     }
@@ -1471,7 +1497,7 @@ struct GroupRun : GroupBase {
             int dev = 0, sms = 0, per_sm = 0;
             GCU(cudaGetDevice(&dev));
             GCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            GCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_group<Op, N>, Op::kThreads, 0));
+            GCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_group_waves<Op, N>, Op::kThreads, 0));
             return (long long)sms * std::max(per_sm, 1);
         }();
         long long issued = 0;
@@ -1490,14 +1516,19 @@ struct GroupRun : GroupBase {
                 if (r.args.size() != sizeof(A)) fail(GLIDE_ERR_STATE, "recorded arguments of the wrong size");
                 const long long blocks = (long long)r.gx * r.gy * r.gz;
                 if (blocks > 0x7fffffffLL) fail(GLIDE_ERR_SHAPE, "grouped launch over 2^31 tiles");
-                P->item[k] = GroupItem{int(blocks), r.gx, r.gy, L.items[q].first};
+                P->item[k] = GroupItem{int(nb), r.gx, r.gy, L.items[q].first};
                 std::memcpy(static_cast<void*>(&P->args[k]), r.args.data(), sizeof(A));
                 nb += blocks;
             }
             if (nb > 0x7fffffffLL) fail(GLIDE_ERR_SHAPE, "grouped launch over 2^31 tiles");
+            if (nb == 0) continue;  // no tiles (a block per tile would run one of an empty item)
             P->n = k;
-            const long long grid = waves > 0 ? std::min(nb, waves * wave) : nb;
-            k_group<Op, N><<<unsigned(std::max(grid, 1LL)), Op::kThreads, 0, s>>>(*P);
+            if (waves > 0) {
+                const long long grid = std::min(nb, waves * wave);
+                k_group_waves<Op, N><<<unsigned(std::max(grid, 1LL)), Op::kThreads, 0, s>>>(*P, int(nb));
+            } else {
+                k_group<Op, N><<<unsigned(std::max(nb, 1LL)), Op::kThreads, 0, s>>>(*P);
+            }
             check_launch("grouped launch");
             ++issued;
         }
@@ -1539,7 +1570,7 @@ struct GroupRun : GroupBase {
         const int n = int(members.size());
         if (!P.exec) {
             std::lock_guard<std::mutex> lock(g_capture_mu);
-            upload_maps(P);
+            upload_maps(P, s);
             cudaGraph_t g = nullptr;
             long long nodes = 0;
             GCU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1625,15 +1656,20 @@ struct GroupRun : GroupBase {
     }
 
     // statistics and the members' own records of the solve
-    void finish(const Plan& pro, int cfg, glide_stats* st, const std::function<double(int)>& bytes) {
-        int bad = -1, late = -1;
+    void finish(const Plan& pro, int cfg, glide_stats* st, const std::function<double(int)>& bytes,
+                cudaStream_t s) {
+        int bad = -1, late = -1, word = 0;
         for (size_t k = 0; k < members.size(); ++k) {
             const GroupMember& g = host[k];
             Solver<R>& m = *members[k];
-            if (g.status == GS_TIMEOUT) {
+            if (g.status == GS_STAGING) {
                 // clear the word, so the member's next solve starts clean
-                GCU(cudaMemset(m.err_dev, 0, sizeof(int)));
-                if (late < 0) late = int(k);
+                GCU(cudaMemsetAsync(m.err_dev, 0, sizeof(int), s));
+                GCU(cudaStreamSynchronize(s));
+                if (late < 0) {
+                    late = int(k);
+                    word = g.err_word;
+                }
             }
             if (st) {
                 glide_stats& o = st[k];
@@ -1655,6 +1691,8 @@ struct GroupRun : GroupBase {
             m.last_cycles = g.cycles;
             if (g.status == GS_NONFINITE && bad < 0) bad = int(k);
         }
+        if (late >= 0 && (word & kStageBadMaps))
+            fail(GLIDE_ERR_STATE, "member " + std::to_string(late) + ": staging maps failed their check");
         if (late >= 0)
             fail(GLIDE_ERR_TIMEOUT, "member " + std::to_string(late) + ": a bounded wait for staged tiles gave up");
         if (bad >= 0) fail(GLIDE_ERR_NONFINITE, "member " + std::to_string(bad) + ": residual norm is not finite");
@@ -1736,7 +1774,7 @@ struct GroupRun : GroupBase {
             const int steps = g.cycles - g.fas_cycles;
             return g.fas_cycles * sec_bytes[T_FAS][k] + steps * (sec_bytes[T_BACKUP][k] + sec_bytes[T_NEWTON][k]) +
                    g.prologues * sec_bytes[T_PRO][k] + g.rejects * sec_bytes[T_UNDO][k];
-        });
+        }, s);
     }
 
     void backward(double dt, int start, int grad_mask, glide_stats* st, cudaStream_t s) override {
@@ -1758,7 +1796,8 @@ struct GroupRun : GroupBase {
         note_shape(C, 2);
         solve(plans[P_ADJ_PRO], [&](int) -> Plan& { return C; }, 1, false, s);
         run_plan(plans[P_GRAD], s);
-        finish(plans[P_ADJ_PRO], 1, st, [&](int k) { return host[k].cycles * C.bytes[0][k] + plans[P_GRAD].bytes[0][k]; });
+        finish(plans[P_ADJ_PRO], 1, st, [&](int k) { return host[k].cycles * C.bytes[0][k] + plans[P_GRAD].bytes[0][k]; },
+               s);
     }
 };
 
@@ -2315,6 +2354,10 @@ int glide_group_set_tuning(glide_group g, int key, int value) {
         if (key == GLIDE_GROUP_TUNE_WAVES) {
             if (value < 0 || value > 64) fail(GLIDE_ERR_ARG, "waves must lie in [0, 64]");
             g->impl->waves = value;
+            g->impl->invalidate();
+        } else if (key == GLIDE_GROUP_TUNE_SPOIL_MAPS) {
+            if (value != 0 && value != 1) fail(GLIDE_ERR_ARG, "spoil_maps must be 0 or 1");
+            g->impl->spoil_maps = value;
             g->impl->invalidate();
         } else {
             fail(GLIDE_ERR_ARG, "unknown group tuning key");

@@ -79,7 +79,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// Tensor maps of the arrays one stencil launch stages (kernel parameter).
+// Bits of a handle's error word set by a staging block.
+constexpr int kStageWaitGaveUp = 1;  // the bounded wait for the copies gave up
+constexpr int kStageBadMaps = 2;     // the maps did not carry kBoxMapsTag: nothing was copied
+
+constexpr int kBoxMapsTag = 0x474c4d50;
+
+// Tensor maps of the arrays one stencil launch stages (a kernel parameter,
+// or an element of a device array the host filled for a grouped launch).
 template <int N>
 struct BoxMaps {
     CUtensorMap m[N];
@@ -88,6 +95,9 @@ struct BoxMaps {
     // lowers it to make that wait give up); the wait that lets copies still
     // in flight land after a give-up always uses kTmaWaitPolls
     int wait_polls = kTmaWaitPolls;
+    // checked before the first copy: maps read from global memory that do not
+    // carry it (not written, or not yet) are never handed to the TMA unit
+    int tag = kBoxMapsTag;
 };
 
 // Scalar staging of one array into the box layout, indices clamped.
@@ -122,12 +132,17 @@ __device__ __forceinline__ void box_fixup(BoxT<R, BH>& t, int rows, int cols, in
 
 // Stage N arrays of one tile.  TMA path: thread 0 issues the copies, every
 // thread waits on the barrier, edge tiles are fixed up.  Returns false on
-// every thread of the block if the wait gave up (the error word is then set
-// and the block must return without touching the boxes).
+// every thread of the block if the maps fail their check or the wait gave up
+// (the error word is then set and the block must return without touching the
+// boxes).
 template <class R, int N, int BH = kBoxH, int BY = kBoxY>
 __device__ __forceinline__ bool stage_boxes(BoxT<R, BH>* const (&dst)[N], const Arr<R> (&src)[N],
                                             const BoxMaps<N>& maps, int i0, int j0, unsigned long long* bar,
                                             int* err) {
+    if (maps.use && maps.tag != kBoxMapsTag) {  // the same value on every thread
+        if (threadIdx.x == 0) atomicOr(err, kStageBadMaps);
+        return false;
+    }
     if (!maps.use) {
 #pragma unroll
         for (int q = 0; q < N; ++q) stage_box_scalar<R, BH, BY>(*dst[q], src[q], i0, j0);
@@ -146,7 +161,7 @@ __device__ __forceinline__ bool stage_boxes(BoxT<R, BH>* const (&dst)[N], const 
     }
     const bool ok = __syncthreads_and(mbar_wait(bar, 0, maps.wait_polls));
     if (!ok) {
-        if (threadIdx.x == 0) atomicOr(err, 1);
+        if (threadIdx.x == 0) atomicOr(err, kStageWaitGaveUp);
         mbar_wait(bar, 0);  // let copies still in flight land before the block exits
         return false;
     }

@@ -66,12 +66,17 @@ class HierarchyGroup:
                                                     _stream_ptr()))
         return [s.to_dict() for s in st]
 
-    def set_tuning(self, waves: int | None = None):
-        """Launch shape of the grouped launches: `waves` x the GPU's resident
-        blocks per launch, each block striding over the running members'
-        tiles (default 1); 0 launches one block per tile."""
+    def set_tuning(self, waves: int | None = None, spoil_maps: bool | None = None):
+        """Launch shape of the grouped launches: 0 (default) launches one
+        block per tile; `waves` > 0 launches that many waves of the GPU's
+        resident blocks, each block striding over the tiles.  `spoil_maps`
+        uploads the staging maps without the tag the kernels check before
+        their first copy (a test of that check: the next call fails with
+        GLIDE_ERR_STATE)."""
         if waves is not None:
             _lib.check(_lib.load().glide_group_set_tuning(self._g, 1, int(waves)))
+        if spoil_maps is not None:
+            _lib.check(_lib.load().glide_group_set_tuning(self._g, 2, 1 if spoil_maps else 0))
 
     def counters(self) -> dict:
         """Grouped launches issued so far, and the shape of the last forward

@@ -319,7 +319,11 @@ int glide_transfer(int op, int dtype, int ny_fine, int nx_fine, const void* src,
  * glide_forward takes them on the host.  stats: n entries, one per member
  * (may be NULL).  A
  * member whose residual becomes non-finite returns GLIDE_ERR_NONFINITE after
- * the others finish.  Plans (the merged launch lists and their graphs) are
+ * the others finish; one whose staged tiles fail (a bounded wait that gave
+ * up: GLIDE_ERR_TIMEOUT; staging maps in device memory that fail their
+ * check, so that no copy used them: GLIDE_ERR_STATE) stops and is reported
+ * the same way.  The staging maps of a plan are copied to the device on the
+ * call's stream before its graph is captured.  Plans (the merged launch lists and their graphs) are
  * rebuilt when dt, start_level, grad_mask or any member's configuration
  * changes. */
 typedef struct glide_group_s* glide_group;
@@ -329,11 +333,17 @@ int glide_group_forward(glide_group g, double dt, int start_level, glide_stats* 
 int glide_group_backward(glide_group g, double dt, int start_level, int grad_mask, glide_stats* stats,
                          void* stream);
 /* Launch shape of the grouped launches (no counterpart in the reference).
- * GLIDE_GROUP_TUNE_WAVES: the grid is value x the resident blocks of the
- * GPU, every block striding over the tiles of the running members (default
- * 1); 0 launches one block per tile of every member instead.  Plans are
- * recaptured on the next call. */
+ * GLIDE_GROUP_TUNE_WAVES: 0 (default) launches one block per tile of every
+ * member; value > 0 makes the grid value x the resident blocks of the GPU,
+ * every block striding over the tiles.  Plans are recaptured on the next
+ * call. */
 #define GLIDE_GROUP_TUNE_WAVES 1
+/* GLIDE_GROUP_TUNE_SPOIL_MAPS: 1 uploads every staging map without the tag
+ * the kernels check before their first copy, which tests that check: each
+ * member stops after its first stencil launch and the call fails with
+ * GLIDE_ERR_STATE, no copy having used the maps; 0 (default) restores the
+ * plain upload.  Plans are rebuilt on the next call. */
+#define GLIDE_GROUP_TUNE_SPOIL_MAPS 2
 int glide_group_set_tuning(glide_group g, int key, int value);
 /* launches: grouped launches issued so far.  shape (4 ints, may be NULL): the
  * last forward cycle's grouped launches and the members' launches they

@@ -121,6 +121,33 @@ def test_group_refuses_mixed_members():
         HierarchyGroup([b.mg.hierarchy, b.mg.hierarchy])  # a handle twice
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_group_stops_on_staging_maps_that_fail_their_check(precision):
+    """Staging maps in device memory that do not carry their tag are never
+    handed to the TMA unit: the first stencil launch of each member records
+    that in the member's error word, the member stops, and the call fails
+    with GLIDE_ERR_STATE.  With the maps uploaded intact the same group solves
+    again (the words were cleared when reported)."""
+    from glide_b200 import _lib
+    from glide_b200.group import HierarchyGroup
+    members = _members(precision)[:3]
+    g = HierarchyGroup([m.mg.hierarchy for m in members])
+    g.set_tuning(spoil_maps=True)
+    with pytest.raises(_lib.GlideError) as err:
+        g.forward(DT)
+    assert err.value.code == _lib.GLIDE_ERR_STATE
+    assert "staging maps" in str(err.value)
+    g.set_tuning(spoil_maps=False)
+    for m in members:  # the state the failed call left is not a solve's; start again from the dome
+        h = m.mg.hierarchy
+        for f in ("u", "v"):
+            h.set(f, 0, torch.zeros_like(h.get(f, 0)), restrict_down=True)
+        h.set("H", 0, m.mg.levels[0].state.H_prev.data, restrict_down=True)
+    st = g.forward(DT)
+    assert all(np.isfinite(s["final_norm"]) and s["vcycles"] > 0 for s in st)
+    g.close()
+
+
 def test_group_reports_a_nonfinite_member_and_solves_the_others():
     """A member whose residual is not finite makes the group call return
     GLIDE_ERR_NONFINITE after the others finish; the others' solves are
