@@ -3,7 +3,7 @@
 // A group runs the same solver cycle on many independent hierarchies (the
 // members of an ensemble, of uneven sizes).  Each member's cycle is recorded
 // as its sequence of launches; launches of one kind from different members
-// are merged into ONE persistent launch over a table of items, one per
+// are merged into ONE launch over a table of items, one per
 // member: its arguments and its tile grid.  The table is the launch's kernel
 // parameters (__grid_constant__, up to 32 KB, read through the constant
 // bank).  A block finds its tile's item by a binary search over the table
@@ -62,7 +62,7 @@ struct GroupItem {
 };
 
 constexpr int kGroupParamBytes = 32000;  // below the 32764-byte kernel parameter limit
-constexpr int kGroupMaxItems = 64;        // items of one launch (two per lane of the scanning warp)
+constexpr int kGroupMaxItems = 64;        // items of one launch (six steps of the item search at most)
 
 template <class A>
 constexpr int group_capacity() {
