@@ -108,7 +108,7 @@ def parse(argv=None):
     ap.add_argument("--enth-column-l1", type=int, default=None, help="1: column kernel prefers max L1")
     ap.add_argument("--mode", default="step",
                     choices=["step", "sweeps", "kernels", "thermal", "columns", "ensemble", "group", "vti",
-                             "coupled"],
+                             "coupled", "configs"],
                     help="sweeps: only N fine-level Vanka sweeps on the workload (profiling case)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--presolve", type=int, default=0, help="sweeps mode: V-cycles run before timing")
@@ -1303,6 +1303,159 @@ def reference_gpu_leg(a, f):
     return out, warm
 
 
+CONFIG_CASES = {
+    # C1: the 64^2 slab (dx 1000 m, 4 levels, dt 10 a), one step of 3 V-cycles
+    "C1": dict(n=64, dx=1000.0, levels=4, dt=10.0, steps=20, warmup=3),
+    # C2: the 512^2 dome (dx 1500 m, R 600 km, 5 levels, dt 10 a), 20 steps of 3 V-cycles
+    "C2": dict(n=512, dx=1500.0, levels=5, dt=10.0, steps=20, warmup=3),
+}
+CONFIG_VCYCLES = 3
+
+
+def _config_fields(name, c):
+    from cases import dome, slab_c1
+    return slab_c1(c["n"], c["n"], c["dx"]) if name == "C1" else dome(c["n"], c["dx"], 600e3, seed=0)
+
+
+def _config_ours(f, c, precision, stream):
+    """This build on one configuration, the reference algorithm (reference
+    mode, its 10/20/50/200 schedule and 30 local Newton iterations) with
+    exactly CONFIG_VCYCLES forward cycles per step; then forward + adjoint
+    steps (CONFIG_VCYCLES adjoint cycles from lambda = 0, forcing -dJ/du of
+    J = 0.5 |u - 0.95 u*|^2, then the gradients)."""
+    from glide_b200.hierarchy import Hierarchy
+    n = c["n"]
+    h = Hierarchy(n, n, c["dx"], c["levels"], precision=precision)
+    load_dome(h, f)
+    for adj in (False, True):
+        h.set_fas(adj, maximum_vcycles=CONFIG_VCYCLES, relative_tolerance=0.0, absolute_tolerance=0.0)
+    step = step_fn(h, c["dt"])
+    stats = []
+    for _ in range(c["warmup"]):
+        step()
+    fwd_ms = event_time(lambda: stats.append(step()), c["steps"], stream)
+
+    def fwd_adj():
+        step()
+        h.set("adj_f_u", 0, -0.05 * h.get("u", 0))
+        h.set("adj_f_v", 0, -0.05 * h.get("v", 0))
+        h.set("adj_f_H", 0, 0.0)
+        for nm in ("lambda_u", "lambda_v", "lambda_H"):
+            h.set(nm, 0, 0.0, restrict_down=True)
+        return h.backward(c["dt"], 0)
+    fwd_adj()
+    adj = []
+    fa_ms = event_time(lambda: adj.append(fwd_adj()), max(2, c["steps"] // 4), stream)
+    rel = [s["final_norm"] / s["initial_norm"] for s in stats if s["initial_norm"] > 0]
+    arel = [s["final_norm"] / s["initial_norm"] for s in adj if s["initial_norm"] > 0]
+    return {"ms_per_step": fwd_ms, "steps_per_s": 1000.0 / fwd_ms,
+            "worst_relative_residual": float(max(rel)) if rel else None,
+            "forward_adjoint_ms": fa_ms, "grads_per_s": 1000.0 / fa_ms,
+            "worst_adjoint_relative_residual": float(max(arel)) if arel else None}
+
+
+def _config_reference_gpu(f, c):
+    """The reference's own kernels on the GPU (oracle/ref_gpu.py), the same
+    steps as _config_ours: CONFIG_VCYCLES forward (and adjoint) cycles per
+    step, binary32 as the reference computes."""
+    import torch
+    from oracle import ref_gpu
+    n = c["n"]
+    m = ref_gpu.RefGpuModel(n, n, c["dx"], c["levels"])
+    for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+        m.set_field(k, torch.as_tensor(f[k], device="cuda"))
+    for cfg in (m.fas, m.adj):
+        cfg.maximum_vcycles, cfg.relative_tolerance, cfg.absolute_tolerance = CONFIG_VCYCLES, 0.0, 0.0
+    for _ in range(c["warmup"]):
+        m.forward(c["dt"])
+    stream = torch.cuda.current_stream()
+    rel = []
+    fwd_ms = event_time(lambda: (m.forward(c["dt"]), rel.append(m.history[-1] / m.history[0])), c["steps"],
+                        stream)
+    top = m.levels[0]
+
+    def fwd_adj():
+        m.forward(c["dt"])
+        m.backward(c["dt"], dJdu=0.05 * top.u, dJdv=0.05 * top.v)
+        return m.adj_history[-1] / m.adj_history[0]
+    fwd_adj()
+    arel = []
+    fa_ms = event_time(lambda: arel.append(fwd_adj()), max(2, c["steps"] // 4), stream)
+    del m
+    torch.cuda.empty_cache()
+    return {"ms_per_step": fwd_ms, "steps_per_s": 1000.0 / fwd_ms, "worst_relative_residual": float(max(rel)),
+            "forward_adjoint_ms": fa_ms, "grads_per_s": 1000.0 / fa_ms,
+            "worst_adjoint_relative_residual": float(max(arel))}
+
+
+def _config_cpu_oracle(f, c, budget_s):
+    """The binary64 C++/OpenMP oracle on host cores (wall clock): complete
+    steps of CONFIG_VCYCLES V-cycles while they fit the budget, else one
+    complete forward V-cycle and one complete adjoint V-cycle, each timed
+    once and multiplied by CONFIG_VCYCLES (the sample says which)."""
+    from oracle.glide_oracle import OracleHierarchy
+    n = c["n"]
+    o = OracleHierarchy(n, n, c["dx"], c["levels"])
+    for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+        o.set_field(k, f[k])
+    top = o.levels[0]
+    o.fas.relative_tolerance = o.fas.absolute_tolerance = 0.0
+    o.adj.relative_tolerance = o.adj.absolute_tolerance = 0.0
+    o.fas.maximum_vcycles = o.adj.maximum_vcycles = 1
+    t0 = time.perf_counter()
+    o.solve(c["dt"])
+    t_f1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.backward(c["dt"], dJdu=0.05 * top.u, dJdv=0.05 * top.v)
+    t_a1 = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0))
+    whole = CONFIG_VCYCLES * (t_f1 + t_a1) * 3 < budget_s
+    if whole:  # complete steps, best of 3
+        o.fas.maximum_vcycles = o.adj.maximum_vcycles = CONFIG_VCYCLES
+        fwd, fa = [], []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            o.solve(c["dt"])
+            t1 = time.perf_counter()
+            o.backward(c["dt"], dJdu=0.05 * top.u, dJdv=0.05 * top.v)
+            t2 = time.perf_counter()
+            fwd.append(t1 - t0)
+            fa.append(t2 - t0)
+        t_fwd, t_fa = min(fwd), min(fa)
+        sample = f"complete steps of {CONFIG_VCYCLES} forward and {CONFIG_VCYCLES} adjoint V-cycles, best of 3"
+    else:
+        t_fwd = CONFIG_VCYCLES * t_f1
+        t_fa = t_fwd + CONFIG_VCYCLES * t_a1
+        sample = (f"one complete forward V-cycle ({t_f1:.2f} s, with its residuals) and one complete adjoint "
+                  f"V-cycle with the gradients ({t_a1:.2f} s) from the start state, times {CONFIG_VCYCLES}")
+    return {"ms_per_step": 1e3 * t_fwd, "steps_per_s": 1.0 / t_fwd, "forward_adjoint_ms": 1e3 * t_fa,
+            "grads_per_s": 1.0 / t_fa, "cores": cores, "sample": sample}
+
+
+def run_configs(a):
+    """The configurations' table: C1 (64^2 slab) and C2 (512^2 dome) forward
+    steps of 3 V-cycles, and their forward + adjoint steps with gradients
+    (C3 is the C2 dome's gradient), for this build in binary64 and in mixed
+    precision (the same algorithm: binary32 smoother and coarse levels under
+    binary64 defect correction), for the reference's own kernels on the same
+    GPU, and for the binary64 C++/OpenMP oracle on the host cores."""
+    import torch
+    stream = torch.cuda.current_stream()
+    out = {"vcycles_per_step": CONFIG_VCYCLES,
+           "algorithm": "the reference's FASCD and FASAdjoint (10/20/50/200 sweeps, 30 local Newton iterations, "
+                        "reference mode), a fixed 3 V-cycles per forward or adjoint solve"}
+    for name, c in CONFIG_CASES.items():
+        f = _config_fields(name, c)
+        row = {"grid": f"{c['n']}^2", "dx": c["dx"], "levels": c["levels"], "dt": c["dt"], "steps": c["steps"],
+               "warmup": c["warmup"]}
+        row["ours_fp64"] = _config_ours(f, c, "fp64", stream)
+        row["ours_mixed"] = _config_ours(f, c, "mixed", stream)
+        row["reference_gpu"] = _config_reference_gpu(f, c)
+        row["cpu_oracle_fp64"] = _config_cpu_oracle(f, c, a.cpu_seconds)
+        out[name] = row
+    return out
+
+
 def run_reference(a):
     """The reference arm.  `value`: the reference's own kernels compiled for
     the host (oracle/_ref, binary32 as written) with its host loop -- one
@@ -1440,6 +1593,9 @@ def main():
         return 0
     if a.mode == "group":
         print(json.dumps({"mode": "group", **run_group_case(a)}), flush=True)
+        return 0
+    if a.mode == "configs":
+        print(json.dumps({"mode": "configs", **run_configs(a)}), flush=True)
         return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
