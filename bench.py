@@ -401,8 +401,11 @@ def kernel_roofline(a, h, stream, fields=None, probe=False):
     # state-preserving kernels first, then the sweep (which moves the state)
     kernels = [("k_residual", lambda: k.residual(0, a.dt, 8), 15 * n * itemsize),
                ("k_jvp", lambda: k.jvp(0, a.dt, reference_rows=False), 14 * n * itemsize)]
-    kernels += [("k_block_factor", lambda: k.block_factor(0, a.dt), 34 * n * itemsize),
-                ("k_block_sweep", lambda: k.block_sweep(0, a.dt), 34 * n * itemsize)]
+    # the block factors: 25 values per cell, in 13 bfloat16 pairs (52 bytes)
+    # under the binary32 tangent smoother
+    fbytes = 52 if itemsize == 4 else 25 * itemsize
+    kernels += [("k_block_factor", lambda: k.block_factor(0, a.dt), (9 * itemsize + fbytes) * n),
+                ("k_block_sweep", lambda: k.block_sweep(0, a.dt), (9 * itemsize + fbytes) * n)]
     kernels += [("k_vanka_sweep", lambda: k.vanka_sweep(0, a.dt, 1), 15 * n * itemsize)]
     for name, fn, nbytes in kernels:
         fn()

@@ -11,6 +11,8 @@
 // the u faces on x = 0, nx, the v faces on y = 0, ny, or masked cells).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "forward_kernels.cuh"
 #include "tma.cuh"
 
@@ -484,13 +486,66 @@ __global__ void __launch_bounds__(kSweepThreads) k_adjoint_sweep(AdjSweepArgs<R>
 // 25 values per cell, structure-of-arrays (value k of cell (i,j) at
 // f[k * plane + i * pitch + j]), L below the diagonal, U above it and the
 // pivot reciprocals on it.  The smoother then costs one triangular solve.
+//
+// The binary32 tangent smoother (the forward direction) stores its factors
+// in bfloat16 pairs (8 significant bits, the binary32 exponent range) and
+// solves with them in binary32: the stored factors are 25 of the 34 values a
+// sweep moves per cell, and the smoother needs only an approximate inverse,
+// since the Newton residual it serves covers every row.  The adjoint keeps
+// binary32 factors: its sweep zeroes the pinned rows' right-hand side, so
+// the values next to them are the smoother's own and would carry the
+// factors' rounding into the converged adjoint.  Binary64 smoothers keep
+// binary64 factors.  The buffer is sized for R either way.
 // -------------------------------------------------------------------------
+// Storage of one cell's 25 factors: kPlanes planes of `type`, at
+// f[q * plane + i * pitch + j].
+template <class R, bool TR>
+struct FactorStore {
+    using type = R;
+    static constexpr int kPlanes = 25;
+    static __device__ __forceinline__ void put(R* base, size_t plane, size_t at, const R (&M)[25]) {
+        R* f = base + at;
+#pragma unroll
+        for (int k = 0; k < 25; ++k) f[k * plane] = M[k];
+    }
+    static __device__ __forceinline__ void get(const R* base, size_t plane, size_t at, R (&M)[25]) {
+        const R* f = base + at;
+#pragma unroll
+        for (int k = 0; k < 25; ++k) M[k] = __ldg(f + k * plane);
+    }
+};
+// bfloat16 pairs: factors 2q and 2q + 1 in plane q (factor 24 alone in plane
+// 12), one 4-byte load per pair.
+template <>
+struct FactorStore<float, false> {
+    using type = __nv_bfloat162;
+    static constexpr int kPlanes = 13;
+    static __device__ __forceinline__ void put(float* base, size_t plane, size_t at, const float (&M)[25]) {
+        __nv_bfloat162* f = reinterpret_cast<__nv_bfloat162*>(base) + at;
+#pragma unroll
+        for (int q = 0; q < 13; ++q) f[q * plane] = __floats2bfloat162_rn(M[2 * q], q < 12 ? M[2 * q + 1] : 0.0f);
+    }
+    static __device__ __forceinline__ void get(const float* base, size_t plane, size_t at, float (&M)[25]) {
+        const unsigned* f = reinterpret_cast<const unsigned*>(base) + at;
+#pragma unroll
+        for (int q = 0; q < 13; ++q) {
+            const unsigned w = __ldg(f + q * plane);
+            __nv_bfloat162 h;
+            static_assert(sizeof(h) == sizeof(w), "a bfloat16 pair is one word");
+            memcpy(&h, &w, sizeof(w));
+            const float2 v = __bfloat1622float2(h);
+            M[2 * q] = v.x;
+            if (q < 12) M[2 * q + 1] = v.y;
+        }
+    }
+};
+
 template <class R>
 struct BlockArgs {
     Arr<R> u, v, H, phi, mask, bed, B, beta;
     Arr<R> ru, rv, rH;  // residual of the linear system (sweep)
     Arr<R> xu, xv, xH;  // unknowns, updated in place (sweep)
-    R* f;               // factors
+    R* f;               // factors (FactorStore<R, TR> layout; the buffer holds 25 planes of R)
     size_t plane;
     int pitch;
     int* err;           // set when a bounded wait gives up
@@ -543,9 +598,7 @@ __device__ __forceinline__ void block_factor_tile(const BlockArgs<R>& a, const B
         }
         M[k * 5 + k] = inv;
     }
-    R* f = a.f + size_t(i) * a.pitch + j;
-#pragma unroll
-    for (int k = 0; k < 25; ++k) f[k * a.plane] = M[k];
+    FactorStore<R, TR>::put(a.f, a.plane, size_t(i) * a.pitch + j, M);
 }
 
 template <class R, bool TR>
@@ -580,10 +633,8 @@ __device__ __forceinline__ void block_sweep_tile(const BlockArgs<R>& a, BLK blk)
             if (i == ny - 1) b[3] = R(0);
             if (a.mask.at(i, j) > R(0.5)) b[4] = R(0);
         }
-        const R* f = a.f + size_t(i) * a.pitch + j;
         R M[25];
-#pragma unroll
-        for (int k = 0; k < 25; ++k) M[k] = ldg(f + k * a.plane);
+        FactorStore<R, TR>::get(a.f, a.plane, size_t(i) * a.pitch + j, M);
         R y0 = b[0];
         R y1 = b[1] - M[5] * y0;
         R y2 = b[2] - M[10] * y0 - M[11] * y1;

@@ -1091,7 +1091,7 @@ struct Solver : SolverBase {
     void block_factor(int l, double dt, const Lin& L, cudaStream_t s) {
         BlockArgs<R> a = block_args(l, dt, L);
         dim3 g(lv[l].blocks_x(), lv[l].blocks_y());
-        const double bytes = lb(l, 9 + 25);  // state read, 25 factor planes written
+        const double bytes = lb(l, 9) + factor_bytes(l, L.tr);  // state read, 25 factor planes written
         if (record(G_BLOCK_FACTOR, L.tr ? 1 : 0, g, a, bytes)) {
             attach_maps(box_maps(l, kStateBoxes));
             return;
@@ -1115,12 +1115,20 @@ struct Solver : SolverBase {
         }
     }
 
+    // the 25 factor planes of level l
+    double factor_bytes(int l, bool tr) const {
+        const double per_cell = tr ? FactorStore<R, true>::kPlanes * sizeof(typename FactorStore<R, true>::type)
+                                   : FactorStore<R, false>::kPlanes * sizeof(typename FactorStore<R, false>::type);
+        return lb(l, per_cell / double(sizeof(R)));
+    }
+
     // 25 factors, r, x read; x written
     void block_sweep(int l, const BlockArgs<R>& a, bool tr, dim3 g, cudaStream_t s) {
-        if (record(G_BLOCK_SWEEP, tr ? 1 : 0, g, a, lb(l, 34))) return;
+        const double bytes = lb(l, 9) + factor_bytes(l, tr);
+        if (record(G_BLOCK_SWEEP, tr ? 1 : 0, g, a, bytes)) return;
         if (tr) k_block_sweep<R, true><<<g, kSweepThreads, 0, s>>>(a);
         else k_block_sweep<R, false><<<g, kSweepThreads, 0, s>>>(a);
-        counted("linear_sweep", lb(l, 34));
+        counted("linear_sweep", bytes);
     }
 
     void adj_sweeps(int l, double dt, int n, cudaStream_t s) { lin_sweeps(l, dt, n, adj_sys(), s); }
