@@ -87,7 +87,8 @@ def parse(argv=None):
     ap.add_argument("--members", type=int, default=64, help="ensemble mode: members")
     ap.add_argument("--ens-steps", type=int, default=10, help="ensemble mode: timed forward+adjoint steps")
     ap.add_argument("--ens-workers", type=int, default=16, help="ensemble mode: host workers (streams)")
-    ap.add_argument("--ens-precision", default="fp64", choices=["fp64", "mixed"], help="ensemble members")
+    ap.add_argument("--ens-precision", default=None, choices=["fp64", "mixed"],
+                    help="ensemble members (default: mixed; fp64 with --ens-grouped, which has no mixed form)")
     ap.add_argument("--ens-cold-tune", action="store_true", help="ensemble: autotune on the cold first step")
     ap.add_argument("--ens-grouped", action="store_true",
                     help="ensemble: grouped launches (glide_b200.group) instead of per-stream member solves")
@@ -833,19 +834,23 @@ def run_ensemble(a):
     U(1e-3, 3e-3) /m), each step a forward solve and an adjoint solve to a
     relative residual of 1e-8, the solver schedule autotuned per size class
     among Newton, short FASCD and the classic FASCD schedule; members run
-    concurrently (see glide_b200.ensemble)."""
+    concurrently (see glide_b200.ensemble), in mixed precision unless
+    --ens-precision says otherwise (grouped solves: binary64)."""
     import torch
     from cases import dome
     from glide_b200.ensemble import Ensemble, member_specs
     from glide_b200.model import IceDynamics
     sizes = tuple(int(x) for x in a.ens_sizes.split(","))
     specs = member_specs(a.members, seed=0, sizes=sizes)
+    precision = a.ens_precision or ("fp64" if a.ens_grouped else "mixed")
+    if a.ens_grouped and precision == "mixed":
+        raise SystemExit("--ens-grouped: grouped solves take binary64 or binary32 members, not mixed ones")
     max_cycles = max(a.max_vcycles, 100)  # small steep domes need up to ~60 classic cycles
     members = []
     for sp in specs:
         f = dome(sp.n, sp.dx, sp.radius, seed=sp.seed, lapse=sp.lapse)
         m = IceDynamics(n_levels=sp.levels, ny=sp.n, nx=sp.n, dx=sp.dx, reference_quirks=False,
-                        precision=a.ens_precision)
+                        precision=precision)
         mg = m.mg
         for k, grp in (("bed", mg.geometry), ("B", mg.rheology), ("beta", mg.sliding), ("smb", mg.forcing)):
             getattr(grp, k).set(torch.as_tensor(f[k]))
@@ -899,7 +904,7 @@ def run_ensemble(a):
             "mean_forward_cycles": float(np.mean(fv)), "mean_adjoint_cycles": float(np.mean(bv)),
             "worst_forward_relative_residual": worst, "forward_solves_converged": converged,
             "max_cycles": max_cycles, "workers": ens.workers, "adjoint": a.ens_adjoint,
-            "forward_retries": ens.retries, "precision": a.ens_precision,
+            "forward_retries": ens.retries, "precision": precision,
             "grouped": ens.grouped,
             "grouped_forward_members": len(ens._fwd_keys),
             "grouped_adjoint_members": len(ens._adj_keys),
