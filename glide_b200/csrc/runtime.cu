@@ -1493,9 +1493,10 @@ struct GroupRun : GroupBase {
         P.valid = true;
     }
 
-    // One persistent launch per N items of L (N: what fits the parameter
-    // space): at most one wave of resident blocks, striding over the tiles
-    // of the items whose member runs.
+    // One launch per N items of L (N: what fits the parameter space): one
+    // block per tile of every item (waves == 0), or `waves` waves of resident
+    // blocks striding over the tiles; blocks of an item whose member does not
+    // run this cycle return at once.
     template <class Op>
     long long issue_op(const Launch& L, cudaStream_t s) {
         using A = typename Op::Args;
