@@ -1440,26 +1440,31 @@ def _config_cpu_oracle(f, c, budget_s):
             "grads_per_s": 1.0 / t_fa, "cores": cores, "sample": sample}
 
 
-def run_configs(a):
+def run_configs(a, reference=False):
     """The configurations' table: C1 (64^2 slab) and C2 (512^2 dome) forward
     steps of 3 V-cycles, and their forward + adjoint steps with gradients
-    (C3 is the C2 dome's gradient), for this build in binary64 and in mixed
-    precision (the same algorithm: binary32 smoother and coarse levels under
-    binary64 defect correction), for the reference's own kernels on the same
-    GPU, and for the binary64 C++/OpenMP oracle on the host cores."""
+    (C3 is the C2 dome's gradient).  This build's arm times binary64 and
+    mixed precision (the same algorithm: binary32 smoother and coarse levels
+    under binary64 defect correction); the reference arm (--impl reference)
+    times the reference's own kernels on the same GPU and the binary64
+    C++/OpenMP oracle on the host cores."""
     import torch
     stream = torch.cuda.current_stream()
     out = {"vcycles_per_step": CONFIG_VCYCLES,
            "algorithm": "the reference's FASCD and FASAdjoint (10/20/50/200 sweeps, 30 local Newton iterations, "
                         "reference mode), a fixed 3 V-cycles per forward or adjoint solve"}
+    if reference:
+        out["impl"] = "reference"
     for name, c in CONFIG_CASES.items():
         f = _config_fields(name, c)
         row = {"grid": f"{c['n']}^2", "dx": c["dx"], "levels": c["levels"], "dt": c["dt"], "steps": c["steps"],
                "warmup": c["warmup"]}
-        row["ours_fp64"] = _config_ours(f, c, "fp64", stream)
-        row["ours_mixed"] = _config_ours(f, c, "mixed", stream)
-        row["reference_gpu"] = _config_reference_gpu(f, c)
-        row["cpu_oracle_fp64"] = _config_cpu_oracle(f, c, a.cpu_seconds)
+        if reference:
+            row["reference_gpu"] = _config_reference_gpu(f, c)
+            row["cpu_oracle_fp64"] = _config_cpu_oracle(f, c, a.cpu_seconds)
+        else:
+            row["ours_fp64"] = _config_ours(f, c, "fp64", stream)
+            row["ours_mixed"] = _config_ours(f, c, "mixed", stream)
         out[name] = row
     return out
 
@@ -1571,7 +1576,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if a.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(a)), flush=True)
+            if a.mode == "configs":
+                print(json.dumps({"mode": "configs", **run_configs(a, reference=True)}), flush=True)
+            else:
+                print(json.dumps(run_reference(a)), flush=True)
         return 0
     import torch.distributed as dist
     if a.mode == "sweeps":
