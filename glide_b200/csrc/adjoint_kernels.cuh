@@ -431,6 +431,15 @@ __global__ void __launch_bounds__(kSweepThreads) k_adjoint_sweep(AdjSweepArgs<R>
     else if (tid < kTile * kTile + kTile) { i = i0 + (tid - kTile * kTile); j = j0 - 1; }
     else { i = i0 - 1; j = j0 + (tid - kTile * kTile - kTile); }
     const bool live = i >= 0 && i < ny && j >= 0 && j < nx;
+    // the owned cells' unknowns, loaded with the factors rather than after the
+    // barrier (only this thread writes them)
+    const bool own = tid < kTile * kTile && live;
+    R xu0 = R(0), xv0 = R(0), xh0 = R(0);
+    if (own) {
+        xu0 = a.xu.at(i, j);
+        xv0 = a.xv.at(i, j);
+        xh0 = a.xH.at(i, j);
+    }
     R d4 = 0;
     R dd[4] = {0, 0, 0, 0};
     if (live) {
@@ -622,6 +631,15 @@ __device__ __forceinline__ void block_sweep_tile(const BlockArgs<R>& a, BLK blk)
     else if (tid < kTile * kTile + kTile) { i = i0 + (tid - kTile * kTile); j = j0 - 1; }
     else { i = i0 - 1; j = j0 + (tid - kTile * kTile - kTile); }
     const bool live = i >= 0 && i < ny && j >= 0 && j < nx;
+    // the owned cells' unknowns, loaded with the factors rather than after the
+    // barrier (only this thread writes them)
+    const bool own = tid < kTile * kTile && live;
+    R xu0 = R(0), xv0 = R(0), xh0 = R(0);
+    if (own) {
+        xu0 = a.xu.at(i, j);
+        xv0 = a.xv.at(i, j);
+        xh0 = a.xH.at(i, j);
+    }
     R d4 = 0;
     R dd[4] = {0, 0, 0, 0};
     if (live) {
@@ -654,16 +672,16 @@ __device__ __forceinline__ void block_sweep_tile(const BlockArgs<R>& a, BLK blk)
         for (int q = 0; q < 4; ++q) dl[di][dj][q] = dd[q];
     }
     __syncthreads();
-    if (tid < kTile * kTile && live) {
+    if (own) {
         const int di = i - (i0 - 1), dj = j - (j0 - 1);
         const R w = a.omega;
         R du = (j > 0 ? dl[di][dj - 1][1] : R(0)) + dl[di][dj][0];
-        a.xu.at(i, j) = a.xu.at(i, j) - w * du;
+        a.xu.at(i, j) = xu0 - w * du;
         if (j == nx - 1) a.xu.at(i, nx) = a.xu.at(i, nx) - w * dl[di][dj][1];
         R dv = (i > 0 ? dl[di - 1][dj][3] : R(0)) + dl[di][dj][2];
-        a.xv.at(i, j) = a.xv.at(i, j) - w * dv;
+        a.xv.at(i, j) = xv0 - w * dv;
         if (i == ny - 1) a.xv.at(ny, j) = a.xv.at(ny, j) - w * dl[di][dj][3];
-        a.xH.at(i, j) = a.xH.at(i, j) - w * d4;
+        a.xH.at(i, j) = xh0 - w * d4;
     }
 }
 
