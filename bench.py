@@ -347,9 +347,9 @@ def run_kernels(a):
 # binary32 fine-level kernels on the 2048^2 workload, from one ncu capture of
 # `python bench.py --mode kernels` on a B200 (the command and the figures are
 # in profiles/ssa_kernels_fp32_2048.md, with the commit they were taken at).
-NCU_TRAFFIC_2048_FP32 = {"k_residual": 222.960e6, "k_jvp": 218.918e6, "k_block_factor": 305.355e6,
-                         "k_block_sweep": 356.605e6, "k_vanka_sweep": 245.614e6}
-NCU_TRAFFIC_SOURCE = "profiles/ssa_kernels_fp32_2048.md (ncu, build 7a7c827)"
+NCU_TRAFFIC_2048_FP32 = {"k_residual": 222.868e6, "k_jvp": 218.683e6, "k_block_factor": 305.240e6,
+                         "k_block_sweep": 356.349e6, "k_vanka_sweep": 245.624e6}
+NCU_TRAFFIC_SOURCE = "profiles/ssa_kernels_fp32_2048.md (ncu, build e3ba9a8)"
 
 
 def kernel_roofline(a, h, stream, fields=None, probe=False):
