@@ -62,6 +62,40 @@ def test_c1_adjoint_matches_reference_f64():
         assert rel_err(grads[k], g[f"out_grad_{k}"]) <= 1e-12, k
 
 
+def test_c1_adjoint_solution_depends_on_the_smoother():
+    """A property of the reference's adjoint, shown on the oracle pinned to
+    it: the adjoint sweep zeroes the right-hand side of the pinned rows
+    (Dirichlet faces, masked cells), and the adjoint residual leaves those
+    rows out, so the residual does not determine lambda there.  Two solves of
+    the C1 adjoint that converge the residual to 1e-12 under different
+    smoother weights end at different lambda: by about 2 % next to the
+    domain edges and 0.1 % inside, and the bed gradient moves by about 2 %.
+    This is why binary32 adjoint smoothers keep binary32 block factors:
+    rounding the factors would move the converged adjoint the same way."""
+    from cases import slab_c1
+    from oracle.glide_oracle import OracleHierarchy
+    f = slab_c1()
+
+    def run(omega):
+        o = OracleHierarchy(64, 64, 1000.0, 4)
+        for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
+            o.set_field(k, f[k])
+        o.fas.maximum_vcycles, o.fas.relative_tolerance, o.fas.absolute_tolerance = 30, 1e-11, 0.0
+        o.solve(10.0)
+        top = o.levels[0]
+        o.adj.maximum_vcycles, o.adj.relative_tolerance, o.adj.absolute_tolerance = 200, 1e-12, 0.0
+        for lev in o.levels:
+            lev.adj_vanka.omega = omega
+        g = o.backward(10.0, dJdu=0.1 * top.u, dJdv=0.1 * top.v)
+        assert o.adj_history[-1] <= 1e-12 * o.adj_history[0]
+        return top.l_v.copy(), g["bed"]
+
+    lv_a, bed_a = run(0.5)
+    lv_b, bed_b = run(0.8)
+    assert rel_err(lv_b, lv_a) >= 1e-3
+    assert rel_err(bed_b, bed_a) >= 1e-3
+
+
 @pytest.mark.parametrize("tag,calving", [("", 0.0), ("_calving", 2.0)])
 def test_random_residual_matches_reference(tag, calving):
     g = load_golden("random_residual_f64")
