@@ -49,6 +49,28 @@ GRAD_ALL = 15
 
 MAX_HISTORY = 256
 
+# glide_set_tuning keys (GLIDE_TUNE_*) and glide_group_set_tuning keys (GLIDE_GROUP_TUNE_*)
+TUNE_SWEEP_BLOCKS_PER_SM = 1
+TUNE_MIXED_INNER_VCYCLES = 2
+TUNE_FORWARD_METHOD = 3
+TUNE_NEWTON_SWITCH_EXP10 = 4
+TUNE_TANGENT_VCYCLES = 5
+TUNE_TMA_STAGING = 6
+TUNE_REPORT_NOT_CONVERGED = 7
+TUNE_TMA_GIVE_UP = 8
+GROUP_TUNE_WAVES = 1
+GROUP_TUNE_SPOIL_MAPS = 2
+
+# glide_enthalpy_set_tuning keys (GLIDE_ENTH_TUNE_*) and enthalpy term bits (GLIDE_ENTH_*)
+ENTH_TUNE_POINT_BLOCKS = 1
+ENTH_TUNE_COLUMN_BLOCKS = 2
+ENTH_TUNE_COLUMN_L1 = 3
+ENTH_TUNE_COLUMN_KERNEL = 4
+ENTH_HORIZ_ADV = 1
+ENTH_SIGMA_DOT = 2
+ENTH_DRAINAGE = 4
+ENTH_MAX_HISTORY = 256
+
 # glide_transfer op codes
 TRANSFER_OPS = {
     "restrict_vfacet": 0, "restrict_hfacet": 1, "restrict_cell_avg": 2, "restrict_cell_max": 3,

@@ -118,8 +118,8 @@ class EnthalpyTermFlags:
 
     @property
     def bitmask(self) -> int:
-        return ((1 if self.horizontal_advection else 0) | ((1 if self.omega else 0) << 1)
-                | ((1 if self.drainage else 0) << 2))
+        return ((_lib.ENTH_HORIZ_ADV if self.horizontal_advection else 0)
+                | (_lib.ENTH_SIGMA_DOT if self.omega else 0) | (_lib.ENTH_DRAINAGE if self.drainage else 0))
 
 
 def _no_hook(i):
@@ -260,13 +260,14 @@ class EnthalpyOperators:
         threads per SM), "smem8" (the same at 8 blocks per SM) or "local"
         (per-thread arrays)."""
         if column_kernel is not None:
-            _ecall("glide_enthalpy_set_tuning", self._h, 4, {"local": 0, "smem": 1, "smem8": 2}[column_kernel])
+            _ecall("glide_enthalpy_set_tuning", self._h, _lib.ENTH_TUNE_COLUMN_KERNEL,
+                   {"local": 0, "smem": 1, "smem8": 2}[column_kernel])
         if point_blocks_per_sm is not None:
-            _ecall("glide_enthalpy_set_tuning", self._h, 1, int(point_blocks_per_sm))
+            _ecall("glide_enthalpy_set_tuning", self._h, _lib.ENTH_TUNE_POINT_BLOCKS, int(point_blocks_per_sm))
         if column_blocks_per_sm is not None:
-            _ecall("glide_enthalpy_set_tuning", self._h, 2, int(column_blocks_per_sm))
+            _ecall("glide_enthalpy_set_tuning", self._h, _lib.ENTH_TUNE_COLUMN_BLOCKS, int(column_blocks_per_sm))
         if column_prefers_l1 is not None:
-            _ecall("glide_enthalpy_set_tuning", self._h, 3, int(bool(column_prefers_l1)))
+            _ecall("glide_enthalpy_set_tuning", self._h, _lib.ENTH_TUNE_COLUMN_L1, int(bool(column_prefers_l1)))
 
     def counters(self):
         """(kernels launched, their algorithmic bytes) so far on this

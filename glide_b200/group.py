@@ -74,9 +74,9 @@ class HierarchyGroup:
         their first copy (a test of that check: the next call fails with
         GLIDE_ERR_STATE)."""
         if waves is not None:
-            _lib.check(_lib.load().glide_group_set_tuning(self._g, 1, int(waves)))
+            _lib.check(_lib.load().glide_group_set_tuning(self._g, _lib.GROUP_TUNE_WAVES, int(waves)))
         if spoil_maps is not None:
-            _lib.check(_lib.load().glide_group_set_tuning(self._g, 2, 1 if spoil_maps else 0))
+            _lib.check(_lib.load().glide_group_set_tuning(self._g, _lib.GROUP_TUNE_SPOIL_MAPS, 1 if spoil_maps else 0))
 
     def counters(self) -> dict:
         """Grouped launches issued so far, and the shape of the last forward

@@ -202,21 +202,21 @@ class Hierarchy:
         gives up at once, so the call fails with GLIDE_ERR_TIMEOUT (a test of
         that path; the blocks still let their copies land before returning)."""
         if sweep_blocks_per_sm is not None:
-            call("glide_set_tuning", self._h, 1, int(sweep_blocks_per_sm))
+            call("glide_set_tuning", self._h, _lib.TUNE_SWEEP_BLOCKS_PER_SM, int(sweep_blocks_per_sm))
         if mixed_inner_vcycles is not None:
-            call("glide_set_tuning", self._h, 2, int(mixed_inner_vcycles))
+            call("glide_set_tuning", self._h, _lib.TUNE_MIXED_INNER_VCYCLES, int(mixed_inner_vcycles))
         if forward_method is not None:
-            call("glide_set_tuning", self._h, 3, {"fascd": 0, "newton": 1}[forward_method])
+            call("glide_set_tuning", self._h, _lib.TUNE_FORWARD_METHOD, {"fascd": 0, "newton": 1}[forward_method])
         if newton_switch_exp10 is not None:
-            call("glide_set_tuning", self._h, 4, int(newton_switch_exp10))
+            call("glide_set_tuning", self._h, _lib.TUNE_NEWTON_SWITCH_EXP10, int(newton_switch_exp10))
         if tangent_vcycles is not None:
-            call("glide_set_tuning", self._h, 5, int(tangent_vcycles))
+            call("glide_set_tuning", self._h, _lib.TUNE_TANGENT_VCYCLES, int(tangent_vcycles))
         if tma_staging is not None:
-            call("glide_set_tuning", self._h, 6, int(bool(tma_staging)))
+            call("glide_set_tuning", self._h, _lib.TUNE_TMA_STAGING, int(bool(tma_staging)))
         if report_not_converged is not None:
-            call("glide_set_tuning", self._h, 7, int(bool(report_not_converged)))
+            call("glide_set_tuning", self._h, _lib.TUNE_REPORT_NOT_CONVERGED, int(bool(report_not_converged)))
         if tma_give_up is not None:
-            call("glide_set_tuning", self._h, 8, int(bool(tma_give_up)))
+            call("glide_set_tuning", self._h, _lib.TUNE_TMA_GIVE_UP, int(bool(tma_give_up)))
 
     def launch_count(self) -> int:
         c = ctypes.c_longlong()

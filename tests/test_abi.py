@@ -20,6 +20,50 @@ def declared_functions():
     return sorted(set(names))
 
 
+def header_defines():
+    """Every integer #define GLIDE_* of the public headers."""
+    out = {}
+    for h in sorted((ROOT / "include").glob("*.h")):
+        for name, val in re.findall(r"^#define (GLIDE_\w+) (-?\d+)\b", h.read_text(), flags=re.M):
+            out[name] = int(val)
+    return out
+
+
+def python_name(define):
+    """The glide_b200._lib constant that mirrors a header define."""
+    name = define[len("GLIDE_"):]
+    if name.startswith(("ERR_", "F64", "F32", "MIXED")) or name == "OK":
+        return "GLIDE_" + name
+    if name.startswith("GRAD_") and name.endswith("_BIT"):
+        return name[:-len("_BIT")]
+    return name
+
+
+def test_python_constants_match_the_headers():
+    """Error codes, precisions, flags, tuning keys (solver, group, enthalpy),
+    term bits and VTI kinds as the Python layer passes them through the ABI
+    equal the headers' values, and none of the keys lacks a mirror."""
+    from glide_b200 import _lib
+    defines = header_defines()
+    must = [d for d in defines if d.startswith(("GLIDE_ERR_", "GLIDE_TUNE_", "GLIDE_GROUP_TUNE_",
+                                                "GLIDE_ENTH_TUNE_", "GLIDE_VTI_"))]
+    assert len(must) >= 20
+    checked = 0
+    for d, v in defines.items():
+        if d.startswith(("GLIDE_RESTRICT_", "GLIDE_PROLONG_")):
+            op = d[len("GLIDE_"):].lower().replace("prolong_", "prolongate_")
+            assert _lib.TRANSFER_OPS[op] == v, d
+            checked += 1
+            continue
+        mirror = getattr(_lib, python_name(d), None)
+        if mirror is None:
+            assert d not in must, f"{d} has no Python mirror"
+            continue
+        assert mirror == v, (d, mirror, v)
+        checked += 1
+    assert checked >= 50
+
+
 def test_headers_declare_entry_points():
     names = declared_functions()
     assert "glide_forward" in names and "glide_enthalpy_column_sweep" in names
