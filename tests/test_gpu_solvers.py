@@ -281,8 +281,9 @@ def test_rejected_newton_step_is_undone():
 def test_adjoint_converges_to_reference_adjoint(precision):
     """Converged adjoint of C1 (binary64 reference form) against the fast
     forms: lambda to 1e-8 relative, gradients to 1e-7.  The mixed adjoint
-    smoother keeps binary32 block factors: with bfloat16 ones the values next
-    to the pinned rows (whose right-hand side the adjoint sweep zeroes) moved
+    smoother keeps binary32 block factors: in reference mode the converged
+    adjoint depends on the cycle's path (the reference's v-face prolongation
+    writes into the pinned v faces), and with bfloat16 factors it moved
     2.4e-6 from binary64."""
     def run(prec, quirks):
         h, st = _solve_c1(precision=prec, quirks=quirks)

@@ -62,22 +62,25 @@ def test_c1_adjoint_matches_reference_f64():
         assert rel_err(grads[k], g[f"out_grad_{k}"]) <= 1e-12, k
 
 
-def test_c1_adjoint_solution_depends_on_the_smoother():
+def test_c1_adjoint_solution_depends_on_the_smoother_in_reference_mode():
     """A property of the reference's adjoint, shown on the oracle pinned to
-    it: the adjoint sweep zeroes the right-hand side of the pinned rows
-    (Dirichlet faces, masked cells), and the adjoint residual leaves those
-    rows out, so the residual does not determine lambda there.  Two solves of
-    the C1 adjoint that converge the residual to 1e-12 under different
-    smoother weights end at different lambda: by about 2 % next to the
-    domain edges and 0.1 % inside, and the bed gradient moves by about 2 %.
-    This is why binary32 adjoint smoothers keep binary32 block factors:
-    rounding the factors would move the converged adjoint the same way."""
+    it.  The reference prolongates v-face corrections with its u-face kernel
+    run on the v arrays, which writes into the pinned v faces (rows 0 and
+    ny).  The adjoint residual leaves pinned rows out and the adjoint sweep
+    zeroes their right-hand side, so nothing brings those values back: two
+    solves of the C1 adjoint that converge the residual to 1e-12 under
+    different smoother weights end at different lambda (about 2 % next to the
+    domain edges, 0.1 % inside; the bed gradient moves by about 2 %).  With
+    the corrected transfers (native mode) the pinned faces stay zero and the
+    two solves agree to rounding.  This is why the binary32 adjoint smoothers
+    keep binary32 block factors: in reference mode, rounding the factors
+    moves the converged adjoint the same way."""
     from cases import slab_c1
     from oracle.glide_oracle import OracleHierarchy
     f = slab_c1()
 
-    def run(omega):
-        o = OracleHierarchy(64, 64, 1000.0, 4)
+    def run(omega, quirks):
+        o = OracleHierarchy(64, 64, 1000.0, 4, reference_quirks=quirks)
         for k in ("bed", "B", "beta", "smb", "H", "H_prev"):
             o.set_field(k, f[k])
         o.fas.maximum_vcycles, o.fas.relative_tolerance, o.fas.absolute_tolerance = 30, 1e-11, 0.0
@@ -90,10 +93,16 @@ def test_c1_adjoint_solution_depends_on_the_smoother():
         assert o.adj_history[-1] <= 1e-12 * o.adj_history[0]
         return top.l_v.copy(), g["bed"]
 
-    lv_a, bed_a = run(0.5)
-    lv_b, bed_b = run(0.8)
+    lv_a, bed_a = run(0.5, True)
+    lv_b, bed_b = run(0.8, True)
     assert rel_err(lv_b, lv_a) >= 1e-3
     assert rel_err(bed_b, bed_a) >= 1e-3
+    assert np.abs(lv_a[[0, -1]]).max() >= 1e-3 * np.abs(lv_a).max()  # the pinned v faces moved
+    lv_a, bed_a = run(0.5, False)
+    lv_b, bed_b = run(0.8, False)
+    assert rel_err(lv_b, lv_a) <= 1e-10
+    assert rel_err(bed_b, bed_a) <= 1e-10
+    assert np.abs(lv_a[[0, -1]]).max() == 0.0
 
 
 @pytest.mark.parametrize("tag,calving", [("", 0.0), ("_calving", 2.0)])
