@@ -166,4 +166,17 @@ def test_grouping_partitions_members_by_size_and_count():
     assert ens._parts(()) == []
     ens.group_max_cells = 256 * 256
     assert [k for k in keys if ens._in_groups(k)] == [0, 1, 2, 4, 5, 6]
+    ens.members[1].mg.hierarchy.precision = "mixed"  # no grouped form: solved on the worker streams
+    assert [k for k in keys if ens._in_groups(k)] == [0, 2, 4, 5, 6]
     ens.close()
+
+
+def test_bench_ensemble_precision_defaults():
+    """The bench's ensemble runs mixed-precision members by default, binary64
+    members when grouped, and refuses grouped mixed members before it builds
+    any member."""
+    import bench
+    a = bench.parse(["--mode", "ensemble", "--ens-grouped", "--ens-precision", "mixed"])
+    with pytest.raises(SystemExit, match="grouped solves"):
+        bench.run_ensemble(a)
+    assert bench.parse(["--mode", "ensemble"]).ens_precision is None
